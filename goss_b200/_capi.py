@@ -1,0 +1,174 @@
+"""ctypes binding of the C ABI in ``include/goss_b200.h``.
+
+The runtime library ``goss_b200/_lib/libgoss_b200.so`` is required: there is
+no CPU implementation behind this package, so a missing or unloadable
+library raises :class:`ExtensionMissingError` instead of falling back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+RUNTIME_SO = PKG / "_lib" / "libgoss_b200.so"
+
+ABI_VERSION = 1
+
+GOSS_EXPLICIT_EULER, GOSS_RK4, GOSS_GRL1, GOSS_GRL2, GOSS_THETA, GOSS_ESDIRK23A = range(6)
+GOSS_FP64, GOSS_FP32 = 0, 1
+GOSS_OK, GOSS_ERR_ARGUMENT, GOSS_ERR_CUDA, GOSS_ERR_NEWTON, GOSS_ERR_UNSUPPORTED, GOSS_ERR_TIMEOUT = range(6)
+GOSS_FLAG_NONFINITE, GOSS_FLAG_NEWTON_FAILED, GOSS_FLAG_ITERATION_CAP = 1, 2, 4
+
+SOLVER_KINDS = {
+    "ExplicitEuler": GOSS_EXPLICIT_EULER,
+    "RK4": GOSS_RK4,
+    "GRL1": GOSS_GRL1,
+    "GRL2": GOSS_GRL2,
+    "ThetaSolver": GOSS_THETA,
+    "ESDIRK23a": GOSS_ESDIRK23A,
+}
+
+
+class ExtensionMissingError(RuntimeError):
+    """The compiled goss_b200 CUDA library is not available."""
+
+
+class GossError(RuntimeError):
+    """An error status returned by the goss_b200 runtime."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class SolverParams(C.Structure):
+    _fields_ = [
+        ("ldt", C.c_double),
+        ("delta", C.c_double),
+        ("eta_0", C.c_double),
+        ("kappa", C.c_double),
+        ("relative_tolerance", C.c_double),
+        ("max_relative_previous_residual", C.c_double),
+        ("max_iterations", C.c_int32),
+        ("always_recompute_jacobian", C.c_int32),
+        ("num_refinements_without_always_recomputing_jacobian", C.c_int32),
+        ("min_dt", C.c_double),
+        ("theta", C.c_double),
+    ]
+
+
+class ModelDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("name", C.c_char_p),
+        ("num_states", C.c_uint32),
+        ("num_parameters", C.c_uint32),
+        ("num_field_parameters", C.c_uint32),
+        ("num_monitored", C.c_uint32),
+        ("state_names", C.POINTER(C.c_char_p)),
+        ("parameter_names", C.POINTER(C.c_char_p)),
+        ("field_parameter_names", C.POINTER(C.c_char_p)),
+        ("field_parameter_indices", C.POINTER(C.c_uint32)),
+        ("initial_conditions", C.POINTER(C.c_double)),
+        ("default_parameters", C.POINTER(C.c_double)),
+        ("linear_terms", C.POINTER(C.c_uint8)),
+        ("supported_solvers", C.c_uint32),
+        ("launch", C.c_void_p),
+        ("eval", C.c_void_p),
+        ("solver_state_rows", C.CFUNCTYPE(C.c_uint32, C.c_int32)),
+        ("op_census_linearized", C.POINTER(C.c_uint32)),
+        ("op_census_rhs", C.POINTER(C.c_uint32)),
+    ]
+
+
+_dp = C.POINTER(C.c_double)
+_u32p = C.POINTER(C.c_uint32)
+_i64p = C.POINTER(C.c_int64)
+_sys = C.c_void_p
+_desc = C.POINTER(ModelDesc)
+
+_PROTOS = {
+    "goss_abi_version": (C.c_uint32, []),
+    "goss_last_error": (C.c_char_p, []),
+    "goss_system_last_error": (C.c_char_p, [_sys]),
+    "goss_solver_default_params": (C.c_int, [C.c_int32, C.POINTER(SolverParams)]),
+    "goss_system_create": (C.c_int, [_desc, C.c_int32, C.POINTER(SolverParams), C.c_uint32, C.c_int32, C.c_int32,
+                                     C.POINTER(C.c_void_p)]),
+    "goss_system_destroy": (C.c_int, [_sys]),
+    "goss_system_set_solver_params": (C.c_int, [_sys, C.POINTER(SolverParams)]),
+    "goss_system_get_solver_params": (C.c_int, [_sys, C.POINTER(SolverParams)]),
+    "goss_system_forward": (C.c_int, [_sys, C.c_double, C.c_double]),
+    "goss_system_forward_async": (C.c_int, [_sys, C.c_double, C.c_double]),
+    "goss_system_synchronize": (C.c_int, [_sys]),
+    "goss_system_solve": (C.c_int, [_sys, _dp, _dp, C.c_uint64, C.c_int32]),
+    "goss_system_set_field_state_indices": (C.c_int, [_sys, _u32p, C.c_uint32]),
+    "goss_system_get_field_states": (C.c_int, [_sys, _dp, C.c_int32]),
+    "goss_system_set_field_states": (C.c_int, [_sys, _dp, C.c_int32]),
+    "goss_system_get_field_state_components": (C.c_int, [_sys, _dp, C.c_uint32, _u32p, C.c_int32]),
+    "goss_system_set_field_state_components": (C.c_int, [_sys, _dp, C.c_uint32, _u32p, C.c_int32]),
+    "goss_system_get_field_parameters": (C.c_int, [_sys, _dp, C.c_int32]),
+    "goss_system_set_field_parameters": (C.c_int, [_sys, _dp, C.c_int32]),
+    "goss_system_get_states": (C.c_int, [_sys, _dp]),
+    "goss_system_set_states": (C.c_int, [_sys, _dp]),
+    "goss_system_set_parameter": (C.c_int, [_sys, C.c_uint32, C.c_double]),
+    "goss_system_get_parameter": (C.c_int, [_sys, C.c_uint32, _dp]),
+    "goss_system_reset_default": (C.c_int, [_sys]),
+    "goss_system_set_num_threads": (C.c_int, [_sys, C.c_uint32]),
+    "goss_system_get_num_threads": (C.c_uint32, [_sys]),
+    "goss_system_num_nodes": (C.c_uint32, [_sys]),
+    "goss_system_set_block_size": (C.c_int, [_sys, C.c_uint32]),
+    "goss_system_status": (C.c_int, [_sys, _u32p, C.c_int32]),
+    "goss_system_node_status": (C.c_int, [_sys, C.POINTER(C.c_uint8)]),
+    "goss_system_counters": (C.c_int, [_sys, _i64p, _i64p, _i64p]),
+    "goss_system_device_states": (C.c_int, [_sys, C.POINTER(_dp), C.POINTER(C.c_uint64)]),
+    "goss_system_device_field_params": (C.c_int, [_sys, C.POINTER(_dp), C.POINTER(C.c_uint64)]),
+    "goss_system_set_stream": (C.c_int, [_sys, C.c_void_p]),
+    "goss_lu_factorize": (C.c_int, [C.c_uint32, _dp]),
+    "goss_forward_backward_subst": (C.c_int, [C.c_uint32, _dp, _dp, _dp]),
+    "goss_model_eval": (C.c_int, [_desc, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, C.c_uint64, _dp, C.c_int32]),
+}
+
+#: every function the header declares (checked by the tests)
+EXPORTED = sorted(_PROTOS)
+
+_lib = None
+
+
+def lib():
+    """Load the runtime library once; raise if it is not built."""
+    global _lib
+    if _lib is None:
+        if not RUNTIME_SO.exists():
+            raise ExtensionMissingError(
+                f"{RUNTIME_SO} is missing; build it with goss_b200.build.build_runtime() "
+                "(python -c 'import __graft_entry__ as g; g.build()')")
+        try:
+            handle = C.CDLL(str(RUNTIME_SO))
+        except OSError as exc:
+            raise ExtensionMissingError(f"cannot load {RUNTIME_SO}: {exc}") from exc
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(handle, name)
+            f.restype = res
+            f.argtypes = args
+        if handle.goss_abi_version() != ABI_VERSION:
+            raise ExtensionMissingError("libgoss_b200.so was built for another ABI version")
+        _lib = handle
+    return _lib
+
+
+def check(rc: int, sys_handle=None) -> None:
+    """Raise the exception that corresponds to a status code."""
+    if rc == GOSS_OK:
+        return
+    L = lib()
+    msg = L.goss_system_last_error(sys_handle).decode() if sys_handle else ""
+    if not msg:
+        msg = L.goss_last_error().decode()
+    if rc == GOSS_ERR_ARGUMENT:
+        raise ValueError(msg)
+    raise GossError(rc, msg)
+
+
+def ptr(a):
+    """double* of a C-contiguous float64 numpy array."""
+    return a.ctypes.data_as(_dp)

@@ -1,0 +1,420 @@
+"""Emit model source for every target from one :class:`ModelIR`.
+
+Targets
+-------
+``emit_oracle_c``
+    Plain C functions used by the CPU restatement in ``oracle/``.
+``emit_goss_plugin``
+    A ``goss::ParameterizedODE`` subclass plus ``extern "C" create_<Name>()``,
+    the plugin shape of the reference generator (``python/goss/codegeneration.py:51-114``),
+    so the reference's own compiled solvers can run the model.
+``emit_device``
+    CUDA ``__device__`` functions templated on the arithmetic type ``T``
+    that the sm_100a solver kernels inline.
+
+All three print the same :class:`Program` objects with the same printer, so
+their arithmetic is identical operation for operation.
+"""
+from __future__ import annotations
+
+import json
+import re
+from typing import Dict, List, Sequence
+
+import sympy as sp
+
+from .ir import CONST, FIELD, STATE, TIME_CLS, Assign, ModelIR, Output, Program, count_ops
+from .odeparse import TIME
+from .printer import CPrinter, c_double
+
+_RESERVED = {
+    "auto", "break", "case", "char", "const", "continue", "default", "do", "double", "else", "enum",
+    "extern", "float", "for", "goto", "if", "inline", "int", "long", "register", "restrict", "return",
+    "short", "signed", "sizeof", "static", "struct", "switch", "typedef", "union", "unsigned", "void",
+    "volatile", "while", "bool", "class", "new", "delete", "this", "template", "typename", "namespace",
+    "operator", "private", "public", "protected", "virtual", "friend", "true", "false", "time",
+    "values", "states", "linear", "rhs", "monitored", "only_linear", "jac", "exp", "log", "sqrt", "pow",
+    "floor", "ceil", "fabs", "abs", "sin", "cos", "tan", "tanh", "fmax", "fmin", "std", "goss",
+}
+
+
+def cxx_name(name: str) -> str:
+    """Member/local name for the goss C++ class (gotran keeps plain names)."""
+    return name + "_" if name in _RESERVED else name
+
+
+def model_class_name(model_name: str) -> str:
+    # gotran capitalises the ODE name (codegeneration.py:297)
+    return model_name.capitalize()
+
+
+def c_ident(model_name: str) -> str:
+    s = re.sub(r"[^0-9A-Za-z_]", "_", model_name)
+    if s[0].isdigit():
+        s = "m_" + s
+    return s
+
+
+# ---------------------------------------------------------------------------
+# helpers shared by the C-like targets
+# ---------------------------------------------------------------------------
+
+def _body_lines(prog: Program, pr_for, decl_for, out_for, split_code: List[str] = None) -> List[str]:
+    lines: List[str] = []
+    for idx, b in enumerate(prog.body):
+        if prog.split is not None and idx == prog.split and split_code:
+            lines.extend(split_code)
+        if isinstance(b, Assign):
+            lines.append(f"{decl_for(b)} = {pr_for(b.cls)(b.expr)};")
+        else:
+            lines.append(f"{out_for(b)} = {pr_for(STATE)(b.expr)};")
+    if prog.split is not None and prog.split == len(prog.body) and split_code:
+        lines.extend(split_code)
+    return lines
+
+
+class ModelSource:
+    """Bundle of everything generated for one model + field-parameter set."""
+
+    def __init__(self, ir: ModelIR, name: str = None):
+        self.ir = ir
+        self.model = ir.model
+        self.name = name or self.model.name
+        self.ident = c_ident(self.name)
+        self.rhs = ir.rhs_program()
+        self.lin = ir.linearized_program(split=True)
+        self.linear_terms = ir.linear_terms()
+        self.mon = ir.monitored_program() if ir.monitored else None
+        self.params = list(self.model.parameters)
+        self.states = list(self.model.states)
+        self.pindex = {p: i for i, p in enumerate(self.params)}
+        self.sindex = {s: i for i, s in enumerate(self.states)}
+        self.fparams = list(ir.field_parameters)
+        self.findex = {p: i for i, p in enumerate(self.fparams)}
+        self.inter_names = set(self.model.intermediates)
+
+    # -- metadata -----------------------------------------------------------
+    def metadata(self) -> Dict:
+        return dict(
+            name=self.name,
+            ident=self.ident,
+            class_name=model_class_name(self.name),
+            state_names=self.states,
+            parameter_names=self.params,
+            initial_conditions=[float(v) for v in self.model.states.values()],
+            default_parameters=[float(v) for v in self.model.parameters.values()],
+            field_parameter_names=self.fparams,
+            field_parameter_indices=[self.pindex[p] for p in self.fparams],
+            field_state_names=list(self.ir.field_states),
+            field_state_indices=[self.sindex[s] for s in self.ir.field_states],
+            monitored_names=list(self.ir.monitored),
+            linear_terms=self.linear_terms,
+            intermediate_names=list(self.model.intermediates),
+            op_census=dict(rhs=count_ops(self.rhs), linearized=count_ops(self.ir.linearized_program(split=False))),
+        )
+
+    # =======================================================================
+    # C restatement (oracle)
+    # =======================================================================
+    def _c_printer(self) -> CPrinter:
+        def sym(s):
+            n = s.name
+            if s == TIME:
+                return "time"
+            if n in self.sindex:
+                return f"s_{n}"
+            if n in self.pindex:
+                return f"p_{n}"
+            return f"v_{n}"
+        return CPrinter(sym)
+
+    def _c_head(self) -> List[str]:
+        lines = [f"const double s_{s} = states[{i}];" for i, s in enumerate(self.states)]
+        lines += [f"const double p_{p} = params[{i}];" for i, p in enumerate(self.params)]
+        return lines
+
+    def emit_oracle_c(self) -> str:
+        pr = self._c_printer()
+        decl = lambda b: f"const double v_{b.name}"
+        out = lambda b: f"{b.array}[{b.index}]"
+        m = self.ident
+        L = []
+        L.append(f"/* Generated by goss_b200.codegen from the '{self.name}' model; do not edit. */")
+        L.append("/* Test infrastructure: C restatement of the model consumed by the oracle. */")
+        L.append("#include <math.h>")
+        L.append('#include "goss_oracle.h"')
+        L.append("")
+        L.append("#if defined(__GNUC__)")
+        L.append('#pragma GCC diagnostic ignored "-Wunused-variable"')
+        L.append('#pragma GCC diagnostic ignored "-Wunused-parameter"')
+        L.append("#endif")
+        L.append("")
+        L.append(f"static void {m}_rhs(const double* states, double time, const double* params, double* values)")
+        L.append("{")
+        L += ["  " + x for x in self._c_head()]
+        L += ["  " + x for x in _body_lines(self.rhs, lambda c: pr, decl, out)]
+        L.append("}")
+        L.append("")
+        L.append(f"static void {m}_linearized(const double* states, double time, const double* params,")
+        L.append("    double* linear, double* rhs, int only_linear)")
+        L.append("{")
+        L += ["  " + x for x in self._c_head()]
+        L += ["  " + x for x in _body_lines(self.lin, lambda c: pr, decl, out,
+                                             split_code=["if (only_linear) return;"])]
+        L.append("}")
+        L.append("")
+        if self.mon is not None:
+            L.append(f"static void {m}_monitored(const double* states, double time, const double* params, double* monitored)")
+            L.append("{")
+            L += ["  " + x for x in self._c_head()]
+            L += ["  " + x for x in _body_lines(self.mon, lambda c: pr, decl, out)]
+            L.append("}")
+            L.append("")
+        ns, npar = len(self.states), len(self.params)
+        L.append(f"static const double {m}_ic[{ns}] = {{" + ", ".join(c_double(v) for v in self.model.states.values()) + "};")
+        L.append(f"static const double {m}_defaults[{npar}] = {{" + ", ".join(c_double(v) for v in self.model.parameters.values()) + "};" if npar else f"static const double {m}_defaults[1] = {{0.0}};")
+        lt = self.linear_terms
+        L.append(f"static const unsigned char {m}_linear_terms[{ns}] = {{" + ", ".join(str(v) for v in lt) + "};")
+        nfp = len(self.fparams)
+        fidx = [self.pindex[p] for p in self.fparams] or [0]
+        L.append(f"static const unsigned {m}_field_param_index[{max(nfp,1)}] = {{" + ", ".join(str(v) for v in fidx) + "};")
+        L.append("")
+        L.append(f"const oracle_model* oracle_model_{m}(void)")
+        L.append("{")
+        L.append("  static oracle_model model;")
+        L.append(f"  model.name = \"{self.name}\";")
+        L.append(f"  model.num_states = {ns};")
+        L.append(f"  model.num_params = {npar};")
+        L.append(f"  model.num_field_params = {nfp};")
+        L.append(f"  model.field_param_index = {m}_field_param_index;")
+        L.append(f"  model.rhs = {m}_rhs;")
+        L.append(f"  model.linearized = {m}_linearized;")
+        L.append(f"  model.ic = {m}_ic;")
+        L.append(f"  model.default_params = {m}_defaults;")
+        L.append(f"  model.linear_terms = {m}_linear_terms;")
+        L.append("  return &model;")
+        L.append("}")
+        return "\n".join(L) + "\n"
+
+    # =======================================================================
+    # goss C++ plugin (runs inside the reference's compiled solvers)
+    # =======================================================================
+    def emit_goss_plugin(self) -> str:
+        cls = model_class_name(self.name)
+        def sym(s):
+            if s == TIME:
+                return "time"
+            return cxx_name(s.name)
+        pr = CPrinter(sym, fn=dict(exp="std::exp", log="std::log", sqrt="std::sqrt", fabs="std::fabs",
+                                   floor="std::floor", ceil="std::ceil", pow="std::pow", fmax="std::fmax",
+                                   fmin="std::fmin", sin="std::sin", cos="std::cos", tan="std::tan",
+                                   tanh="std::tanh"))
+        decl = lambda b: f"const double {cxx_name(b.name)}"
+        out = lambda b: f"{b.array}[{b.index}]"
+        head = [f"const double {cxx_name(s)} = states[{i}];" for i, s in enumerate(self.states)]
+        ns, npar = len(self.states), len(self.params)
+        nfs, nfp, nmon = len(self.ir.field_states), len(self.fparams), len(self.ir.monitored)
+        I = lambda n: " " * n
+        L = []
+        guard = self.ident.upper() + "_GOSS_PLUGIN_H"
+        L.append(f"// Generated by goss_b200.codegen from the '{self.name}' model; do not edit.")
+        L.append("// goss::ParameterizedODE plugin consumed by the oracle build of the reference solvers.")
+        L.append(f"#ifndef {guard}")
+        L.append(f"#define {guard}")
+        L.append("#include <cmath>")
+        L.append("#include <memory>")
+        L.append("#include <stdexcept>")
+        L.append('#include "goss/ParameterizedODE.h"')
+        L.append("")
+        L.append("namespace goss {")
+        L.append(f"class {cls} : public ParameterizedODE")
+        L.append("{")
+        L.append("  public:")
+        init = ", ".join(f"{cxx_name(p)}({c_double(v)})" for p, v in self.model.parameters.items())
+        L.append(f"    {cls}() : ParameterizedODE({ns}, {npar}, {nfs}, {nfp}, {nmon})" + (f", {init}" if init else ""))
+        L.append("    {")
+        for i, s in enumerate(self.states):
+            L.append(f'        _state_names[{i}] = "{s}";')
+        for i, p in enumerate(self.params):
+            L.append(f'        _parameter_names[{i}] = "{p}";')
+        for i, s in enumerate(self.ir.field_states):
+            L.append(f'        _field_state_names[{i}] = "{s}";')
+            L.append(f"        _field_state_indices[{i}] = {self.sindex[s]};")
+        for i, p in enumerate(self.fparams):
+            L.append(f'        _field_parameter_names[{i}] = "{p}";')
+        for i, mname in enumerate(self.ir.monitored):
+            L.append(f'        _monitored_names[{i}] = "{mname}";')
+        for p in self.params:
+            L.append(f'        _param_to_value["{p}"] = &{cxx_name(p)};')
+        for i, f in enumerate(self.linear_terms):
+            if f:
+                L.append(f"        _linear_terms[{i}] = 1;")
+        L.append("    }")
+        cinit = ", ".join(f"{cxx_name(p)}(ode.{cxx_name(p)})" for p in self.params)
+        L.append(f"    {cls}(const {cls}& ode) : ParameterizedODE(ode)" + (f", {cinit}" if cinit else "") + " {}")
+        L.append("")
+        L.append("    void eval(const double* states, double time, double* values)")
+        L.append("    {")
+        L += [I(8) + x for x in head + _body_lines(self.rhs, lambda c: pr, decl, out)]
+        L.append("    }")
+        L.append("")
+        L.append("    void linearized_eval(const double* states, double time, double* linear, double* rhs,")
+        L.append("                         bool only_linear) const")
+        L.append("    {")
+        L += [I(8) + x for x in head + _body_lines(self.lin, lambda c: pr, decl, out,
+                                                  split_code=["if (only_linear) return;"])]
+        L.append("    }")
+        L.append("")
+        L.append("    void get_ic(goss::DoubleVector* values) const")
+        L.append("    {")
+        L.append("        values->n = _num_states;")
+        L.append("        values->data.reset(new double[_num_states]);")
+        for i, v in enumerate(self.model.states.values()):
+            L.append(f"        values->data[{i}] = {c_double(v)};")
+        L.append("    }")
+        L.append("")
+        L.append("    std::shared_ptr<ODE> copy() const { return std::make_shared<" + cls + ">(*this); }")
+        L.append("")
+        L.append("    void eval_monitored(const double* states, double time, double* monitored) const")
+        L.append("    {")
+        if self.mon is None:
+            L.append(f'        throw std::runtime_error("No monitored in the \\\'{cls}\\\' model.");')
+        else:
+            L += [I(8) + x for x in head + _body_lines(self.mon, lambda c: pr, decl, out)]
+        L.append("    }")
+        L.append("")
+        L.append("    void set_field_parameters(const double* field_params)")
+        L.append("    {")
+        for i, p in enumerate(self.fparams):
+            L.append(f"        {cxx_name(p)} = field_params[{i}];")
+        if not self.fparams:
+            L.append("        (void)field_params;")
+        L.append("    }")
+        L.append("")
+        L.append("  private:")
+        if self.params:
+            L.append("    double " + ", ".join(cxx_name(p) for p in self.params) + ";")
+        L.append("};")
+        L.append("}  // namespace goss")
+        L.append("")
+        L.append(f'extern "C" __attribute__((visibility("default"))) goss::ParameterizedODE* create_{cls}()')
+        L.append("{")
+        L.append(f"    return new goss::{cls};")
+        L.append("}")
+        L.append("#endif")
+        return "\n".join(L) + "\n"
+
+    # =======================================================================
+    # CUDA device code
+    # =======================================================================
+    def _dev_printers(self):
+        """Printers for arithmetic type T and for double (time-only) context."""
+        def make(ctx_double: bool):
+            def sym(s):
+                n = s.name
+                if s == TIME:
+                    return "time" if ctx_double else "T(time)"
+                if n in self.sindex:
+                    return f"s_{n}"
+                if n in self.pindex:
+                    if n in self.findex:
+                        j = self.findex[n]
+                        return f"double(F[{j}])" if ctx_double else f"F[{j}]"
+                    k = self.pindex[n]
+                    return f"PD[{k}]" if ctx_double else f"P[{k}]"
+                # intermediate: its declared type follows its class
+                cls = self._cls_of(n)
+                if cls == TIME_CLS and not ctx_double:
+                    return f"T(v_{n})"
+                return f"v_{n}"
+            if ctx_double:
+                fn = dict(exp="exp", log="log", sqrt="sqrt", fabs="fabs", floor="floor", ceil="ceil",
+                          pow="pow", fmax="fmax", fmin="fmin")
+                lit = c_double
+            else:
+                fn = dict(exp="gexp", log="glog", sqrt="gsqrt", fabs="gfabs", floor="gfloor", ceil="gceil",
+                          pow="gpow", fmax="gfmax", fmin="gfmin", sin="gsin", cos="gcos", tan="gtan",
+                          tanh="gtanh")
+                lit = lambda v: f"T({c_double(v)})"
+            return CPrinter(sym, fn=fn, lit=lit)
+        return make(False), make(True)
+
+    def _cls_of(self, name: str) -> int:
+        return self._cls_map.get(name, STATE)
+
+    @property
+    def _cls_map(self) -> Dict[str, int]:
+        if not hasattr(self, "_cls_cache"):
+            d = {}
+            for prog in (self.rhs, self.lin) + ((self.mon,) if self.mon else ()):
+                for b in prog.assigns():
+                    d[b.name] = b.cls
+            self._cls_cache = d
+        return self._cls_cache
+
+    def _dev_body(self, prog: Program) -> List[str]:
+        prT, prD = self._dev_printers()
+        def pr_for(cls):
+            return prD if cls == TIME_CLS else prT
+        def decl(b):
+            t = "double" if b.cls == TIME_CLS else "T"
+            return f"const {t} v_{b.name}"
+        out = lambda b: f"{b.array}[{b.index}]"
+        p2 = Program(prog.name, prog.body, None)
+        return _body_lines(p2, pr_for, decl, out)
+
+    def emit_device(self) -> str:
+        cls = model_class_name(self.name)
+        ns, npar, nfp = len(self.states), len(self.params), len(self.fparams)
+        L = []
+        guard = self.ident.upper() + "_DEVICE_CUH"
+        L.append(f"// Generated by goss_b200.codegen from the '{self.name}' model; do not edit.")
+        L.append("// Device-side model: rhs and linearised rhs templated on the arithmetic type T.")
+        L.append(f"#ifndef {guard}")
+        L.append(f"#define {guard}")
+        L.append('#include "goss_device_math.cuh"')
+        L.append("")
+        L.append("namespace goss_b200 { namespace models {")
+        L.append("")
+        L.append(f"struct {cls} {{")
+        L.append(f'  static constexpr const char* name = "{self.name}";')
+        L.append(f"  static constexpr int num_states = {ns};")
+        L.append(f"  static constexpr int num_params = {npar};")
+        L.append(f"  static constexpr int num_field_params = {nfp};")
+        L.append(f"  static constexpr int num_monitored = {len(self.ir.monitored)};")
+        L.append("")
+        head = [f"const T s_{s} = y[{i}];" for i, s in enumerate(self.states)]
+        sig = ("const T* __restrict__ y, const double time, const T* __restrict__ P, "
+               "const double* __restrict__ PD, const T* __restrict__ F")
+        L.append("  // values = f(y, time)")
+        L.append("  template <typename T>")
+        L.append(f"  __device__ static __forceinline__ void rhs({sig}, T* __restrict__ values)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_body(self.rhs)]
+        L.append("    (void)time; (void)P; (void)PD; (void)F;")
+        L.append("  }")
+        L.append("")
+        lin_full = self.ir.linearized_program(split=False)
+        L.append("  // rhs = f(y, time), linear[i] = d f_i / d y_i")
+        L.append("  template <typename T>")
+        L.append(f"  __device__ static __forceinline__ void linearized({sig}, T* __restrict__ linear, T* __restrict__ rhs)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_body(lin_full)]
+        L.append("    (void)time; (void)P; (void)PD; (void)F;")
+        L.append("  }")
+        if self.mon is not None:
+            L.append("")
+            L.append("  template <typename T>")
+            L.append(f"  __device__ static __forceinline__ void monitored_values({sig}, T* __restrict__ monitored)")
+            L.append("  {")
+            L += ["    " + x for x in head + self._dev_body(self.mon)]
+            L.append("    (void)time; (void)P; (void)PD; (void)F;")
+            L.append("  }")
+        L.append("};")
+        L.append("")
+        L.append("}}  // namespace goss_b200::models")
+        L.append("#endif")
+        return "\n".join(L) + "\n"
+
+    def metadata_json(self) -> str:
+        return json.dumps(self.metadata(), indent=1)

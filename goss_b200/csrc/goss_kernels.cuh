@@ -1,0 +1,907 @@
+// sm_100a solver kernels of the multi-node solve path.
+//
+// One CUDA thread owns one mesh node for the whole call: its states are
+// loaded once from the component-major FP64 arrays (states[i*ld + node],
+// coalesced across the warp), kept in registers across every internal step
+// of the interval, and stored once at the end.  Uniform model parameters
+// travel in the kernel's parameter block (constant bank, read as free
+// operands); per-node field parameters are loaded once into registers.
+//
+// Each kernel restates the arithmetic of one reference solver; the FP64
+// instantiation follows the reference operation order so that it agrees with
+// the FP64 CPU oracle to rounding.
+//
+//   explicit_kernel<M, T, ExplicitEuler>  cpp/goss/ExplicitEuler.cpp:64-87
+//   explicit_kernel<M, T, RK4>            cpp/goss/RK4.cpp:68-102
+//   explicit_kernel<M, T, GRL1>           cpp/goss/GRL1.cpp:61-82, GRL1.h:72-84
+//   explicit_kernel<M, T, GRL2>           cpp/goss/GRL2.cpp:63-86
+//   theta_kernel<M>                       cpp/goss/ThetaSolver.cpp:49-155,
+//                                         ImplicitODESolver.cpp:92-262, ODE.cpp:47-132
+//   esdirk_kernel<M>                      cpp/goss/ESDIRK23a.cpp:101-316
+#ifndef GOSS_KERNELS_CUH
+#define GOSS_KERNELS_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "goss_b200.h"
+#include "goss_device_math.cuh"
+
+namespace goss_b200 {
+
+constexpr double kGossEps = 3.0e-16;  // GOSS_EPS, cpp/goss/constants.h:25
+
+template <class M>
+struct Dims {
+    static constexpr int n = M::num_states;
+    static constexpr int np = M::num_params > 0 ? M::num_params : 1;
+    static constexpr int nfp = M::num_field_params > 0 ? M::num_field_params : 1;
+};
+
+// std::max / std::min semantics (first argument wins ties and NaNs)
+__device__ __forceinline__ double std_max(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double std_min(double a, double b) { return (b < a) ? b : a; }
+
+// ---------------------------------------------------------------------------
+// kernel argument blocks (passed by value; __grid_constant__ keeps them in the
+// parameter bank so indexing them costs no local-memory copy)
+// ---------------------------------------------------------------------------
+template <class M, typename T>
+struct ExplicitArgs {
+    double* states;
+    const double* fparams;
+    uint32_t* flags;
+    uint8_t* node_status;
+    uint64_t ld;
+    uint64_t nsteps;
+    double t;
+    double ldt;
+    double delta;
+    uint32_t N;
+    T P[Dims<M>::np];
+    double PD[Dims<M>::np];
+};
+
+template <class M>
+struct ImplicitArgs {
+    double* states;
+    const double* fparams;
+    double* sstate;  // per-node solver state, [rows][ld]
+    uint32_t* flags;
+    uint8_t* node_status;
+    uint64_t ld;
+    uint64_t max_loop;
+    double t;
+    double interval;
+    goss_solver_params sp;
+    uint32_t N;
+    double P[Dims<M>::np];
+};
+
+template <class M, typename T>
+struct EvalArgs {
+    const double* states;
+    const double* fparams;
+    const double* times;
+    double* out;
+    uint64_t ld;
+    uint32_t N;
+    int32_t what;
+    T P[Dims<M>::np];
+    double PD[Dims<M>::np];
+};
+
+// ---------------------------------------------------------------------------
+// explicit solvers
+// ---------------------------------------------------------------------------
+enum class Explicit { Euler, RK4, GRL1, GRL2 };
+
+template <class M, typename T>
+__device__ __forceinline__ void load_field(const double* __restrict__ fp, uint64_t ld, uint32_t node,
+                                           T (&F)[Dims<M>::nfp])
+{
+#pragma unroll
+    for (int k = 0; k < Dims<M>::nfp; ++k)
+        F[k] = (k < M::num_field_params) ? T(fp[k * ld + node]) : T(0);
+}
+
+// GRL increment of one state, FP64: the reference expression
+// b/a*(exp(a*h) - 1.0) or b*h (GRL1.h:80-83)
+__device__ __forceinline__ double grl_increment(double a, double b, double h, double delta)
+{
+    return (fabs(a) > delta) ? b / a * (exp(a * h) - 1.0) : b * h;
+}
+
+// GRL increment of one state, FP32: b*h*phi1(a*h), algebraically identical
+// and free of the cancellation in exp(a*h) - 1 (see phi1f)
+__device__ __forceinline__ float grl_increment(float a, float b, float h, float /*delta*/)
+{
+    return b * h * phi1f(a * h);
+}
+
+template <class M, typename T, Explicit S>
+__global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ ExplicitArgs<M, T> a)
+{
+    constexpr int n = M::num_states;
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= a.N)
+        return;
+    double y[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+        y[i] = a.states[i * a.ld + node];
+    T F[Dims<M>::nfp];
+    load_field<M, T>(a.fparams, a.ld, node, F);
+
+    const double ldt = a.ldt;
+    const T h = T(ldt);
+    const T delta = T(a.delta);
+    double lt = a.t;
+    for (uint64_t step = 0; step < a.nsteps; ++step) {
+        T yt[n];
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            yt[i] = T(y[i]);
+        if constexpr (S == Explicit::Euler) {
+            T f[n];
+            M::template rhs<T>(yt, lt, a.P, a.PD, F, f);
+#pragma unroll
+            for (int i = 0; i < n; ++i)
+                y[i] += ldt * double(f[i]);
+        } else if constexpr (S == Explicit::RK4) {
+            // RK4.cpp:79-98 with RK4::axpy (RK4.h:70-74).  Stage inputs are
+            // formed in FP64 (y + a*k) and rounded to T; the weighted sum is
+            // accumulated in the order k1 + 2 k2 + 2 k3 + k4 of the reference.
+            const double hh = 0.5 * ldt;
+            T k[n], sum[n], tmp[n];
+            M::template rhs<T>(yt, lt, a.P, a.PD, F, k);
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                sum[i] = k[i];
+                tmp[i] = T(y[i] + hh * double(k[i]));
+            }
+            M::template rhs<T>(tmp, lt + 0.5 * ldt, a.P, a.PD, F, k);
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                sum[i] = sum[i] + T(2.0) * k[i];
+                tmp[i] = T(y[i] + hh * double(k[i]));
+            }
+            M::template rhs<T>(tmp, lt + 0.5 * ldt, a.P, a.PD, F, k);
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                sum[i] = sum[i] + T(2.0) * k[i];
+                tmp[i] = T(y[i] + ldt * double(k[i]));
+            }
+            M::template rhs<T>(tmp, lt + ldt, a.P, a.PD, F, k);
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                sum[i] = sum[i] + k[i];
+                y[i] += ldt * double(sum[i]) / 6.0;
+            }
+        } else if constexpr (S == Explicit::GRL1) {
+            T lin[n], rhs[n];
+            M::template linearized<T>(yt, lt, a.P, a.PD, F, lin, rhs);
+#pragma unroll
+            for (int i = 0; i < n; ++i)
+                y[i] = y[i] + double(grl_increment(lin[i], rhs[i], h, delta));
+        } else {
+            // GRL2: GRL2.cpp:78-82.  The reference's branch threshold is a
+            // self-initialised local (GRL2.cpp:67) whose -O3 build behaves as 0:
+            // the exponential form is used whenever the linear term is non-zero.
+            T lin[n], rhs[n], y2[n];
+            M::template linearized<T>(yt, lt, a.P, a.PD, F, lin, rhs);
+#pragma unroll
+            for (int i = 0; i < n; ++i) {
+                if constexpr (sizeof(T) == 8)
+                    y2[i] = y[i] + grl_increment(double(lin[i]), double(rhs[i]), ldt * 0.5, 0.0);
+                else
+                    y2[i] = T(y[i] + double(grl_increment(lin[i], rhs[i], T(ldt * 0.5), T(0))));
+            }
+            M::template linearized<T>(y2, lt, a.P, a.PD, F, lin, rhs);
+#pragma unroll
+            for (int i = 0; i < n; ++i)
+                y[i] = y[i] + double(grl_increment(lin[i], rhs[i], h, T(0)));
+        }
+        lt += ldt;
+    }
+    bool finite = true;
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+        a.states[i * a.ld + node] = y[i];
+        finite = finite && isfinite(y[i]);
+    }
+    if (!finite) {
+        a.node_status[node] |= GOSS_FLAG_NONFINITE;
+        atomicOr(a.flags, GOSS_FLAG_NONFINITE);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dense linear algebra on one node's n x n matrix
+// ---------------------------------------------------------------------------
+// Matrix accessors: thread-local array or a node's slice of a component-major
+// global array (element (r, c) of node at base[(r*n + c)*ld + node]).
+template <int n>
+struct LocalMat {
+    double* m;
+    __device__ __forceinline__ double& operator()(int r, int c) const { return m[r * n + c]; }
+};
+template <int n>
+struct GlobalMat {
+    double* base;
+    uint64_t ld;
+    __device__ __forceinline__ double& operator()(int r, int c) const { return base[(uint64_t)(r * n + c) * ld]; }
+};
+
+// ODE::lu_factorize (ODE.cpp:69-100): Doolittle, no pivoting
+template <int n, class Mat>
+__device__ void lu_factorize(const Mat& A)
+{
+    for (int k = 1; k < n; k++) {
+        for (int i = 0; i <= k - 1; ++i) {
+            double sum = 0.0;
+            for (int r = 0; r <= i - 1; r++)
+                sum += A(i, r) * A(r, k);
+            A(i, k) -= sum;
+            sum = 0.0;
+            for (int r = 0; r <= i - 1; r++)
+                sum += A(k, r) * A(r, i);
+            A(k, i) = (A(k, i) - sum) / A(i, i);
+        }
+        double sum = 0.0;
+        for (int r = 0; r <= k - 1; r++)
+            sum += A(k, r) * A(r, k);
+        A(k, k) -= sum;
+    }
+}
+
+// ODE::forward_backward_subst (ODE.cpp:102-132); b and dx may alias
+template <int n, class Mat>
+__device__ void forward_backward_subst(const Mat& A, const double* b, double* dx)
+{
+    dx[0] = b[0];
+    for (int i = 1; i < n; ++i) {
+        double sum = 0.0;
+        for (int j = 0; j <= i - 1; ++j)
+            sum = sum + A(i, j) * dx[j];
+        dx[i] = b[i] - sum;
+    }
+    dx[n - 1] = dx[n - 1] / A(n - 1, n - 1);
+    for (int i = n - 2; i >= 0; i--) {
+        double sum = 0;
+        for (int j = i + 1; j < n; ++j)
+            sum = sum + A(i, j) * dx[j];
+        dx[i] = (dx[i] - sum) / A(i, i);
+    }
+}
+
+template <int n>
+__device__ __forceinline__ double l2norm(const double* v)
+{
+    double s = 0;
+    for (int i = 0; i < n; ++i)
+        s += v[i] * v[i];
+    return sqrt(s);
+}
+
+// FP64 model right-hand side with the per-node parameter block
+template <class M>
+__device__ __forceinline__ void rhs64(const double* y, double t, const double* P, const double* F, double* out)
+{
+    M::template rhs<double>(y, t, P, P, F, out);
+}
+
+// ODE::compute_jacobian (ODE.cpp:47-67) into any matrix accessor
+template <class M, class Mat>
+__device__ void compute_jacobian(double* y, double t, const double* P, const double* F, const Mat& J, double* f1,
+                                 double* f2)
+{
+    constexpr int n = M::num_states;
+    rhs64<M>(y, t, P, F, f1);
+    for (int i = 0; i < n; ++i) {
+        const double ysafe = y[i];
+        const double max = 1e-5 > fabs(ysafe) ? 1e-5 : fabs(ysafe);
+        const double delta = sqrt(1e-15 * max);
+        y[i] += delta;
+        rhs64<M>(y, t, P, F, f2);
+        for (int j = 0; j < n; ++j)
+            J(j, i) = (f2[j] - f1[j]) / delta;
+        y[i] = ysafe;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ThetaSolver
+// ---------------------------------------------------------------------------
+// per-node solver state rows
+enum ThetaRows { TH_ETA = 0, TH_RECOMPUTE, TH_ALWAYS, TH_JUSTREFINED, TH_JACCOMP, TH_REJECTS, TH_ACCEPTED, TH_ROWS };
+
+template <class M>
+__global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ ImplicitArgs<M> a)
+{
+    constexpr int n = M::num_states;
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= a.N)
+        return;
+    const goss_solver_params& sp = a.sp;
+    double y[n], z1[n], prev[n], ft1[n], yz[n], f1[n], b[n], dz[n], g1[n], g2[n];
+    double Jm[n * n];
+    const LocalMat<n> J{Jm};
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+        y[i] = a.states[i * a.ld + node];
+    double F[Dims<M>::nfp];
+    load_field<M, double>(a.fparams, a.ld, node, F);
+    double* ss = a.sstate + node;
+    const uint64_t ld = a.ld;
+    double eta = ss[TH_ETA * ld];
+    int recompute = ss[TH_RECOMPUTE * ld] != 0.0;
+    int always = ss[TH_ALWAYS * ld] != 0.0;
+    int justrefined = ss[TH_JUSTREFINED * ld] != 0.0;
+    double jac_comp = ss[TH_JACCOMP * ld], rejects = ss[TH_REJECTS * ld], accepted = ss[TH_ACCEPTED * ld];
+
+    double t = a.t;
+    const double dt = a.interval;
+    const double t_end = t + dt;
+    const double ldt_0 = sp.ldt;
+    double ldt = ldt_0 > 0 ? ldt_0 : dt;
+    int num_refinements = 0;
+    const double eps = kGossEps * 1000;
+    uint8_t status = 0;
+    for (int i = 0; i < n; ++i)
+        prev[i] = 0.0;
+    uint64_t guard = 0;
+    while (true) {
+        if (++guard > a.max_loop) {
+            status |= GOSS_FLAG_ITERATION_CAP;
+            break;
+        }
+        for (int i = 0; i < n; ++i)
+            z1[i] = 0.0;
+        if (fabs(sp.theta - 1.0) > kGossEps) {
+            rhs64<M>(y, t, a.P, F, ft1);
+            for (int i = 0; i < n; ++i)
+                prev[i] = (1 - sp.theta) * ft1[i];
+        }
+        if (num_refinements <= sp.num_refinements_without_always_recomputing_jacobian)
+            always = 1;
+        // ImplicitODESolver::newton_solve (ImplicitODESolver.cpp:114-245)
+        const double tn = t + sp.theta * ldt;
+        const double alpha = sp.theta;
+        bool step_ok = true;
+        int newton_iterations = 0;
+        double relative_previous_residual = 1.0, relative_residual = 1.0, previous_residual = 1.0;
+        double initial_residual = 1.0, residual;
+        do {
+            for (int i = 0; i < n; ++i)
+                yz[i] = y[i] + z1[i];
+            rhs64<M>(yz, tn, a.P, F, f1);
+            for (int i = 0; i < n; ++i)
+                b[i] = -z1[i] * 1.0 + ldt * (prev[i] + alpha * f1[i]);
+            residual = l2norm<n>(b);
+            if (relative_residual < sp.relative_tolerance)
+                break;
+            if (recompute || always) {
+                // compute_factorized_jacobian (ImplicitODESolver.cpp:92-105)
+                compute_jacobian<M>(yz, tn, a.P, F, J, g1, g2);
+                const double scale = -ldt * alpha;
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < n; ++j)
+                        J(i, j) *= scale;
+                for (int i = 0; i < n; ++i)
+                    J(i, i) += 1.0 * 1.0;
+                lu_factorize<n>(J);
+                jac_comp += 1;
+                recompute = 0;
+            }
+            forward_backward_subst<n>(J, b, dz);
+            if (newton_iterations == 0) {
+                initial_residual = residual;
+                eta = eta > kGossEps ? eta : kGossEps;
+                eta = pow(eta, 0.8);
+            } else {
+                relative_previous_residual = residual / previous_residual;
+                recompute = relative_previous_residual >= sp.max_relative_previous_residual;
+                if (relative_previous_residual >= 1) {
+                    step_ok = false;
+                    rejects += 1;
+                    recompute = 1;
+                    break;
+                }
+                const double scaled = std_max(
+                    pow(relative_previous_residual, (double)(sp.max_iterations - newton_iterations)), kGossEps);
+                if (residual > (sp.kappa * sp.relative_tolerance * (1 - relative_previous_residual) / scaled))
+                    recompute = 1;
+                eta = relative_previous_residual / (1.0 - relative_previous_residual);
+            }
+            if (newton_iterations > sp.max_iterations) {
+                recompute = 1;
+                rejects += 1;
+                step_ok = false;
+                break;
+            }
+            for (int i = 0; i < n; ++i)
+                z1[i] += dz[i];
+            relative_residual = residual / initial_residual;
+            previous_residual = residual;
+            newton_iterations++;
+        } while (eta * relative_residual >= sp.kappa * sp.relative_tolerance);
+
+        if (step_ok) {
+            for (int i = 0; i < n; ++i)
+                y[i] += z1[i];
+            t += ldt;
+            accepted += 1;
+            if (fabs(t - t_end) < eps)
+                break;
+            if (!justrefined) {
+                const double tmp = 2.0 * ldt;
+                if (ldt_0 > 0. && tmp >= ldt_0)
+                    ldt = ldt_0;
+                else
+                    ldt = tmp;
+            } else {
+                justrefined = 0;
+            }
+            if ((t + ldt + kGossEps) > t_end)
+                ldt = t_end - t;
+        } else {
+            ldt /= 2.0;
+            if (ldt < sp.min_dt) {
+                status |= GOSS_FLAG_NEWTON_FAILED;
+                break;
+            }
+            justrefined = 1;
+            num_refinements += 1;
+        }
+    }
+    bool finite = true;
+    for (int i = 0; i < n; ++i) {
+        a.states[i * a.ld + node] = y[i];
+        finite = finite && isfinite(y[i]);
+    }
+    if (!finite)
+        status |= GOSS_FLAG_NONFINITE;
+    ss[TH_ETA * ld] = eta;
+    ss[TH_RECOMPUTE * ld] = recompute;
+    ss[TH_ALWAYS * ld] = always;
+    ss[TH_JUSTREFINED * ld] = justrefined;
+    ss[TH_JACCOMP * ld] = jac_comp;
+    ss[TH_REJECTS * ld] = rejects;
+    ss[TH_ACCEPTED * ld] = accepted;
+    if (status) {
+        a.node_status[node] |= status;
+        atomicOr(a.flags, (uint32_t)status);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ESDIRK23a
+// ---------------------------------------------------------------------------
+enum EsdirkRows {
+    ES_PREV_DT = 0, ES_LOC_ERROR, ES_ETA, ES_NEWTON_IT, ES_FIRST, ES_NEWJAC, ES_JACCOMP, ES_REJECTS, ES_ACCEPTED,
+    ES_SCALARS  // jac[n*n] and jfac[n*n] follow
+};
+
+struct EsdirkCoef {
+    double gamma, a21, a22, a31, a32, a33, a41, a42, a43, a44, b1, b2, b3, b4, bh1, bh2, bh3, c2, c3, c4;
+    double s_fac, tol, etamin, kappa;
+};
+
+// ESDIRK23a constructor (ESDIRK23a.cpp:27-39)
+__device__ __forceinline__ EsdirkCoef esdirk_coefficients()
+{
+    EsdirkCoef c;
+    const double gamma = 0.43586652150845899942;
+    c.gamma = gamma;
+    c.a21 = gamma;
+    c.a22 = gamma;
+    c.a31 = (-4 * gamma * gamma + 6 * gamma - 1) / (4 * gamma);
+    c.a32 = (-2 * gamma + 1) / (4 * gamma);
+    c.a33 = gamma;
+    c.a41 = (6 * gamma - 1) / (12 * gamma);
+    c.a42 = -1 / ((24 * gamma - 12) * gamma);
+    c.a43 = (-6 * gamma * gamma + 6 * gamma - 1) / (6 * gamma - 3);
+    c.a44 = gamma;
+    c.b1 = c.a41;
+    c.b2 = c.a42;
+    c.b3 = c.a43;
+    c.b4 = c.a44;
+    c.bh1 = c.a31;
+    c.bh2 = c.a32;
+    c.bh3 = c.a33;
+    c.c2 = 2.0 * gamma;
+    c.c3 = 1.0;
+    c.c4 = 1.0;
+    c.s_fac = 0.9;
+    c.tol = 1.0e-5;
+    c.etamin = 1.0e-10;
+    c.kappa = 1.0e-1;
+    return c;
+}
+
+template <class M>
+struct EsdirkNode {
+    static constexpr int n = M::num_states;
+    const double* P;
+    const double* F;
+    const goss_solver_params* sp;
+    EsdirkCoef c;
+    GlobalMat<n> jac, jfac;
+    double prev_dt, loc_error, eta, dt;
+    int newton_iterations, first_step, new_jacobian;
+    double jac_comp, rejects, accepted;
+    double z1[n], z2[n], z3[n], z4[n], prev[n], yh[n];
+    double y_int[n], z_int[n], b[n], dz[n], prev_dz[n], g1[n], g2[n];
+
+    // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
+    __device__ void ode_jacobian(double* y, double t)
+    {
+        compute_jacobian<M>(y, t, P, F, jac, g1, g2);
+        jac_comp += 1;
+        new_jacobian = 1;
+    }
+    // ESDIRK23a::compute_factorized_jacobian(dt) (ESDIRK23a.cpp:101-115)
+    __device__ void factorize(double h)
+    {
+        const double scale = -h * c.a22;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                jfac(i, j) = jac(i, j) * scale;
+        for (int i = 0; i < n; ++i)
+            jfac(i, i) += 1.0 * 1.0;
+        lu_factorize<n>(jfac);
+    }
+    // ESDIRK23a::compute_stage_val (ESDIRK23a.cpp:201-258)
+    __device__ bool stage(double* z, const double* y, double t_s, double h)
+    {
+        newton_iterations = 0;
+        bool conv_ok = true;
+        for (int i = 0; i < n; ++i)
+            dz[i] = 0.0, prev_dz[i] = 0.0;
+        eta = pow(std_max(eta, c.etamin), 0.8);
+        int guard = 0;
+        do {
+            for (int i = 0; i < n; i++)
+                y_int[i] = y[i] + h * prev[i] + c.gamma * h * z[i];
+            rhs64<M>(y_int, t_s, P, F, z_int);
+            for (int i = 0; i < n; i++)
+                b[i] = -z[i] + z_int[i];
+            for (int i = 0; i < n; i++)
+                prev_dz[i] = dz[i];
+            forward_backward_subst<n>(jfac, b, dz);
+            if (newton_iterations >= 1) {
+                const double theta = l2norm<n>(dz) / l2norm<n>(prev_dz);
+                if (!(theta <= 1)) {
+                    rejects += 1;
+                    conv_ok = false;
+                    break;
+                }
+                eta = theta / (1.0 - theta);
+            }
+            if (newton_iterations > sp->max_iterations || ++guard > 100000) {
+                rejects += 1;
+                conv_ok = false;
+                break;
+            }
+            for (int i = 0; i < n; i++)
+                z[i] += dz[i];
+            newton_iterations++;
+        } while (eta * l2norm<n>(dz) > c.kappa * c.tol);
+        return conv_ok;
+    }
+    // ESDIRK23a::do_step (ESDIRK23a.cpp:134-199)
+    __device__ bool do_step(double* y, double t0, double h)
+    {
+        rhs64<M>(y, t0, P, F, z1);
+        for (int i = 0; i < n; i++) {
+            z2[i] = z1[i];
+            prev[i] = z1[i] * c.a21;
+        }
+        bool step_ok = stage(z2, y, t0 + c.c2 * h, h);
+        if (step_ok) {
+            for (int i = 0; i < n; i++) {
+                z3[i] = z2[i];
+                prev[i] = z1[i] * c.bh1 + z2[i] * c.bh2;
+            }
+            step_ok = stage(z3, y, t0 + c.c3 * h, h);
+        }
+        if (step_ok) {
+            for (int i = 0; i < n; i++) {
+                z4[i] = z3[i];
+                prev[i] = z1[i] * c.b1 + z2[i] * c.b2 + z3[i] * c.b3;
+            }
+            step_ok = stage(z4, y, t0 + c.c4 * h, h);
+        }
+        if (step_ok) {
+            for (int i = 0; i < n; i++)
+                yh[i] = h * ((c.b1 - c.bh1) * z1[i] + (c.b2 - c.bh2) * z2[i] + (c.b3 - c.gamma) * z3[i] +
+                             c.gamma * z4[i]);
+            forward_backward_subst<n>(jfac, yh, yh);
+            loc_error = l2norm<n>(yh);
+            if (loc_error > c.tol) {
+                rejects += 1;
+                step_ok = false;
+            } else {
+                for (int i = 0; i < n; i++)
+                    y[i] = y[i] + h * (c.b1 * z1[i] + c.b2 * z2[i] + c.b3 * z3[i] + c.gamma * z4[i]);
+                accepted += 1;
+            }
+        }
+        return step_ok;
+    }
+    // ESDIRK23a::reduce_time_step (ESDIRK23a.cpp:260-278)
+    __device__ void reduce(double& h)
+    {
+        double reduction_factor = 1.0, e = loc_error;
+        int guard = 0;
+        do {
+            reduction_factor *= 0.6;
+            e *= 0.1;
+        } while (e > c.tol && ++guard < 4096);
+        h = std_max(reduction_factor * h, sp->min_dt);
+    }
+    // ESDIRK23a::advance_one_step (ESDIRK23a.cpp:117-132)
+    __device__ void advance(double* y, double t0, double& h)
+    {
+        bool ok = do_step(y, t0, h);
+        int guard = 0;
+        while (!ok && h > sp->min_dt && ++guard < 4096) {
+            if (!new_jacobian)
+                ode_jacobian(y, t0);
+            reduce(h);
+            factorize(h);
+            ok = do_step(y, t0, h);
+        }
+        new_jacobian = 0;
+    }
+};
+
+template <class M>
+__global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ ImplicitArgs<M> a)
+{
+    constexpr int n = M::num_states;
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= a.N)
+        return;
+    const uint64_t ld = a.ld;
+    double y[n];
+    for (int i = 0; i < n; ++i)
+        y[i] = a.states[i * ld + node];
+    double F[Dims<M>::nfp];
+    load_field<M, double>(a.fparams, ld, node, F);
+    double* ss = a.sstate + node;
+    EsdirkNode<M> s;
+    s.P = a.P;
+    s.F = F;
+    s.sp = &a.sp;
+    s.c = esdirk_coefficients();
+    s.jac = GlobalMat<n>{ss + (uint64_t)ES_SCALARS * ld, ld};
+    s.jfac = GlobalMat<n>{ss + (uint64_t)(ES_SCALARS + n * n) * ld, ld};
+    s.prev_dt = ss[ES_PREV_DT * ld];
+    s.loc_error = ss[ES_LOC_ERROR * ld];
+    s.eta = ss[ES_ETA * ld];
+    s.newton_iterations = (int)ss[ES_NEWTON_IT * ld];
+    s.first_step = ss[ES_FIRST * ld] != 0.0;
+    s.new_jacobian = ss[ES_NEWJAC * ld] != 0.0;
+    s.jac_comp = ss[ES_JACCOMP * ld];
+    s.rejects = ss[ES_REJECTS * ld];
+    s.accepted = ss[ES_ACCEPTED * ld];
+
+    // ESDIRK23a::forward (ESDIRK23a.cpp:280-316)
+    const double t0 = a.t, interval = a.interval;
+    const double min_dt = a.sp.min_dt;
+    double local_t = 0;
+    uint8_t status = 0;
+    double h = std_max(s.c.s_fac * s.prev_dt * pow((s.c.tol / s.loc_error), 0.25), min_dt);
+    h = std_min(h, interval);
+    if (s.first_step) {
+        s.prev_dt = h;
+        s.ode_jacobian(y, t0);
+    }
+    uint64_t guard = 0;
+    while (local_t < interval) {
+        if (++guard > a.max_loop) {
+            status |= GOSS_FLAG_ITERATION_CAP;
+            break;
+        }
+        if (h * 1.1 >= interval - local_t)
+            h = interval - local_t;
+        if (s.newton_iterations >= 2)
+            s.ode_jacobian(y, t0 + local_t);
+        if (fabs((h - s.prev_dt) / s.prev_dt) > 0.2 || s.new_jacobian)
+            s.factorize(h);
+        s.advance(y, t0 + local_t, h);
+        s.prev_dt = h;
+        local_t += h;
+        h = std_max(s.c.s_fac * s.prev_dt * pow((s.c.tol / s.loc_error), 0.25), min_dt);
+    }
+    s.first_step = 0;
+    bool finite = true;
+    for (int i = 0; i < n; ++i) {
+        a.states[i * ld + node] = y[i];
+        finite = finite && isfinite(y[i]);
+    }
+    if (!finite)
+        status |= GOSS_FLAG_NONFINITE;
+    ss[ES_PREV_DT * ld] = s.prev_dt;
+    ss[ES_LOC_ERROR * ld] = s.loc_error;
+    ss[ES_ETA * ld] = s.eta;
+    ss[ES_NEWTON_IT * ld] = s.newton_iterations;
+    ss[ES_FIRST * ld] = s.first_step;
+    ss[ES_NEWJAC * ld] = s.new_jacobian;
+    ss[ES_JACCOMP * ld] = s.jac_comp;
+    ss[ES_REJECTS * ld] = s.rejects;
+    ss[ES_ACCEPTED * ld] = s.accepted;
+    if (status) {
+        a.node_status[node] |= status;
+        atomicOr(a.flags, (uint32_t)status);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// batched model evaluation (ODE::eval / ODE::linearized_eval on many states)
+// ---------------------------------------------------------------------------
+template <class M, typename T>
+__global__ void __launch_bounds__(128) eval_kernel(const __grid_constant__ EvalArgs<M, T> a)
+{
+    constexpr int n = M::num_states;
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= a.N)
+        return;
+    T y[n], o1[n], o2[n];
+    for (int i = 0; i < n; ++i)
+        y[i] = T(a.states[i * a.ld + node]);
+    T F[Dims<M>::nfp];
+    load_field<M, T>(a.fparams, a.ld, node, F);
+    const double t = a.times[node];
+    if (a.what == 0) {
+        M::template rhs<T>(y, t, a.P, a.PD, F, o1);
+        for (int i = 0; i < n; ++i)
+            a.out[i * a.ld + node] = double(o1[i]);
+    } else if (a.what == 1) {
+        M::template linearized<T>(y, t, a.P, a.PD, F, o1, o2);
+        for (int i = 0; i < n; ++i) {
+            a.out[i * a.ld + node] = double(o1[i]);
+            a.out[(n + i) * a.ld + node] = double(o2[i]);
+        }
+    } else if constexpr (M::num_monitored > 0) {
+        T mon[M::num_monitored];
+        M::template monitored_values<T>(y, t, a.P, a.PD, F, mon);
+        for (int i = 0; i < M::num_monitored; ++i)
+            a.out[i * a.ld + node] = double(mon[i]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers (called through goss_model_desc::launch / ::eval)
+// ---------------------------------------------------------------------------
+inline unsigned long explicit_num_steps(double ldt_0, double dt)
+{
+    // e.g. GRL1.cpp:66
+    return ldt_0 > 0 ? (unsigned long)ceil(dt / ldt_0 - 1.0E-12) : 1UL;
+}
+
+template <class M>
+inline uint32_t solver_state_rows(int32_t solver)
+{
+    constexpr uint32_t n = M::num_states;
+    if (solver == GOSS_THETA)
+        return TH_ROWS;
+    if (solver == GOSS_ESDIRK23A)
+        return ES_SCALARS + 2 * n * n;
+    return 0;
+}
+
+template <class M, typename T, Explicit S>
+inline int launch_explicit(const goss_launch* L)
+{
+    ExplicitArgs<M, T> a;
+    a.states = L->states;
+    a.fparams = L->field_params;
+    a.flags = L->flags;
+    a.node_status = L->node_status;
+    a.ld = L->ld;
+    a.N = L->num_nodes;
+    const double ldt_0 = L->solver_params->ldt;
+    const unsigned long nsteps = explicit_num_steps(ldt_0, L->interval);
+    a.nsteps = nsteps;
+    a.ldt = L->interval / nsteps;
+    a.t = L->t;
+    a.delta = L->solver_params->delta;
+    for (int i = 0; i < Dims<M>::np; ++i) {
+        const double v = i < M::num_params ? L->params[i] : 0.0;
+        a.P[i] = T(v);
+        a.PD[i] = v;
+    }
+    const unsigned block = L->block ? L->block : 128;
+    const unsigned grid = (L->num_nodes + block - 1) / block;
+    if (grid == 0)
+        return 0;
+    explicit_kernel<M, T, S><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
+}
+
+template <class M>
+inline int launch_implicit(const goss_launch* L)
+{
+    ImplicitArgs<M> a;
+    a.states = L->states;
+    a.fparams = L->field_params;
+    a.sstate = L->solver_state;
+    a.flags = L->flags;
+    a.node_status = L->node_status;
+    a.ld = L->ld;
+    a.N = L->num_nodes;
+    a.t = L->t;
+    a.interval = L->interval;
+    a.sp = *L->solver_params;
+    a.max_loop = L->max_loop ? L->max_loop : (1ull << 24);
+    for (int i = 0; i < Dims<M>::np; ++i)
+        a.P[i] = i < M::num_params ? L->params[i] : 0.0;
+    const unsigned block = L->block ? L->block : 64;
+    const unsigned grid = (L->num_nodes + block - 1) / block;
+    if (grid == 0)
+        return 0;
+    if (L->solver == GOSS_THETA)
+        theta_kernel<M><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    else
+        esdirk_kernel<M><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
+}
+
+template <class M>
+inline int launch_solver(const goss_launch* L)
+{
+    const bool f32 = L->precision == GOSS_FP32;
+    switch (L->solver) {
+    case GOSS_EXPLICIT_EULER:
+        return f32 ? launch_explicit<M, float, Explicit::Euler>(L) : launch_explicit<M, double, Explicit::Euler>(L);
+    case GOSS_RK4:
+        return f32 ? launch_explicit<M, float, Explicit::RK4>(L) : launch_explicit<M, double, Explicit::RK4>(L);
+    case GOSS_GRL1:
+        return f32 ? launch_explicit<M, float, Explicit::GRL1>(L) : launch_explicit<M, double, Explicit::GRL1>(L);
+    case GOSS_GRL2:
+        return f32 ? launch_explicit<M, float, Explicit::GRL2>(L) : launch_explicit<M, double, Explicit::GRL2>(L);
+    case GOSS_THETA:
+    case GOSS_ESDIRK23A:
+        if (f32)
+            return GOSS_ERR_UNSUPPORTED;
+        return launch_implicit<M>(L);
+    default:
+        return GOSS_ERR_ARGUMENT;
+    }
+}
+
+template <class M, typename T>
+inline int launch_eval_t(const goss_eval_launch* L)
+{
+    EvalArgs<M, T> a;
+    a.states = L->states;
+    a.fparams = L->field_params;
+    a.times = L->times;
+    a.out = L->out;
+    a.ld = L->ld;
+    a.N = L->num_nodes;
+    a.what = L->what;
+    for (int i = 0; i < Dims<M>::np; ++i) {
+        const double v = i < M::num_params ? L->params[i] : 0.0;
+        a.P[i] = T(v);
+        a.PD[i] = v;
+    }
+    const unsigned block = 128;
+    const unsigned grid = (L->num_nodes + block - 1) / block;
+    if (grid == 0)
+        return 0;
+    eval_kernel<M, T><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
+}
+
+template <class M>
+inline int launch_eval(const goss_eval_launch* L)
+{
+    return L->precision == GOSS_FP32 ? launch_eval_t<M, float>(L) : launch_eval_t<M, double>(L);
+}
+
+}  // namespace goss_b200
+#endif

@@ -1,0 +1,118 @@
+// Generated by goss_b200.codegen from the 'beeler_reuter_1977' model; do not edit.
+// Device-side model: rhs and linearised rhs templated on the arithmetic type T.
+#ifndef BEELER_REUTER_1977_DEVICE_CUH
+#define BEELER_REUTER_1977_DEVICE_CUH
+#include "goss_device_math.cuh"
+
+namespace goss_b200 { namespace models {
+
+struct Beeler_reuter_1977 {
+  static constexpr const char* name = "beeler_reuter_1977";
+  static constexpr int num_states = 8;
+  static constexpr int num_params = 10;
+  static constexpr int num_field_params = 0;
+
+  // values = f(y, time)
+  template <typename T>
+  __device__ static __forceinline__ void rhs(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  {
+    const T s_m = y[0];
+    const T s_h = y[1];
+    const T s_j = y[2];
+    const T s_Cai = y[3];
+    const T s_d = y[4];
+    const T s_f = y[5];
+    const T s_x1 = y[6];
+    const T s_V = y[7];
+    const T v_i_Na = ((s_V - ((P[0])))*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
+    const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
+    const T v_alpha_m = (((-T(47.0)) - ((s_V)))/((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0)))));
+    const T v_beta_m = (T(0.7095526727489909)*gexp((-(T(0.056)*s_V))));
+    const T v_alpha_h = (T(5.497962438709065e-10)*gexp((-(T(0.25)*s_V))));
+    const T v_beta_h = (T(1.7)/(T(1.0) + (T(0.1580253208896478)*gexp((-(T(0.082)*s_V))))));
+    const T v_alpha_j = (T(1.8690473007222892e-10)*gexp((-(T(0.25)*s_V)))/(T(1.0) + (T(1.6788275299956603e-07)*gexp((-(T(0.2)*s_V))))));
+    const T v_beta_j = (T(0.3)/(T(1.0) + (T(0.040762203978366204)*gexp((-(T(0.1)*s_V))))));
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*glog((T(0.001)*s_Cai)))));
+    const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
+    const T v_alpha_d = (T(0.095)*gexp((T(0.05) - ((T(0.01)*s_V))))/(T(1.0) + (T(1.4332881385696572)*gexp((-(T(0.07199424046076314)*s_V))))));
+    const T v_beta_d = (T(0.07)*gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))))/(T(1.0) + gexp((T(2.2) + (T(0.05)*s_V)))));
+    const T v_alpha_f = (T(0.012)*gexp(((-T(0.224)) - ((T(0.008)*s_V))))/(T(1.0) + (T(66.5465065250986)*gexp((T(0.14992503748125938)*s_V)))));
+    const T v_beta_f = (T(0.0065)*gexp(((-T(0.6)) - ((T(0.02)*s_V))))/(T(1.0) + gexp(((-T(6.0)) - ((T(0.2)*s_V))))));
+    const T v_i_x1 = (T(0.0019727757115328517)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))));
+    const T v_alpha_x1 = (T(0.031158410986342627)*gexp((T(0.08264462809917356)*s_V))/(T(1.0) + (T(17.41170806332765)*gexp((T(0.05714285714285714)*s_V)))));
+    const T v_beta_x1 = (T(0.0003916464405623223)*gexp((-(T(0.05998800239952009)*s_V)))/(T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V))))));
+    const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
+    const T v_i_K1 = ((T(0.0035)*(T(4.6000000000000005) + (T(0.2)*s_V))/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))));
+    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((time - ((PD[8])) - ((PD[6]*floor(((time - ((PD[8])))/PD[6]))))) <= PD[7])) ? PD[4] : 0.0);
+    values[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
+    values[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
+    values[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
+    values[3] = (T(7.000000000000001e-06) - ((T(0.07)*s_Cai)) - ((T(0.01)*v_i_s)));
+    values[4] = ((v_alpha_d*(T(1.0) - ((s_d)))) - ((v_beta_d*s_d)));
+    values[5] = ((v_alpha_f*(T(1.0) - ((s_f)))) - ((v_beta_f*s_f)));
+    values[6] = ((v_alpha_x1*(T(1.0) - ((s_x1)))) - ((v_beta_x1*s_x1)));
+    values[7] = ((T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1)))/P[9]);
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // rhs = f(y, time), linear[i] = d f_i / d y_i
+  template <typename T>
+  __device__ static __forceinline__ void linearized(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ linear, T* __restrict__ rhs)
+  {
+    const T s_m = y[0];
+    const T s_h = y[1];
+    const T s_j = y[2];
+    const T s_Cai = y[3];
+    const T s_d = y[4];
+    const T s_f = y[5];
+    const T s_x1 = y[6];
+    const T s_V = y[7];
+    const T v_i_Na = ((s_V - ((P[0])))*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
+    const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
+    const T v_alpha_m = (((-T(47.0)) - ((s_V)))/((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0)))));
+    const T v_beta_m = (T(0.7095526727489909)*gexp((-(T(0.056)*s_V))));
+    const T v_alpha_h = (T(5.497962438709065e-10)*gexp((-(T(0.25)*s_V))));
+    const T v_beta_h = (T(1.7)/(T(1.0) + (T(0.1580253208896478)*gexp((-(T(0.082)*s_V))))));
+    const T v_alpha_j = (T(1.8690473007222892e-10)*gexp((-(T(0.25)*s_V)))/(T(1.0) + (T(1.6788275299956603e-07)*gexp((-(T(0.2)*s_V))))));
+    const T v_beta_j = (T(0.3)/(T(1.0) + (T(0.040762203978366204)*gexp((-(T(0.1)*s_V))))));
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*glog((T(0.001)*s_Cai)))));
+    const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
+    const T v_alpha_d = (T(0.095)*gexp((T(0.05) - ((T(0.01)*s_V))))/(T(1.0) + (T(1.4332881385696572)*gexp((-(T(0.07199424046076314)*s_V))))));
+    const T v_beta_d = (T(0.07)*gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))))/(T(1.0) + gexp((T(2.2) + (T(0.05)*s_V)))));
+    const T v_alpha_f = (T(0.012)*gexp(((-T(0.224)) - ((T(0.008)*s_V))))/(T(1.0) + (T(66.5465065250986)*gexp((T(0.14992503748125938)*s_V)))));
+    const T v_beta_f = (T(0.0065)*gexp(((-T(0.6)) - ((T(0.02)*s_V))))/(T(1.0) + gexp(((-T(6.0)) - ((T(0.2)*s_V))))));
+    const T v_i_x1 = (T(0.0019727757115328517)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))));
+    const T v_alpha_x1 = (T(0.031158410986342627)*gexp((T(0.08264462809917356)*s_V))/(T(1.0) + (T(17.41170806332765)*gexp((T(0.05714285714285714)*s_V)))));
+    const T v_beta_x1 = (T(0.0003916464405623223)*gexp((-(T(0.05998800239952009)*s_V)))/(T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V))))));
+    const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
+    const T v_i_K1 = ((T(0.0035)*(T(4.6000000000000005) + (T(0.2)*s_V))/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))));
+    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((time - ((PD[8])) - ((PD[6]*floor(((time - ((PD[8])))/PD[6]))))) <= PD[7])) ? PD[4] : 0.0);
+    rhs[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
+    rhs[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
+    rhs[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
+    rhs[3] = (T(7.000000000000001e-06) - ((T(0.07)*s_Cai)) - ((T(0.01)*v_i_s)));
+    rhs[4] = ((v_alpha_d*(T(1.0) - ((s_d)))) - ((v_beta_d*s_d)));
+    rhs[5] = ((v_alpha_f*(T(1.0) - ((s_f)))) - ((v_beta_f*s_f)));
+    rhs[6] = ((v_alpha_x1*(T(1.0) - ((s_x1)))) - ((v_beta_x1*s_x1)));
+    rhs[7] = ((T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1)))/P[9]);
+    linear[0] = ((-(v_alpha_m)) - ((v_beta_m)));
+    linear[1] = ((-(v_alpha_h)) - ((v_beta_h)));
+    linear[2] = ((-(v_alpha_j)) - ((v_beta_j)));
+    linear[4] = ((-(v_alpha_d)) - ((v_beta_d)));
+    linear[5] = ((-(v_alpha_f)) - ((v_beta_f)));
+    linear[6] = ((-(v_alpha_x1)) - ((v_beta_x1)));
+    const T v_dE_s_dCai = (-(T(13.0287)/s_Cai));
+    const T v_di_s_dCai = (-(s_d*v_dE_s_dCai*s_f*P[3]));
+    const T v_dV_eff_1_dV = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0));
+    const T v_di_K1_dV = ((T(0.0007000000000000001)/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.016779896026542326)*gexp((T(0.04)*s_V))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))*((-(T(0.3332454995075077)*gexp((T(0.04)*s_V)))) - ((T(5.552628147100417)*gexp((T(0.08)*s_V)))))/(((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V)))))) - ((T(0.00028000000000000003)*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V))*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))))));
+    const T v_di_Na_dV = (P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)));
+    const T v_di_s_dV = (s_d*s_f*P[3]);
+    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))))));
+    linear[3] = ((-T(0.07)) - ((T(0.01)*v_di_s_dCai)));
+    linear[7] = ((-(v_di_K1_dV/P[9])) - ((v_di_Na_dV/P[9])) - ((v_di_s_dV/P[9])) - ((v_di_x1_dV/P[9])));
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+};
+
+}}  // namespace goss_b200::models
+#endif

@@ -1,0 +1,41 @@
+// Generated by goss_b200.codegen from the 'oscilator' model; do not edit.
+// Device-side model: rhs and linearised rhs templated on the arithmetic type T.
+#ifndef OSCILATOR_DEVICE_CUH
+#define OSCILATOR_DEVICE_CUH
+#include "goss_device_math.cuh"
+
+namespace goss_b200 { namespace models {
+
+struct Oscilator {
+  static constexpr const char* name = "oscilator";
+  static constexpr int num_states = 2;
+  static constexpr int num_params = 2;
+  static constexpr int num_field_params = 2;
+
+  // values = f(y, time)
+  template <typename T>
+  __device__ static __forceinline__ void rhs(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    values[0] = (-(F[0]*s_y));
+    values[1] = (F[1]*s_x);
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // rhs = f(y, time), linear[i] = d f_i / d y_i
+  template <typename T>
+  __device__ static __forceinline__ void linearized(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ linear, T* __restrict__ rhs)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    rhs[0] = (-(F[0]*s_y));
+    rhs[1] = (F[1]*s_x);
+    linear[0] = T(0.0);
+    linear[1] = T(0.0);
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+};
+
+}}  // namespace goss_b200::models
+#endif

@@ -1,0 +1,243 @@
+/*
+ * goss_b200 -- C ABI of the B200 (sm_100a) multi-node ODE solve path.
+ *
+ * This is the drop-in boundary that replaces the execution of
+ * goss::ODESystemSolver (reference cpp/goss/ODESystemSolver.h:43-124) and of
+ * the per-node solvers it drives (ExplicitEuler, RK4, GRL1, GRL2,
+ * ThetaSolver, ESDIRK23a).  Only plain C types cross it: pointers, sizes,
+ * doubles and integer status codes.  Host arrays are borrowed for the
+ * duration of a call and the call is complete on return (the reference is
+ * synchronous), except for the *_async entry points.
+ *
+ * Every entry point returns 0 (GOSS_OK) on success or a positive status
+ * code; goss_system_last_error() gives the message.  Status codes map to the
+ * reference's exceptions (std::runtime_error -> RuntimeError in Python).
+ *
+ * Layout conventions
+ *   tangled   = 1 : user arrays are node-major  [num_nodes][k]
+ *   tangled   = 0 : user arrays are component-major [k][num_nodes]
+ *   (the reference's tangled_storage flag, ODESystemSolver.h:238-312)
+ * On the device states live component-major: states[i*ld + node], FP64.
+ */
+#ifndef GOSS_B200_H
+#define GOSS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GOSS_API __attribute__((visibility("default")))
+#else
+#define GOSS_API
+#endif
+
+#define GOSS_B200_ABI_VERSION 1u
+
+/* Solver kinds: the reference solver classes on this path. */
+enum goss_solver_kind {
+    GOSS_EXPLICIT_EULER = 0, /* cpp/goss/ExplicitEuler.cpp:64-87 */
+    GOSS_RK4 = 1,            /* cpp/goss/RK4.cpp:68-102 */
+    GOSS_GRL1 = 2,           /* cpp/goss/GRL1.cpp:61-82 */
+    GOSS_GRL2 = 3,           /* cpp/goss/GRL2.cpp:63-86 */
+    GOSS_THETA = 4,          /* cpp/goss/ThetaSolver.cpp:49-155 */
+    GOSS_ESDIRK23A = 5,      /* cpp/goss/ESDIRK23a.cpp:280-316 */
+    GOSS_NUM_SOLVERS = 6
+};
+
+/* Arithmetic of the right-hand side.  States are always stored and
+ * accumulated in FP64; GOSS_FP32 evaluates the model and the explicit
+ * update in FP32 (implicit solvers keep Newton and LU in FP64). */
+enum goss_precision { GOSS_FP64 = 0, GOSS_FP32 = 1 };
+
+enum goss_status {
+    GOSS_OK = 0,
+    GOSS_ERR_ARGUMENT = 1,    /* invalid argument (std::invalid_argument / ValueError) */
+    GOSS_ERR_CUDA = 2,        /* CUDA runtime failure */
+    GOSS_ERR_NEWTON = 3,      /* ThetaSolver: dt fell below min_dt (ThetaSolver.cpp:133-149) */
+    GOSS_ERR_UNSUPPORTED = 4, /* solver / model combination not available */
+    GOSS_ERR_TIMEOUT = 5,     /* a bounded device loop hit its iteration cap */
+    GOSS_ERR_NOT_ATTACHED = 6
+};
+
+/* Bits of the device status word (goss_system_status). */
+enum goss_flag_bits {
+    GOSS_FLAG_NONFINITE = 1u,     /* a node produced a non-finite state */
+    GOSS_FLAG_NEWTON_FAILED = 2u, /* a node's step size fell below min_dt */
+    GOSS_FLAG_ITERATION_CAP = 4u  /* a node exhausted the loop guard */
+};
+
+/* Solver parameters: the public members of the reference solver classes.
+ * goss_solver_default_params() fills the reference defaults. */
+typedef struct goss_solver_params {
+    double ldt;                     /* ODESolver::_ldt, <= 0: one step per interval (ODESolver.h:137) */
+    double delta;                   /* GRL1::delta (GRL1.h:39) */
+    double eta_0;                   /* ImplicitODESolver.h:36 */
+    double kappa;                   /* ImplicitODESolver.h:37 */
+    double relative_tolerance;      /* ImplicitODESolver.h:38 */
+    double max_relative_previous_residual; /* ImplicitODESolver.h:40 */
+    int32_t max_iterations;         /* ImplicitODESolver.h:39 */
+    int32_t always_recompute_jacobian; /* ImplicitODESolver.h:41 */
+    int32_t num_refinements_without_always_recomputing_jacobian; /* ThetaSolver.h:35, ESDIRK23a.h:37 */
+    double min_dt;                  /* ThetaSolver.h:36, ESDIRK23a.h:38 */
+    double theta;                   /* ThetaSolver.h:37 */
+} goss_solver_params;
+
+/* One kernel launch of a solver over a node range (filled by the runtime,
+ * consumed by a model module's launch function). */
+typedef struct goss_launch {
+    int32_t solver;
+    int32_t precision;
+    uint32_t num_nodes;
+    uint32_t block;          /* threads per block, 0 = module default */
+    uint64_t ld;             /* row stride of the device arrays, >= num_nodes */
+    double* states;          /* device [num_states][ld] */
+    const double* field_params; /* device [num_field_parameters][ld] (may be NULL if none) */
+    double* solver_state;    /* device, solver specific (goss_model_desc.solver_state_rows) */
+    uint32_t* flags;         /* device status word */
+    uint8_t* node_status;    /* device [ld] per-node flag bits */
+    const double* params;    /* host [num_parameters] uniform parameter values */
+    const goss_solver_params* solver_params; /* host */
+    double t;
+    double interval;
+    uint64_t max_loop;       /* guard for adaptive loops (0 = default) */
+    void* stream;            /* cudaStream_t */
+} goss_launch;
+
+/* Batched evaluation of the model on device arrays (used by ODE.eval and the
+ * tests): out = rhs (what = 0) or [linear; rhs] (what = 1). */
+typedef struct goss_eval_launch {
+    int32_t what;
+    int32_t precision;
+    uint32_t num_nodes;
+    uint64_t ld;
+    const double* states;       /* device [num_states][ld] */
+    const double* field_params; /* device [nfp][ld] or NULL */
+    const double* times;        /* device [num_nodes] */
+    double* out;                /* device [num_states][ld] (what=0) or [2*num_states][ld] */
+    const double* params;       /* host [num_parameters] */
+    void* stream;
+} goss_eval_launch;
+
+/* A compiled model: produced by the code generator for one .ode model and one
+ * choice of field parameters; replaces the goss::ParameterizedODE plugin and
+ * its extern "C" create_<Name>() factory (python/goss/codegeneration.py:109-112). */
+typedef struct goss_model_desc {
+    uint32_t abi_version;
+    const char* name;
+    uint32_t num_states;
+    uint32_t num_parameters;
+    uint32_t num_field_parameters;
+    uint32_t num_monitored;
+    const char* const* state_names;
+    const char* const* parameter_names;
+    const char* const* field_parameter_names;
+    const uint32_t* field_parameter_indices;
+    const double* initial_conditions;
+    const double* default_parameters;
+    const uint8_t* linear_terms;
+    uint32_t supported_solvers;   /* bit i set: solver kind i compiled */
+    int (*launch)(const goss_launch* launch);
+    int (*eval)(const goss_eval_launch* launch);
+    /* rows of FP64 per node that solver kind s needs in solver_state */
+    uint32_t (*solver_state_rows)(int32_t solver);
+    /* static FP operation census of one linearized evaluation and one rhs
+     * evaluation: add, mul, div, exp, log, sqrt, pow, cmp, misc */
+    const uint32_t* op_census_linearized;
+    const uint32_t* op_census_rhs;
+} goss_model_desc;
+
+typedef struct goss_system goss_system;
+
+/* ODESystemSolver(uint nodes, shared_ptr<ODESolver>, shared_ptr<ParameterizedODE>)
+ * (ODESystemSolver.cpp:45-59): allocates device state, sets the initial
+ * conditions and default field parameters (reset_default). */
+GOSS_API int goss_system_create(const goss_model_desc* model, int32_t solver, const goss_solver_params* params,
+                                uint32_t num_nodes, int32_t precision, int32_t device, goss_system** out);
+GOSS_API int goss_system_destroy(goss_system* sys);
+
+/* reference defaults of a solver kind */
+GOSS_API int goss_solver_default_params(int32_t solver, goss_solver_params* out);
+GOSS_API int goss_system_set_solver_params(goss_system* sys, const goss_solver_params* params);
+GOSS_API int goss_system_get_solver_params(const goss_system* sys, goss_solver_params* out);
+
+/* ODESystemSolver::forward(t, interval) (ODESystemSolver.cpp:67-79) */
+GOSS_API int goss_system_forward(goss_system* sys, double t, double interval);
+/* ODESystemSolver::solve (ODESystemSolver.cpp:81-99): field_states is
+ * [num_timesteps][num_nodes][nfs] (tangled) or [num_timesteps][nfs][num_nodes];
+ * row 0 is left untouched, row i holds the field states after the step to t[i]. */
+GOSS_API int goss_system_solve(goss_system* sys, double* field_states, const double* t, uint64_t num_timesteps,
+                               int32_t tangled);
+
+/* Field states: the states named by field_state_indices (ParameterizedODE.h:147-150). */
+GOSS_API int goss_system_set_field_state_indices(goss_system* sys, const uint32_t* indices, uint32_t count);
+GOSS_API int goss_system_get_field_states(const goss_system* sys, double* values, int32_t tangled);
+GOSS_API int goss_system_set_field_states(goss_system* sys, const double* values, int32_t tangled);
+GOSS_API int goss_system_get_field_state_components(const goss_system* sys, double* values,
+                                                    uint32_t num_components, const uint32_t* components,
+                                                    int32_t tangled);
+GOSS_API int goss_system_set_field_state_components(goss_system* sys, const double* values,
+                                                    uint32_t num_components, const uint32_t* components,
+                                                    int32_t tangled);
+GOSS_API int goss_system_get_field_parameters(const goss_system* sys, double* values, int32_t tangled);
+GOSS_API int goss_system_set_field_parameters(goss_system* sys, const double* values, int32_t tangled);
+
+/* All states, node-major [num_nodes][num_states] (ODESystemSolver::states()). */
+GOSS_API int goss_system_get_states(const goss_system* sys, double* states);
+GOSS_API int goss_system_set_states(goss_system* sys, const double* states);
+
+/* Uniform model parameters (ParameterizedODE::set_parameter/get_parameter by index). */
+GOSS_API int goss_system_set_parameter(goss_system* sys, uint32_t index, double value);
+GOSS_API int goss_system_get_parameter(const goss_system* sys, uint32_t index, double* value);
+
+/* reset_default() (ODESystemSolver.cpp:192-216); also resets implicit solver state */
+GOSS_API int goss_system_reset_default(goss_system* sys);
+
+/* set_num_threads/get_num_threads keep their API; the device ignores them. */
+GOSS_API int goss_system_set_num_threads(goss_system* sys, uint32_t num_threads);
+GOSS_API uint32_t goss_system_get_num_threads(const goss_system* sys);
+GOSS_API uint32_t goss_system_num_nodes(const goss_system* sys);
+
+/* Launch configuration (threads per block; 0 = model default). */
+GOSS_API int goss_system_set_block_size(goss_system* sys, uint32_t block);
+
+/* Status word accumulated since the last clear (goss_flag_bits). */
+GOSS_API int goss_system_status(goss_system* sys, uint32_t* flags, int32_t clear);
+/* Per-node flag bits [num_nodes]. */
+GOSS_API int goss_system_node_status(const goss_system* sys, uint8_t* out);
+/* Counters of the implicit solvers per node: jacobian computations,
+ * rejected steps, accepted steps (any pointer may be NULL). */
+GOSS_API int goss_system_counters(const goss_system* sys, int64_t* jac_comp, int64_t* rejected, int64_t* accepted);
+
+/* Device-resident access for callers that keep data on the GPU. */
+GOSS_API int goss_system_device_states(goss_system* sys, double** states, uint64_t* ld);
+GOSS_API int goss_system_device_field_params(goss_system* sys, double** field_params, uint64_t* ld);
+GOSS_API int goss_system_set_stream(goss_system* sys, void* stream);
+GOSS_API int goss_system_forward_async(goss_system* sys, double t, double interval);
+GOSS_API int goss_system_synchronize(goss_system* sys);
+
+/* Batched model evaluation on host arrays: states [count][n], times [count],
+ * field_params [count][nfp] (may be NULL), out [count][n] (what=0) or
+ * [count][2n] = (linear, rhs) (what=1). */
+GOSS_API int goss_model_eval(const goss_model_desc* model, int32_t what, int32_t precision, const double* params,
+                             const double* states, const double* field_params, const double* times, uint64_t count,
+                             double* out, int32_t device);
+
+/* Single-matrix helpers of the ODE plugin interface, on the host (the
+ * reference's ODE::lu_factorize / ODE::forward_backward_subst, ODE.cpp:69-132):
+ * in-place LU without pivoting of a row-major n x n matrix, and the solve
+ * with that factorisation (b and x may alias). */
+GOSS_API int goss_lu_factorize(uint32_t n, double* mat);
+GOSS_API int goss_forward_backward_subst(uint32_t n, const double* mat, const double* b, double* x);
+
+GOSS_API const char* goss_system_last_error(const goss_system* sys);
+GOSS_API const char* goss_last_error(void);
+GOSS_API uint32_t goss_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,287 @@
+"""Test infrastructure -- NOT part of the product path.
+
+ctypes access to the oracle: the C restatement (``goss_oracle.c`` plus a
+generated model C file, built into ``oracle/_build/<variant>/liboracle.so``)
+and, when it has been built, the reference's own solvers
+(``oracle/_ref/``, see ``oracle/Makefile`` and ``oracle/ref_driver.cpp``).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+REFDIR = HERE / "_ref"
+
+SOLVERS = {"ExplicitEuler": 0, "RK4": 1, "GRL1": 2, "GRL2": 3, "ThetaSolver": 4, "ESDIRK23a": 5}
+
+_dp = C.POINTER(C.c_double)
+
+
+class _Model(C.Structure):
+    _fields_ = [
+        ("name", C.c_char_p),
+        ("num_states", C.c_int),
+        ("num_params", C.c_int),
+        ("num_field_params", C.c_int),
+        ("field_param_index", C.POINTER(C.c_uint)),
+        ("rhs", C.CFUNCTYPE(None, _dp, C.c_double, _dp, _dp)),
+        ("linearized", C.CFUNCTYPE(None, _dp, C.c_double, _dp, _dp, _dp, C.c_int)),
+        ("ic", _dp),
+        ("default_params", _dp),
+        ("linear_terms", C.POINTER(C.c_ubyte)),
+    ]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [
+        ("ldt", C.c_double),
+        ("delta", C.c_double),
+        ("eta_0", C.c_double),
+        ("kappa", C.c_double),
+        ("relative_tolerance", C.c_double),
+        ("max_relative_previous_residual", C.c_double),
+        ("max_iterations", C.c_int),
+        ("always_recompute_jacobian", C.c_int),
+        ("num_refinements_without_always_recomputing_jacobian", C.c_int),
+        ("min_dt", C.c_double),
+        ("theta", C.c_double),
+    ]
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def build_oracle(variant_dir: Path, ident: str, force: bool = False) -> Path:
+    """Compile goss_oracle.c + the variant's generated C model into a .so."""
+    out = BUILD / variant_dir.name / "liboracle.so"
+    src = variant_dir / "oracle_model.c"
+    deps = [src, HERE / "goss_oracle.c", HERE / "goss_oracle.h"]
+    if not force and out.exists() and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return out
+    out.parent.mkdir(parents=True, exist_ok=True)
+    cmd = [_cc("gcc"), "-O2", "-fPIC", "-shared", "-fopenmp", "-std=c11", f"-I{HERE}", str(HERE / "goss_oracle.c"),
+           str(src), "-lm", "-o", str(out)]
+    subprocess.run(cmd, check=True)
+    return out
+
+
+class OracleModel:
+    """Single-state evaluation of a generated model through the C restatement."""
+
+    def __init__(self, lib_path: Path, ident: str):
+        self.lib = C.CDLL(str(lib_path))
+        getter = getattr(self.lib, f"oracle_model_{ident}")
+        getter.restype = C.POINTER(_Model)
+        self.ptr = getter()
+        self.m = self.ptr.contents
+        self.n = self.m.num_states
+        self.np = self.m.num_params
+        self.nfp = self.m.num_field_params
+        self.lib.oracle_system_create.restype = C.c_void_p
+        self.lib.oracle_system_create.argtypes = [C.POINTER(_Model), C.c_int, C.POINTER(SolverParams), C.c_uint32]
+        self.lib.oracle_system_destroy.argtypes = [C.c_void_p]
+        for f in ("oracle_system_states", "oracle_system_field_params", "oracle_system_params"):
+            getattr(self.lib, f).restype = _dp
+            getattr(self.lib, f).argtypes = [C.c_void_p]
+        self.lib.oracle_system_forward.restype = C.c_int
+        self.lib.oracle_system_forward.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+        self.lib.oracle_system_counters.argtypes = [C.c_void_p] + [C.POINTER(C.c_int64)] * 3
+        self.lib.oracle_default_solver_params.argtypes = [C.c_int, C.POINTER(SolverParams)]
+        self.lib.oracle_compute_jacobian.argtypes = [C.POINTER(_Model), _dp, _dp, C.c_double, _dp, _dp, _dp]
+        self.lib.oracle_lu_factorize.argtypes = [C.c_int, _dp]
+        self.lib.oracle_forward_backward_subst.argtypes = [C.c_int, _dp, _dp, _dp]
+
+    @property
+    def ic(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.m.ic, shape=(self.n,)).copy()
+
+    @property
+    def default_params(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.m.default_params, shape=(max(self.np, 1),))[: self.np].copy()
+
+    def rhs(self, y, t, params=None) -> np.ndarray:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        p = self.default_params if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        out = np.zeros(self.n)
+        self.m.rhs(_ptr(y), float(t), _ptr(p), _ptr(out))
+        return out
+
+    def linearized(self, y, t, params=None, only_linear=False):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        p = self.default_params if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        lin = np.zeros(self.n)
+        rhs = np.zeros(self.n)
+        self.m.linearized(_ptr(y), float(t), _ptr(p), _ptr(lin), _ptr(rhs), int(only_linear))
+        return lin, rhs
+
+    def jacobian(self, y, t, params=None) -> np.ndarray:
+        y = np.array(y, dtype=np.float64)
+        p = self.default_params if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        jac = np.zeros((self.n, self.n))
+        f1, f2 = np.zeros(self.n), np.zeros(self.n)
+        self.lib.oracle_compute_jacobian(self.ptr, _ptr(p), _ptr(y), float(t), _ptr(jac), _ptr(f1), _ptr(f2))
+        return jac
+
+    def solver_params(self, solver: str, **overrides) -> SolverParams:
+        sp = SolverParams()
+        self.lib.oracle_default_solver_params(SOLVERS[solver], C.byref(sp))
+        for k, v in overrides.items():
+            setattr(sp, k, v)
+        return sp
+
+
+class OracleSystem:
+    """Multi-node FP64 CPU solve (restatement of ODESystemSolver::forward)."""
+
+    def __init__(self, model: OracleModel, solver: str, num_nodes: int, **solver_params):
+        self.model = model
+        self.solver = solver
+        self.N = int(num_nodes)
+        self.sp = model.solver_params(solver, **solver_params)
+        self.h = model.lib.oracle_system_create(model.ptr, SOLVERS[solver], C.byref(self.sp), self.N)
+        n, nfp = model.n, model.nfp
+        self.states = np.ctypeslib.as_array(model.lib.oracle_system_states(self.h), shape=(self.N, n))
+        self.field_params = np.ctypeslib.as_array(model.lib.oracle_system_field_params(self.h),
+                                                  shape=(self.N, max(nfp, 1)))[:, :nfp]
+        self.params = np.ctypeslib.as_array(model.lib.oracle_system_params(self.h), shape=(max(model.np, 1),))
+
+    def forward(self, t: float, interval: float, threads: Optional[int] = None) -> int:
+        if threads is None:
+            threads = os.cpu_count() or 1
+        return self.model.lib.oracle_system_forward(self.h, float(t), float(interval), int(threads))
+
+    def counters(self):
+        jc = np.zeros(self.N, dtype=np.int64)
+        rj = np.zeros(self.N, dtype=np.int64)
+        ac = np.zeros(self.N, dtype=np.int64)
+        p = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
+        self.model.lib.oracle_system_counters(self.h, p(jc), p(rj), p(ac))
+        return jc, rj, ac
+
+    def __del__(self):
+        try:
+            self.model.lib.oracle_system_destroy(self.h)
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# the reference's own solvers (oracle/_ref, built by oracle/Makefile)
+# ---------------------------------------------------------------------------
+REF_SOURCES = Path(os.environ.get("GOSS_REFERENCE", "/root/reference"))
+
+
+def _cc(name: str) -> str:
+    p = Path("/usr/bin") / name
+    return str(p) if p.exists() else name
+
+
+def ref_available() -> bool:
+    return (REFDIR / "libgoss_ref_driver.so").exists()
+
+
+def build_ref_core() -> bool:
+    """Build oracle/_ref with the Makefile when the reference sources exist."""
+    if not REF_SOURCES.is_dir():
+        return ref_available()
+    subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REF_SOURCES}"], check=True)
+    return ref_available()
+
+
+def build_ref_plugin(variant_dir: Path, force: bool = False) -> Optional[Path]:
+    """Compile a variant's goss::ParameterizedODE plugin against the reference headers."""
+    variant_dir = Path(variant_dir).resolve()
+    out = REFDIR / variant_dir.name / "libplugin.so"
+    hdr = variant_dir / "goss_plugin.h"
+    if not force and out.exists() and out.stat().st_mtime >= hdr.stat().st_mtime:
+        return out
+    if not REF_SOURCES.is_dir() or not ref_available():
+        return out if out.exists() else None
+    out.parent.mkdir(parents=True, exist_ok=True)
+    src = out.parent / "plugin.cpp"
+    src.write_text(f'#include "{hdr}"\n')
+    subprocess.run([_cc("g++"), "-O3", "-DNDEBUG", "-std=c++17", "-fPIC", "-shared", f"-I{REF_SOURCES / 'cpp'}",
+                    str(src), f"-L{REFDIR}", "-lgoss_ref", f"-Wl,-rpath,{REFDIR}", "-o", str(out)], check=True)
+    return out
+
+
+class RefSystem:
+    """The reference's ODESystemSolver over N nodes (implicit: one per node)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            C.CDLL(str(REFDIR / "libgoss_ref.so"), mode=C.RTLD_GLOBAL)
+            L = C.CDLL(str(REFDIR / "libgoss_ref_driver.so"))
+            L.ref_create.restype = C.c_void_p
+            L.ref_create.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(SolverParams), C.c_uint32]
+            L.ref_destroy.argtypes = [C.c_void_p]
+            L.ref_set_parameter.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
+            L.ref_set_states.argtypes = [C.c_void_p, _dp]
+            L.ref_get_states.argtypes = [C.c_void_p, _dp]
+            L.ref_set_field_parameters.argtypes = [C.c_void_p, _dp]
+            L.ref_set_num_threads.argtypes = [C.c_void_p, C.c_uint32]
+            L.ref_forward.argtypes = [C.c_void_p, C.c_double, C.c_double]
+            L.ref_forward.restype = C.c_int
+            L.ref_num_states.argtypes = [C.c_void_p]
+            L.ref_last_error.argtypes = [C.c_void_p]
+            L.ref_last_error.restype = C.c_char_p
+            L.ref_num_jac_comp.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, plugin: Path, class_name: str, solver: str, num_nodes: int, sp: SolverParams):
+        L = self.lib()
+        self.N = int(num_nodes)
+        self.h = L.ref_create(str(plugin).encode(), class_name.encode(), SOLVERS[solver], C.byref(sp), self.N)
+        if not self.h:
+            raise RuntimeError(f"cannot create reference system from {plugin}")
+        self.n = L.ref_num_states(self.h)
+
+    def set_states(self, states: np.ndarray) -> None:
+        s = np.ascontiguousarray(states, dtype=np.float64).reshape(self.N, self.n)
+        self.lib().ref_set_states(self.h, _ptr(s))
+
+    def get_states(self) -> np.ndarray:
+        out = np.zeros((self.N, self.n))
+        self.lib().ref_get_states(self.h, _ptr(out))
+        return out
+
+    def set_field_parameters(self, fp: np.ndarray) -> None:
+        f = np.ascontiguousarray(fp, dtype=np.float64)
+        self.lib().ref_set_field_parameters(self.h, _ptr(f))
+
+    def set_parameter(self, name: str, value: float) -> None:
+        if self.lib().ref_set_parameter(self.h, name.encode(), float(value)):
+            raise RuntimeError(self.lib().ref_last_error(self.h).decode())
+
+    def set_num_threads(self, threads: int) -> None:
+        self.lib().ref_set_num_threads(self.h, int(threads))
+
+    def forward(self, t: float, interval: float) -> int:
+        return self.lib().ref_forward(self.h, float(t), float(interval))
+
+    def num_jac_comp(self) -> np.ndarray:
+        out = np.zeros(self.N, dtype=np.int64)
+        self.lib().ref_num_jac_comp(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)))
+        return out
+
+    def __del__(self):
+        try:
+            self.lib().ref_destroy(self.h)
+        except Exception:
+            pass
