@@ -1,0 +1,403 @@
+"""Benchmark: cell-steps/s of the ten Tusscher-Panfilov 2006 M-cell model
+with GRL1 over 1,048,576 nodes (FP32 arithmetic, FP64 state accumulation),
+with the FP64 path, the FP32-vs-FP64 V error and the end-to-end API number.
+
+Workload (per GPU): TP06 M-cell, GRL1, internal step 0.01 ms, 1,048,576 nodes,
+per-node field parameters g_Kr, g_Ks, g_CaL, g_to = default * exp(0.2 xi),
+xi ~ N(0, 1) (seed 1234), initial states = IC * (1 + u), u ~ U(-0.05, 0.05),
+stimulus -52 pA/pF for 1 ms at t = 10 ms (model defaults).  One bench step
+is one ``forward(t, 10 ms)`` = 1000 internal steps at every node; W warm-up
+steps plus K timed steps advance the model W+K times 10 ms (the default
+3 + 47 covers the 500 ms of the workload).  The states (159 MB FP64) exceed
+L2 (126 MB) and stay in registers inside a step, so no L2 flush is needed.
+
+Usage::
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MODEL = "tentusscher_panfilov_2006_M_cell"
+FIELDS = ["g_Kr", "g_Ks", "g_CaL", "g_to"]
+N_NODES = 1 << 20
+LDT = 0.01
+INTERVAL = 10.0
+SEED = 1234
+METRIC = "cell-steps/s tenTusscher GRL1 1M nodes: FP32 vs FP64 @V err<=1e-3; adjoint/fwd"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=47)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="goss_b200", choices=["goss_b200", "reference"])
+    ap.add_argument("--nodes", type=int, default=N_NODES)
+    ap.add_argument("--skip-fp64", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--profile", choices=["single", "double"], default=None,
+                    help="only run the timed forward loop in one precision (for ncu captures)")
+    return ap.parse_args()
+
+
+def profile_run(args):
+    """Minimal run for profiler captures: W+K forward calls of one precision."""
+    import goss_b200 as goss
+
+    md, y0, fp = inputs(args.nodes)
+    ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS)
+    solver = goss.solvers.GRL1(ode)
+    solver.internal_time_step = LDT
+    system = goss.ODESystemSolver(args.nodes, solver, ode, precision=args.profile)
+    system.set_states(y0)
+    system.field_parameters = fp
+    t = 0.0
+    for _ in range(args.warmup + args.steps):
+        system.forward(t, INTERVAL)
+        t += INTERVAL
+    print(json.dumps({"profile": args.profile, "nodes": args.nodes, "launches": args.warmup + args.steps,
+                      "finite": bool(np.isfinite(system.states).all())}))
+
+
+def inputs(num_nodes, rank=0):
+    """Seeded states and field parameters of one rank's shard."""
+    from goss_b200 import models
+
+    md = json.loads((models.find_variant(MODEL, FIELDS) / "model.json").read_text())
+    rng = np.random.default_rng(SEED + rank)
+    ic = np.array(md["initial_conditions"])
+    y0 = ic[None, :] * (1.0 + rng.uniform(-0.05, 0.05, (num_nodes, ic.size)))
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * np.exp(0.2 * rng.standard_normal((num_nodes, len(FIELDS))))
+    return md, y0, fp
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args, rank, world, dist):
+    import torch
+
+    import goss_b200 as goss
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    N = args.nodes
+    md, y0, fp = inputs(N, rank)
+    ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS, field_states=["V"])
+    iv = md["state_names"].index("V")
+    stream = torch.cuda.Stream()
+
+    def make(precision):
+        solver = goss.solvers.GRL1(ode)
+        solver.internal_time_step = LDT
+        system = goss.ODESystemSolver(N, solver, ode, precision=precision, device=dev)
+        system.set_stream(stream.cuda_stream)
+        system.set_states(y0)
+        system.field_parameters = fp
+        return system
+
+    def timed(system, steps, warmup, t0=0.0):
+        """device time of `steps` forward calls (CUDA events on the launch stream)."""
+        t = t0
+        for _ in range(warmup):
+            system.forward_async(t, INTERVAL)
+            t += INTERVAL
+        system.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            start.record(stream)
+        for _ in range(steps):
+            system.forward_async(t, INTERVAL)
+            t += INTERVAL
+        with torch.cuda.stream(stream):
+            end.record(stream)
+        system.synchronize()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(end)
+        return ms, t
+
+    steps_per_call = int(round(INTERVAL / LDT))
+    out = {}
+    # --- FP32 (headline) ---------------------------------------------------
+    s32 = make("single")
+    with ClockSampler(dev) as clocks:
+        ms32, t_end = timed(s32, args.steps, args.warmup)
+    # --- FP64 on the same inputs and the same number of steps --------------
+    fp64_ms = None
+    s64 = None
+    if not args.skip_fp64:
+        s64 = make("double")
+        fp64_ms, _ = timed(s64, args.steps, args.warmup)
+    # --- accuracy of FP32 against FP64 at the end of the run ----------------
+    v32 = s32.states[:, iv]
+    err = None
+    if s64 is not None:
+        v64 = s64.states[:, iv]
+        err = float(np.max(np.abs(v32 - v64) / np.maximum(np.abs(v64), 1e-12)))
+        all32, all64 = s32.states, s64.states
+        state_err = np.max(np.abs(all32 - all64) / np.maximum(np.abs(all64), 1e-12), axis=0)
+        out["state_max_rel_err_fp32_vs_fp64"] = {n: float(e) for n, e in zip(md["state_names"], state_err)}
+        del s64
+    # --- end to end through the public API with host buffers -----------------
+    e2e = make("single")
+    v_host = np.ascontiguousarray(y0[:, iv:iv + 1])
+    t = 0.0
+    for _ in range(args.warmup):
+        e2e.field_states = v_host
+        e2e.forward(t, INTERVAL)
+        v_host = e2e.field_states
+        t += INTERVAL
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e.field_states = v_host          # H2D: this step's input (V), N doubles
+        e2e.forward(t, INTERVAL)           # synchronous like the reference
+        v_host = e2e.field_states          # D2H: this step's result (V), N doubles
+        t += INTERVAL
+    e2e_s = time.perf_counter() - w0
+    del e2e
+
+    times = torch.tensor([ms32, fp64_ms or 0.0, e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms32, fp64_ms_max, e2e_s = [float(x) for x in times.tolist()]
+    cell_steps = float(N) * steps_per_call * args.steps * world
+    value = cell_steps / (ms32 / 1e3)
+    out.update(dict(
+        value=value, ms_per_step=ms32 / args.steps, clocks=clocks.summary(),
+        fp64_value=(cell_steps / (fp64_ms_max / 1e3)) if fp64_ms else None,
+        fp32_over_fp64=(fp64_ms_max / ms32) if fp64_ms else None,
+        v_max_rel_err_fp32_vs_fp64=err,
+        e2e={"value": cell_steps / e2e_s, "unit": "cell-steps/s", "h2d_bytes_per_step": 8 * N,
+             "d2h_bytes_per_step": 8 * N, "path": "ODESystemSolver.field_states/forward (public Python API)"},
+        model_time_ms=t_end,
+    ))
+    return out, md
+
+
+def roofline(md, value_fp32, ms_per_step, n_nodes):
+    """Operation census of one GRL1 step (generator) against the CUDA-core peaks."""
+    lin = md["op_census"]["linearized"]
+    n = len(md["state_names"])
+    # MUFU (SFU) ops: exp, log, sqrt and the reciprocal of every division, plus the
+    # exponential of the GRL update; FP32 pipe ops: adds, muls, the multiply of
+    # every division/exp, and ~10 ops of the phi1 update per state
+    sfu = lin["exp"] + lin["log"] + lin["sqrt"] + lin["div"] + n
+    fp = lin["add"] + lin["mul"] + lin["div"] + lin["exp"] + 10 * n
+    sm_clock = 1.965e9
+    sfu_peak = 148 * 16 * sm_clock          # 16 MUFU results / clk / SM
+    fma_peak = 148 * 128 * sm_clock         # 128 FP32 lanes / clk / SM (ops, FMA = 1 op)
+    sfu_rate = sfu * value_fp32
+    fp_rate = fp * value_fp32
+    hbm_bytes = n_nodes * (2 * n * 8 + 4 * 8)  # states in+out, field params in, per launch
+    return dict(
+        bound="sfu",
+        achieved=sfu_rate / 1e9, peak=sfu_peak / 1e9, unit="Gop/s (MUFU)", frac=sfu_rate / sfu_peak,
+        traffic=None,
+        per_cell_step={"sfu_ops": sfu, "fp32_ops": fp},
+        fp32_pipe={"achieved": fp_rate / 1e12, "peak": fma_peak / 1e12, "unit": "Top/s",
+                   "frac": fp_rate / fma_peak},
+        hbm={"achieved_gbs": hbm_bytes / (ms_per_step / 1e3) / 1e9, "algorithmic_bytes_per_launch": hbm_bytes},
+        peak_source="nominal B200: 148 SMs x (16 MUFU | 128 FP32) per clk x 1.965 GHz (no CUDA-core peak "
+                    "in MEASURED_PEAKS.json)",
+    )
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own solvers (oracle/_ref) on a node sample
+# ---------------------------------------------------------------------------
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_sample(target_s=15.0):
+    """Time the reference ODESystemSolver (GRL1, OpenMP over nodes) on a
+    seeded node subset for one 10 ms interval; returns cell-steps/s."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from goss_b200 import models
+
+    vdir = models.find_variant(MODEL, FIELDS)
+    md = json.loads((vdir / "model.json").read_text())
+    threads = cpu_threads()
+    kind = "reference"
+    if pyoracle.ref_available() and (pyoracle.REFDIR / vdir.name / "libplugin.so").exists():
+        def make(nodes):
+            om = pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
+            r = pyoracle.RefSystem(pyoracle.REFDIR / vdir.name / "libplugin.so", md["class_name"], "GRL1", nodes,
+                                   om.solver_params("GRL1", ldt=LDT))
+            _, y0, fp = inputs(nodes)
+            r.set_states(y0)
+            r.set_field_parameters(fp)
+            r.set_num_threads(threads)
+            return r, (lambda t: r.forward(t, INTERVAL))
+    else:
+        kind = "port"
+
+        def make(nodes):
+            om = pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
+            o = pyoracle.OracleSystem(om, "GRL1", nodes, ldt=LDT)
+            _, y0, fp = inputs(nodes)
+            o.states[:] = y0
+            o.field_params[:] = fp
+            return o, (lambda t: o.forward(t, INTERVAL, threads=threads))
+    steps = int(round(INTERVAL / LDT))
+    # calibrate on a small sample, then size the sample to ~target_s
+    nodes = max(threads * 8, 256)
+    obj, fwd = make(nodes)
+    t0 = time.perf_counter()
+    fwd(0.0)
+    dt = time.perf_counter() - t0
+    rate = nodes * steps / dt
+    nodes = int(min(max(rate * target_s / steps, nodes), N_NODES))
+    nodes = max(threads, nodes // threads * threads)
+    obj, fwd = make(nodes)
+    t0 = time.perf_counter()
+    fwd(0.0)
+    dt = time.perf_counter() - t0
+    return dict(value=nodes * steps / dt, unit="cell-steps/s", cores=threads, kind=kind,
+                sample=f"{nodes} seeded nodes of the workload x one 10 ms interval (1000 GRL1 steps), "
+                       f"FP64, {threads} OpenMP threads, {dt:.1f} s")
+
+
+def main():
+    args = _args()
+    if args.profile:
+        profile_run(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    config = {"workload": "tentusscher_panfilov_2006_M_cell GRL1 dt=0.01ms, 1,048,576 nodes per GPU, "
+                          "4 lognormal field parameters, 10 ms per step",
+              "model": MODEL, "solver": "GRL1", "nodes_per_gpu": args.nodes, "internal_dt_ms": LDT,
+              "interval_ms": INTERVAL, "global_batch": args.nodes * world,
+              "parallelism": f"node shards x{world}", "l2": "inputs larger than L2 (159 MB FP64 states)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        res = reference_sample()
+        steps_done = 0
+        line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": config, "impl": "reference",
+                "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": res["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        del steps_done
+        print(json.dumps(line))
+        return
+
+    dist = None
+    if world > 1:
+        import torch.distributed as _dist
+        from datetime import timedelta
+
+        _dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = _dist
+    res, md = run_gpu(args, rank, world, dist)
+    cpu = None
+    if rank == 0 and world == 1:
+        try:
+            cpu = reference_sample()
+        except Exception as exc:  # the baseline is reported, never the target
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": cpu_threads(), "kind": "reference",
+                   "sample": f"failed: {exc}"}
+    if rank == 0:
+        rl = roofline(md, res["value"] / world, res["ms_per_step"], args.nodes)
+        line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 states)",
+                "data": "synthetic (seeded)", "config": config, "roofline": rl, "cpu_baseline": cpu,
+                "e2e": res["e2e"], "gpu_launches": args.steps, "clocks": res["clocks"],
+                "fp64": {"value": res["fp64_value"], "fp32_over_fp64": res["fp32_over_fp64"],
+                         "v_max_rel_err_fp32_vs_fp64": res["v_max_rel_err_fp32_vs_fp64"]},
+                "state_max_rel_err_fp32_vs_fp64": res.get("state_max_rel_err_fp32_vs_fp64")}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -27,6 +27,7 @@ SHIPPED: List[Dict] = [
          field_parameters=["g_Kr", "g_Na", "g_Ks"]),
     dict(name="fitzhughnagumo", ode="tests/fitzhughnagumo.ode", field_parameters=[]),
     dict(name="fitzhughnagumo", ode="tests/fitzhughnagumo.ode", field_parameters=["a", "b"]),
+    dict(name="fitzhughnagumo", ode="tests/fitzhughnagumo.ode", field_parameters=[], monitored=["p_42", "p_V"]),
     dict(name="oscilator", ode="tests/oscilator.ode", field_parameters=[]),
     dict(name="oscilator", ode="tests/oscilator.ode", field_parameters=["a", "b"]),
     dict(name="beeler_reuter_1977", ode="cpp/tests/beeler_reuter_1977.ode", field_parameters=[]),

@@ -11,6 +11,7 @@ struct Beeler_reuter_1977 {
   static constexpr int num_states = 8;
   static constexpr int num_params = 10;
   static constexpr int num_field_params = 0;
+  static constexpr int num_monitored = 0;
 
   // values = f(y, time)
   template <typename T>

@@ -11,6 +11,7 @@ struct Fitzhughnagumo {
   static constexpr int num_states = 2;
   static constexpr int num_params = 11;
   static constexpr int num_field_params = 0;
+  static constexpr int num_monitored = 0;
 
   // values = f(y, time)
   template <typename T>

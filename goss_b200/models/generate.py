@@ -23,8 +23,9 @@ def main() -> int:
     for entry in SHIPPED:
         model = load_ode(ref / entry["ode"])
         assert model.name == entry["name"], (model.name, entry["name"])
-        ident = variant_id(model, entry["field_parameters"])
-        md = write_variant(model, HERE / ident, field_parameters=entry["field_parameters"])
+        mon = entry.get("monitored", [])
+        ident = variant_id(model, entry["field_parameters"], mon)
+        md = write_variant(model, HERE / ident, field_parameters=entry["field_parameters"], monitored=mon)
         print(f"{ident}: {len(md['state_names'])} states, {len(md['parameter_names'])} parameters, "
               f"field parameters {md['field_parameter_names']}")
     return 0

@@ -184,7 +184,7 @@ class ODE:
         batch = np.repeat(y[None, :], n + 1, axis=0)
         batch[np.arange(1, n + 1), np.arange(n)] += deltas
         f = self._eval(0, batch, time)
-        return (f[1:].T - f[0][:, None]) / deltas[None, :]
+        return np.ascontiguousarray((f[1:].T - f[0][:, None]) / deltas[None, :])
 
     def lu_factorize(self, mat: np.ndarray) -> None:
         """In place LU Factorize matrix (jacobian)"""

