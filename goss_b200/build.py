@@ -9,6 +9,7 @@ Builds are incremental: a target is rebuilt when any of its sources is newer.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -38,11 +39,26 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the goss_b200 CUDA extensions cannot be built")
 
 
-def _stale(target: Path, deps: Iterable[Path]) -> bool:
-    if not target.exists():
+def _digest(deps: Iterable[Path], flags: Iterable[str] = ()) -> str:
+    h = hashlib.sha1()
+    for d in deps:
+        h.update(str(d.name).encode())
+        h.update(d.read_bytes() if d.exists() else b"<missing>")
+    h.update(" ".join(flags).encode())
+    return h.hexdigest()
+
+
+def _stale(target: Path, deps: Iterable[Path], flags: Iterable[str] = ()) -> bool:
+    """A target is stale when it is missing or its sources' content changed
+    (content hashes, not mtimes, so copies of the tree do not rebuild)."""
+    stamp = target.with_name(target.name + ".sha1")
+    if not target.exists() or not stamp.exists():
         return True
-    t = target.stat().st_mtime
-    return any(d.exists() and d.stat().st_mtime > t for d in deps)
+    return stamp.read_text().strip() != _digest(deps, flags)
+
+
+def _stamp(target: Path, deps: Iterable[Path], flags: Iterable[str] = ()) -> None:
+    target.with_name(target.name + ".sha1").write_text(_digest(deps, flags) + "\n")
 
 
 def _run(cmd: List[str], cwd: Optional[Path] = None) -> None:
@@ -59,6 +75,7 @@ def build_runtime(force: bool = False) -> Path:
         tmp = RUNTIME_SO.with_suffix(".so.tmp")
         _run([nvcc(), *ARCH, *COMMON, "-shared", str(src), "-o", str(tmp)])
         os.replace(tmp, RUNTIME_SO)
+        _stamp(RUNTIME_SO, deps)
     return RUNTIME_SO
 
 
@@ -71,11 +88,12 @@ def build_variant(vdir: Path, force: bool = False, extra_flags: Optional[List[st
     """Compile one variant directory into ``libgoss_model.so``."""
     vdir = Path(vdir)
     out = vdir / "libgoss_model.so"
-    if force or _stale(out, variant_deps(vdir)):
+    flags = ["--use_fast_math"] + (extra_flags or [])
+    if force or _stale(out, variant_deps(vdir), flags):
         tmp = out.with_suffix(f".so.{os.getpid()}.tmp")
-        flags = ["--use_fast_math", f"-I{vdir}"] + (extra_flags or [])
-        _run([nvcc(), *ARCH, *COMMON, *flags, "-shared", str(vdir / "module.cu"), "-o", str(tmp)])
+        _run([nvcc(), *ARCH, *COMMON, *flags, f"-I{vdir}", "-shared", str(vdir / "module.cu"), "-o", str(tmp)])
         os.replace(tmp, out)
+        _stamp(out, variant_deps(vdir), flags)
     return out
 
 
