@@ -123,6 +123,9 @@ _PROTOS = {
     "goss_system_device_states": (C.c_int, [_sys, C.POINTER(_dp), C.POINTER(C.c_uint64)]),
     "goss_system_device_field_params": (C.c_int, [_sys, C.POINTER(_dp), C.POINTER(C.c_uint64)]),
     "goss_system_set_stream": (C.c_int, [_sys, C.c_void_p]),
+    "goss_model_eval_noalloc": (C.c_int, [_desc, C.c_int32, C.c_int32, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_uint64, C.c_void_p, C.c_void_p]),
+    "goss_model_eval_noalloc_capacity": (C.c_uint64, []),
     "goss_lu_factorize": (C.c_int, [C.c_uint32, _dp]),
     "goss_forward_backward_subst": (C.c_int, [C.c_uint32, _dp, _dp, _dp]),
     "goss_model_eval": (C.c_int, [_desc, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, C.c_uint64, _dp, C.c_int32]),

@@ -793,6 +793,144 @@ GOSS_API int goss_system_solve(goss_system* s, double* field_states, const doubl
     return rc;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched evaluation without any device allocation
+// ---------------------------------------------------------------------------
+// Some callers cannot let a library call cudaMalloc: a process whose GPU
+// memory is owned by another allocator (a framework's caching allocator that
+// has reserved the device, or a fixed memory budget) would see the call fail,
+// block on the allocator's synchronisation, or fragment its pool.  For them
+// goss_model_eval_noalloc keeps its working arrays (the component-major
+// copies of the states, field parameters and results) in this fixed device
+// array instead.  Every GPU on which this library is used holds the array
+// until the process exits.
+#define GOSS_NOALLOC_SCRATCH_DOUBLES (2u * 1024u * 1024u) /* 16 MiB */
+static __device__ __align__(256) double g_eval_scratch[GOSS_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_eval_scratch on the current device.  In host code the
+// symbol is only a host-side stand-in, so the address is looked up once per
+// device with that device current and cached.
+int noalloc_scratch(double** out)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_eval_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(nullptr, GOSS_ERR_CUDA, "cudaGetSymbolAddress of the evaluation scratch failed: %s",
+                        cudaGetErrorString(e));
+        g_scratch_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return 0;
+}
+
+struct RowValues {
+    double v[32];
+};
+
+// dst[r*ld + node] = vals.v[r] for every node < N (values passed by value)
+__global__ void fill_rows_const_kernel(double* __restrict__ dst, uint64_t ld, uint32_t N, uint32_t k, RowValues vals)
+{
+    const uint64_t total = (uint64_t)N * k;
+    for (uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(idx / N), node = (uint32_t)(idx % N);
+        dst[(uint64_t)r * ld + node] = vals.v[r];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+GOSS_API uint64_t goss_model_eval_noalloc_capacity(void) { return GOSS_NOALLOC_SCRATCH_DOUBLES; }
+
+GOSS_API int goss_model_eval_noalloc(const goss_model_desc* m, int32_t what, int32_t precision, const double* params,
+                                     const double* states, const double* field_params, const double* times,
+                                     uint64_t count, double* out, void* stream)
+{
+    if (!m || !states || !times || !out)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL argument");
+    if (what < 0 || what > 2)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "what must be 0 (rhs), 1 (linearized) or 2 (monitored)");
+    if (what == 2 && m->num_monitored == 0)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "No monitored in the '%s' model.", m->name);
+    if (count == 0)
+        return 0;
+    const uint32_t n = m->num_states, nfp = m->num_field_parameters;
+    if (nfp > 32 && !field_params)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "models with more than 32 field parameters need field_params");
+    const uint32_t width = what == 0 ? n : (what == 1 ? 2 * n : m->num_monitored);
+    const uint64_t ld = round_up(count, 32);
+    const uint64_t need = (uint64_t)(n + nfp + width) * ld;
+    if (count > 0xffffffffull || need > GOSS_NOALLOC_SCRATCH_DOUBLES)
+        return fail(nullptr, GOSS_ERR_ARGUMENT,
+                    "goss_model_eval_noalloc: %llu states of model '%s' need %llu scratch doubles; the fixed "
+                    "scratch holds %u (at most %llu states of this model)",
+                    (unsigned long long)count, m->name, (unsigned long long)need, GOSS_NOALLOC_SCRATCH_DOUBLES,
+                    (unsigned long long)(GOSS_NOALLOC_SCRATCH_DOUBLES / (n + nfp + width) / 32 * 32));
+    double* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc)
+        return rc;
+    double* d_states = scratch;                       // [n][ld]
+    double* d_fp = scratch + (uint64_t)n * ld;        // [nfp][ld]
+    double* d_out = d_fp + (uint64_t)nfp * ld;        // [width][ld]
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint32_t N = (uint32_t)count;
+    scatter_kernel<<<grid_for(count * n), 256, 0, st>>>(d_states, ld, states, N, n, nullptr, 1);
+    if (nfp) {
+        if (field_params) {
+            scatter_kernel<<<grid_for(count * nfp), 256, 0, st>>>(d_fp, ld, field_params, N, nfp, nullptr, 1);
+        } else {
+            RowValues vals{};
+            for (uint32_t k = 0; k < nfp; ++k)
+                vals.v[k] = params ? params[m->field_parameter_indices[k]]
+                                   : m->default_parameters[m->field_parameter_indices[k]];
+            fill_rows_const_kernel<<<grid_for(count * nfp), 256, 0, st>>>(d_fp, ld, N, nfp, vals);
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "layout kernel launch failed: %s", cudaGetErrorString(e));
+    goss_eval_launch L{};
+    L.what = what;
+    L.precision = precision;
+    L.num_nodes = N;
+    L.ld = ld;
+    L.states = d_states;
+    L.field_params = nfp ? d_fp : nullptr;
+    L.times = times;
+    L.out = d_out;
+    L.params = params ? params : m->default_parameters;
+    L.stream = stream;
+    rc = m->eval(&L);
+    if (rc)
+        return fail(nullptr, rc, "model evaluation launch failed");
+    gather_kernel<<<grid_for(count * width), 256, 0, st>>>(out, d_out, ld, N, width, nullptr, 1);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "goss_model_eval_noalloc failed: %s", cudaGetErrorString(e));
+    return 0;
+}
+
 // ODE::lu_factorize (ODE.cpp:69-100): Doolittle LU without pivoting.
 GOSS_API int goss_lu_factorize(uint32_t un, double* mat)
 {

@@ -226,6 +226,32 @@ GOSS_API int goss_model_eval(const goss_model_desc* model, int32_t what, int32_t
                              const double* states, const double* field_params, const double* times, uint64_t count,
                              double* out, int32_t device);
 
+/* Batched model evaluation that allocates no device memory.  No counterpart
+ * in the reference: it exists for callers that must not have a library call
+ * cudaMalloc -- a process whose GPU memory belongs to another allocator (a
+ * framework's caching allocator that reserved the device, or a fixed memory
+ * budget), where an allocation would fail, stall on that allocator or
+ * fragment its pool.
+ *
+ * Same arithmetic as goss_model_eval, but every pointer is DEVICE memory on
+ * the current device: states [count][n], field_params [count][nfp] (NULL:
+ * the parameter values), times [count], out [count][width] with width n
+ * (what = 0), 2n (what = 1: linear then rhs) or num_monitored (what = 2).
+ * params is a HOST array of num_parameters values (NULL: defaults).
+ *
+ * Working arrays live in one fixed file-scope device array of
+ * goss_model_eval_noalloc_capacity() doubles (16 MiB) that every GPU using
+ * this library keeps until the process exits; (n + nfp + width) * count,
+ * with count rounded up to 32, must fit or the call fails with
+ * GOSS_ERR_ARGUMENT.  The first call on a device looks up that array's
+ * device address (make the first call before any stream capture).  All calls
+ * share the array, so calls that overlap on the GPU (other streams, other
+ * threads) race; the call synchronises `stream` before it returns. */
+GOSS_API int goss_model_eval_noalloc(const goss_model_desc* model, int32_t what, int32_t precision,
+                                     const double* params, const double* states, const double* field_params,
+                                     const double* times, uint64_t count, double* out, void* stream);
+GOSS_API uint64_t goss_model_eval_noalloc_capacity(void);
+
 /* Single-matrix helpers of the ODE plugin interface, on the host (the
  * reference's ODE::lu_factorize / ODE::forward_backward_subst, ODE.cpp:69-132):
  * in-place LU without pivoting of a row-major n x n matrix, and the solve
