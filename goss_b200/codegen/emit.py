@@ -25,6 +25,7 @@ import sympy as sp
 
 from .ir import CONST, FIELD, STATE, TIME_CLS, Assign, ModelIR, Output, Program, count_ops
 from .odeparse import TIME
+from .hoist import ConstantFolder
 from .printer import CPrinter, c_double
 
 _RESERVED = {
@@ -322,6 +323,10 @@ class ModelSource:
                         return f"double(F[{j}])" if ctx_double else f"F[{j}]"
                     k = self.pindex[n]
                     return f"PD[{k}]" if ctx_double else f"P[{k}]"
+                if n.startswith("__c"):
+                    # derived constant, stored after the parameters
+                    k = len(self.params) + int(n[3:])
+                    return f"PD[{k}]" if ctx_double else f"P[{k}]"
                 # intermediate: its declared type follows its class
                 cls = self._cls_of(n)
                 if cls == TIME_CLS and not ctx_double:
@@ -360,8 +365,57 @@ class ModelSource:
             t = "double" if b.cls == TIME_CLS else "T"
             return f"const {t} v_{b.name}"
         out = lambda b: f"{b.array}[{b.index}]"
-        p2 = Program(prog.name, prog.body, None)
+        p2 = Program(prog.name, self._fold(prog).body, None)
         return _body_lines(p2, pr_for, decl, out)
+
+    # -- parameter-only sub-expressions become derived constants ----------------
+    @property
+    def folder(self) -> ConstantFolder:
+        if not hasattr(self, "_folder"):
+            uniform = {self.model.sym(p) for p in self.params if p not in self.findex}
+            const_inter = {}
+            for prog in (self.rhs, self.lin) + ((self.mon,) if self.mon else ()):
+                for b in prog.assigns():
+                    if b.cls == CONST:
+                        const_inter[self.model.sym(b.name)] = b.expr
+            self._folder = ConstantFolder(uniform, const_inter)
+            self._const_inter = const_inter
+        return self._folder
+
+    def _fold(self, prog: Program) -> Program:
+        f = self.folder
+        body = []
+        for b in prog.body:
+            if isinstance(b, Assign):
+                if b.cls == CONST:
+                    continue
+                body.append(Assign(b.name, f(b.expr), b.cls))
+            else:
+                body.append(Output(b.array, b.index, f(b.expr)))
+        return Program(prog.name, body, None)
+
+    def _derived_host_lines(self) -> List[str]:
+        """Host code filling C[k] with the derived constants from P."""
+        def sym(s):
+            n = s.name
+            if n in self.pindex:
+                return f"P[{self.pindex[n]}]"
+            return f"v_{n}"
+        pr = CPrinter(sym)
+        lines = []
+        order = [b for prog in (self.rhs, self.lin) + ((self.mon,) if self.mon else ())
+                 for b in prog.assigns() if b.cls == CONST]
+        seen = set()
+        for b in order:
+            if b.name in seen:
+                continue
+            seen.add(b.name)
+            lines.append(f"const double v_{b.name} = {pr(b.expr)};")
+        for k, (s, e) in enumerate(self.folder.derived):
+            lines.append(f"C[{k}] = {pr(e)};")
+        if not seen:
+            pass
+        return lines
 
     def emit_device(self) -> str:
         cls = model_class_name(self.name)
@@ -395,6 +449,20 @@ class ModelSource:
         L.append("  }")
         L.append("")
         lin_full = self.ir.linearized_program(split=False)
+        rhs_lines = self._dev_body(self.rhs)
+        lin_lines = self._dev_body(lin_full)
+        mon_lines = self._dev_body(self.mon) if self.mon is not None else []
+        nder = len(self.folder.derived)
+        L.insert(L.index(f"  static constexpr int num_monitored = {len(self.ir.monitored)};") + 1,
+                 f"  static constexpr int num_derived = {nder};")
+        L.append("  // derived constants: parameter-only sub-expressions, evaluated once per")
+        L.append("  // launch on the host in FP64 and stored after the parameters")
+        L.append("  static void derived(const double* P, double* C)")
+        L.append("  {")
+        L += ["    " + x for x in self._derived_host_lines()]
+        L.append("    (void)P; (void)C;")
+        L.append("  }")
+        L.append("")
         L.append("  // rhs = f(y, time), linear[i] = d f_i / d y_i")
         L.append("  template <typename T>")
         L.append(f"  __device__ static __forceinline__ void linearized({sig}, T* __restrict__ linear, T* __restrict__ rhs)")

@@ -34,9 +34,22 @@ constexpr double kGossEps = 3.0e-16;  // GOSS_EPS, cpp/goss/constants.h:25
 template <class M>
 struct Dims {
     static constexpr int n = M::num_states;
-    static constexpr int np = M::num_params > 0 ? M::num_params : 1;
+    // parameter block: the model parameters followed by the derived constants
+    static constexpr int npd = M::num_params + M::num_derived;
+    static constexpr int np = npd > 0 ? npd : 1;
     static constexpr int nfp = M::num_field_params > 0 ? M::num_field_params : 1;
 };
+
+// Fill the FP64 parameter block: parameters, then the model's derived
+// constants computed from them (once per launch, on the host).
+template <class M>
+inline void parameter_block(const double* params, double (&out)[Dims<M>::np])
+{
+    for (int i = 0; i < Dims<M>::np; ++i)
+        out[i] = i < M::num_params ? params[i] : 0.0;
+    if (M::num_derived > 0)
+        M::derived(out, out + M::num_params);
+}
 
 // std::max / std::min semantics (first argument wins ties and NaNs)
 __device__ __forceinline__ double std_max(double a, double b) { return (a < b) ? b : a; }
@@ -119,6 +132,51 @@ __device__ __forceinline__ float grl_increment(float a, float b, float h, float 
     return b * h * phi1f(a * h);
 }
 
+// State accumulators.  FP64 kernels hold each state as a double and update it
+// exactly as the reference does (y = y + increment).  FP32 kernels hold each
+// state as an unevaluated sum hi + lo of two floats ("double-float"): the
+// model reads hi, increments are added with an error-free two-sum and the
+// pair is renormalised, which keeps ~48 significant bits (concentrations such
+// as K_i ~ 138 mM change by less than one float ulp per step) without the
+// FP32<->FP64 conversions that would otherwise compete with the model's
+// exponentials and reciprocals for the MUFU/XU pipe on every step.
+template <typename T>
+struct Acc;
+
+template <>
+struct Acc<double> {
+    double y;
+    __device__ __forceinline__ void load(double v) { y = v; }
+    __device__ __forceinline__ double store() const { return y; }
+    __device__ __forceinline__ double value() const { return y; }
+    __device__ __forceinline__ double plus(double d) const { return y + d; }
+    __device__ __forceinline__ void add(double d) { y = y + d; }
+};
+
+template <>
+struct Acc<float> {
+    float hi, lo;
+    __device__ __forceinline__ void load(double v)
+    {
+        hi = float(v);
+        lo = float(v - double(hi));
+    }
+    __device__ __forceinline__ double store() const { return double(hi) + double(lo); }
+    __device__ __forceinline__ float value() const { return hi; }
+    __device__ __forceinline__ float plus(float d) const { return hi + (lo + d); }
+    __device__ __forceinline__ void add(float d)
+    {
+        // two-sum: s + err == hi + d exactly
+        const float s = __fadd_rn(hi, d);
+        const float bb = __fadd_rn(s, -hi);
+        const float err = __fadd_rn(__fadd_rn(hi, -__fadd_rn(s, -bb)), __fadd_rn(d, -bb));
+        const float l = __fadd_rn(lo, err);
+        // renormalise (|s| >= |l|): hi + lo == s + l
+        hi = __fadd_rn(s, l);
+        lo = __fadd_rn(l, -__fadd_rn(hi, -s));
+    }
+};
+
 template <class M, typename T, Explicit S>
 __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ ExplicitArgs<M, T> a)
 {
@@ -126,64 +184,65 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
     const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= a.N)
         return;
-    double y[n];
+    Acc<T> y[n];
 #pragma unroll
     for (int i = 0; i < n; ++i)
-        y[i] = a.states[i * a.ld + node];
+        y[i].load(a.states[i * a.ld + node]);
     T F[Dims<M>::nfp];
     load_field<M, T>(a.fparams, a.ld, node, F);
 
     const double ldt = a.ldt;
     const T h = T(ldt);
+    const T hh = T(0.5 * ldt);
     const T delta = T(a.delta);
     double lt = a.t;
     for (uint64_t step = 0; step < a.nsteps; ++step) {
         T yt[n];
 #pragma unroll
         for (int i = 0; i < n; ++i)
-            yt[i] = T(y[i]);
+            yt[i] = y[i].value();
         if constexpr (S == Explicit::Euler) {
+            // ExplicitEuler.cpp:80-81
             T f[n];
             M::template rhs<T>(yt, lt, a.P, a.PD, F, f);
 #pragma unroll
             for (int i = 0; i < n; ++i)
-                y[i] += ldt * double(f[i]);
+                y[i].add(h * f[i]);
         } else if constexpr (S == Explicit::RK4) {
-            // RK4.cpp:79-98 with RK4::axpy (RK4.h:70-74).  Stage inputs are
-            // formed in FP64 (y + a*k) and rounded to T; the weighted sum is
+            // RK4.cpp:79-98 with RK4::axpy (RK4.h:70-74); the weighted sum is
             // accumulated in the order k1 + 2 k2 + 2 k3 + k4 of the reference.
-            const double hh = 0.5 * ldt;
             T k[n], sum[n], tmp[n];
             M::template rhs<T>(yt, lt, a.P, a.PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = k[i];
-                tmp[i] = T(y[i] + hh * double(k[i]));
+                tmp[i] = y[i].plus(hh * k[i]);
             }
             M::template rhs<T>(tmp, lt + 0.5 * ldt, a.P, a.PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = sum[i] + T(2.0) * k[i];
-                tmp[i] = T(y[i] + hh * double(k[i]));
+                tmp[i] = y[i].plus(hh * k[i]);
             }
             M::template rhs<T>(tmp, lt + 0.5 * ldt, a.P, a.PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = sum[i] + T(2.0) * k[i];
-                tmp[i] = T(y[i] + ldt * double(k[i]));
+                tmp[i] = y[i].plus(h * k[i]);
             }
             M::template rhs<T>(tmp, lt + ldt, a.P, a.PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = sum[i] + k[i];
-                y[i] += ldt * double(sum[i]) / 6.0;
+                y[i].add(h * sum[i] / T(6.0));
             }
         } else if constexpr (S == Explicit::GRL1) {
+            // GRL1.h:72-84
             T lin[n], rhs[n];
             M::template linearized<T>(yt, lt, a.P, a.PD, F, lin, rhs);
 #pragma unroll
             for (int i = 0; i < n; ++i)
-                y[i] = y[i] + double(grl_increment(lin[i], rhs[i], h, delta));
+                y[i].add(grl_increment(lin[i], rhs[i], h, delta));
         } else {
             // GRL2: GRL2.cpp:78-82.  The reference's branch threshold is a
             // self-initialised local (GRL2.cpp:67) whose -O3 build behaves as 0:
@@ -191,24 +250,21 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
             T lin[n], rhs[n], y2[n];
             M::template linearized<T>(yt, lt, a.P, a.PD, F, lin, rhs);
 #pragma unroll
-            for (int i = 0; i < n; ++i) {
-                if constexpr (sizeof(T) == 8)
-                    y2[i] = y[i] + grl_increment(double(lin[i]), double(rhs[i]), ldt * 0.5, 0.0);
-                else
-                    y2[i] = T(y[i] + double(grl_increment(lin[i], rhs[i], T(ldt * 0.5), T(0))));
-            }
+            for (int i = 0; i < n; ++i)
+                y2[i] = y[i].plus(grl_increment(lin[i], rhs[i], hh, T(0)));
             M::template linearized<T>(y2, lt, a.P, a.PD, F, lin, rhs);
 #pragma unroll
             for (int i = 0; i < n; ++i)
-                y[i] = y[i] + double(grl_increment(lin[i], rhs[i], h, T(0)));
+                y[i].add(grl_increment(lin[i], rhs[i], h, T(0)));
         }
         lt += ldt;
     }
     bool finite = true;
 #pragma unroll
     for (int i = 0; i < n; ++i) {
-        a.states[i * a.ld + node] = y[i];
-        finite = finite && isfinite(y[i]);
+        const double v = y[i].store();
+        a.states[i * a.ld + node] = v;
+        finite = finite && isfinite(v);
     }
     if (!finite) {
         a.node_status[node] |= GOSS_FLAG_NONFINITE;
@@ -809,11 +865,9 @@ inline int launch_explicit(const goss_launch* L)
     a.ldt = L->interval / nsteps;
     a.t = L->t;
     a.delta = L->solver_params->delta;
-    for (int i = 0; i < Dims<M>::np; ++i) {
-        const double v = i < M::num_params ? L->params[i] : 0.0;
-        a.P[i] = T(v);
-        a.PD[i] = v;
-    }
+    parameter_block<M>(L->params, a.PD);
+    for (int i = 0; i < Dims<M>::np; ++i)
+        a.P[i] = T(a.PD[i]);
     const unsigned block = L->block ? L->block : 128;
     const unsigned grid = (L->num_nodes + block - 1) / block;
     if (grid == 0)
@@ -837,8 +891,7 @@ inline int launch_implicit(const goss_launch* L)
     a.interval = L->interval;
     a.sp = *L->solver_params;
     a.max_loop = L->max_loop ? L->max_loop : (1ull << 24);
-    for (int i = 0; i < Dims<M>::np; ++i)
-        a.P[i] = i < M::num_params ? L->params[i] : 0.0;
+    parameter_block<M>(L->params, a.P);
     const unsigned block = L->block ? L->block : 64;
     const unsigned grid = (L->num_nodes + block - 1) / block;
     if (grid == 0)
@@ -884,11 +937,9 @@ inline int launch_eval_t(const goss_eval_launch* L)
     a.ld = L->ld;
     a.N = L->num_nodes;
     a.what = L->what;
-    for (int i = 0; i < Dims<M>::np; ++i) {
-        const double v = i < M::num_params ? L->params[i] : 0.0;
-        a.P[i] = T(v);
-        a.PD[i] = v;
-    }
+    parameter_block<M>(L->params, a.PD);
+    for (int i = 0; i < Dims<M>::np; ++i)
+        a.P[i] = T(a.PD[i]);
     const unsigned block = 128;
     const unsigned grid = (L->num_nodes + block - 1) / block;
     if (grid == 0)

@@ -12,6 +12,7 @@ struct Beeler_reuter_1977 {
   static constexpr int num_params = 10;
   static constexpr int num_field_params = 0;
   static constexpr int num_monitored = 0;
+  static constexpr int num_derived = 7;
 
   // values = f(y, time)
   template <typename T>
@@ -25,7 +26,7 @@ struct Beeler_reuter_1977 {
     const T s_f = y[5];
     const T s_x1 = y[6];
     const T s_V = y[7];
-    const T v_i_Na = ((s_V - ((P[0])))*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
+    const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
     const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
     const T v_alpha_m = (((-T(47.0)) - ((s_V)))/((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0)))));
     const T v_beta_m = (T(0.7095526727489909)*gexp((-(T(0.056)*s_V))));
@@ -44,7 +45,7 @@ struct Beeler_reuter_1977 {
     const T v_beta_x1 = (T(0.0003916464405623223)*gexp((-(T(0.05998800239952009)*s_V)))/(T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V))))));
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
     const T v_i_K1 = ((T(0.0035)*(T(4.6000000000000005) + (T(0.2)*s_V))/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))));
-    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((time - ((PD[8])) - ((PD[6]*floor(((time - ((PD[8])))/PD[6]))))) <= PD[7])) ? PD[4] : 0.0);
+    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     values[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     values[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
     values[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
@@ -52,8 +53,22 @@ struct Beeler_reuter_1977 {
     values[4] = ((v_alpha_d*(T(1.0) - ((s_d)))) - ((v_beta_d*s_d)));
     values[5] = ((v_alpha_f*(T(1.0) - ((s_f)))) - ((v_beta_f*s_f)));
     values[6] = ((v_alpha_x1*(T(1.0) - ((s_x1)))) - ((v_beta_x1*s_x1)));
-    values[7] = ((T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1)))/P[9]);
+    values[7] = (P[14]*(T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1))));
     (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // derived constants: parameter-only sub-expressions, evaluated once per
+  // launch on the host in FP64 and stored after the parameters
+  static void derived(const double* P, double* C)
+  {
+    C[0] = (-(P[0]));
+    C[1] = (-(P[8]));
+    C[2] = (1.0/P[6]);
+    C[3] = (-(P[6]));
+    C[4] = (1.0/P[9]);
+    C[5] = (-(P[3]));
+    C[6] = (-(1.0/P[9]));
+    (void)P; (void)C;
   }
 
   // rhs = f(y, time), linear[i] = d f_i / d y_i
@@ -68,7 +83,7 @@ struct Beeler_reuter_1977 {
     const T s_f = y[5];
     const T s_x1 = y[6];
     const T s_V = y[7];
-    const T v_i_Na = ((s_V - ((P[0])))*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
+    const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
     const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
     const T v_alpha_m = (((-T(47.0)) - ((s_V)))/((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0)))));
     const T v_beta_m = (T(0.7095526727489909)*gexp((-(T(0.056)*s_V))));
@@ -87,7 +102,7 @@ struct Beeler_reuter_1977 {
     const T v_beta_x1 = (T(0.0003916464405623223)*gexp((-(T(0.05998800239952009)*s_V)))/(T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V))))));
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
     const T v_i_K1 = ((T(0.0035)*(T(4.6000000000000005) + (T(0.2)*s_V))/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))));
-    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((time - ((PD[8])) - ((PD[6]*floor(((time - ((PD[8])))/PD[6]))))) <= PD[7])) ? PD[4] : 0.0);
+    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     rhs[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     rhs[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
     rhs[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
@@ -95,7 +110,7 @@ struct Beeler_reuter_1977 {
     rhs[4] = ((v_alpha_d*(T(1.0) - ((s_d)))) - ((v_beta_d*s_d)));
     rhs[5] = ((v_alpha_f*(T(1.0) - ((s_f)))) - ((v_beta_f*s_f)));
     rhs[6] = ((v_alpha_x1*(T(1.0) - ((s_x1)))) - ((v_beta_x1*s_x1)));
-    rhs[7] = ((T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1)))/P[9]);
+    rhs[7] = (P[14]*(T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1))));
     linear[0] = ((-(v_alpha_m)) - ((v_beta_m)));
     linear[1] = ((-(v_alpha_h)) - ((v_beta_h)));
     linear[2] = ((-(v_alpha_j)) - ((v_beta_j)));
@@ -103,14 +118,14 @@ struct Beeler_reuter_1977 {
     linear[5] = ((-(v_alpha_f)) - ((v_beta_f)));
     linear[6] = ((-(v_alpha_x1)) - ((v_beta_x1)));
     const T v_dE_s_dCai = (-(T(13.0287)/s_Cai));
-    const T v_di_s_dCai = (-(s_d*v_dE_s_dCai*s_f*P[3]));
+    const T v_di_s_dCai = (P[15]*s_d*v_dE_s_dCai*s_f);
     const T v_dV_eff_1_dV = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0));
     const T v_di_K1_dV = ((T(0.0007000000000000001)/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.016779896026542326)*gexp((T(0.04)*s_V))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))*((-(T(0.3332454995075077)*gexp((T(0.04)*s_V)))) - ((T(5.552628147100417)*gexp((T(0.08)*s_V)))))/(((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V)))))) - ((T(0.00028000000000000003)*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V))*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))))));
     const T v_di_Na_dV = (P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)));
     const T v_di_s_dV = (s_d*s_f*P[3]);
     const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))))));
     linear[3] = ((-T(0.07)) - ((T(0.01)*v_di_s_dCai)));
-    linear[7] = ((-(v_di_K1_dV/P[9])) - ((v_di_Na_dV/P[9])) - ((v_di_s_dV/P[9])) - ((v_di_x1_dV/P[9])));
+    linear[7] = ((P[16]*v_di_K1_dV) + (P[16]*v_di_Na_dV) + (P[16]*v_di_s_dV) + (P[16]*v_di_x1_dV));
     (void)time; (void)P; (void)PD; (void)F;
   }
 };

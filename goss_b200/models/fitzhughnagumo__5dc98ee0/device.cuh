@@ -12,6 +12,7 @@ struct Fitzhughnagumo {
   static constexpr int num_params = 11;
   static constexpr int num_field_params = 2;
   static constexpr int num_monitored = 0;
+  static constexpr int num_derived = 8;
 
   // values = f(y, time)
   template <typename T>
@@ -19,13 +20,28 @@ struct Fitzhughnagumo {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_V_amp = (P[0] - ((P[1])));
-    const T v_V_th = (P[1] + (v_V_amp*F[0]));
-    const T v_I = ((-(P[5]*s_s*(s_V - ((P[1])))/v_V_amp)) + (P[4]*(s_V - ((P[1])))*(s_V - ((v_V_th)))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)));
-    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp(((5.0*time) - ((5.0*PD[10]))))))))/(1.0 + exp(((5.0*time) - ((5.0*PD[8])) - ((5.0*PD[10]))))));
+    const T v_V_th = (P[1] + (P[11]*F[0]));
+    const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     values[0] = (v_I + T(v_i_Stim));
-    values[1] = (F[1]*(s_V - ((P[1])) - ((P[6]*s_s))));
+    values[1] = (F[1]*(s_V + P[12] + (P[17]*s_s)));
     (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // derived constants: parameter-only sub-expressions, evaluated once per
+  // launch on the host in FP64 and stored after the parameters
+  static void derived(const double* P, double* C)
+  {
+    const double v_V_amp = (P[0] - ((P[1])));
+    C[0] = v_V_amp;
+    C[1] = (-(P[1]));
+    C[2] = (-(P[5]/v_V_amp));
+    C[3] = (P[4]/(v_V_amp*v_V_amp));
+    C[4] = ((-(5.0*P[8])) - ((5.0*P[10])));
+    C[5] = (-(5.0*P[10]));
+    C[6] = (-(P[6]));
+    C[7] = (-(P[4]/(v_V_amp*v_V_amp)));
+    (void)P; (void)C;
   }
 
   // rhs = f(y, time), linear[i] = d f_i / d y_i
@@ -34,14 +50,13 @@ struct Fitzhughnagumo {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_V_amp = (P[0] - ((P[1])));
-    const T v_V_th = (P[1] + (v_V_amp*F[0]));
-    const T v_I = ((-(P[5]*s_s*(s_V - ((P[1])))/v_V_amp)) + (P[4]*(s_V - ((P[1])))*(s_V - ((v_V_th)))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)));
-    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp(((5.0*time) - ((5.0*PD[10]))))))))/(1.0 + exp(((5.0*time) - ((5.0*PD[8])) - ((5.0*PD[10]))))));
+    const T v_V_th = (P[1] + (P[11]*F[0]));
+    const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     rhs[0] = (v_I + T(v_i_Stim));
-    rhs[1] = (F[1]*(s_V - ((P[1])) - ((P[6]*s_s))));
-    linear[1] = (-(F[1]*P[6]));
-    const T v_dI_dV = ((-(P[5]*s_s/v_V_amp)) + (P[4]*(s_V - ((P[1])))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)) + (P[4]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)) - ((P[4]*(s_V - ((P[1])))*(s_V - ((v_V_th)))/(v_V_amp*v_V_amp))));
+    rhs[1] = (F[1]*(s_V + P[12] + (P[17]*s_s)));
+    linear[1] = (P[17]*F[1]);
+    const T v_dI_dV = ((P[13]*s_s) + (P[14]*(s_V + P[12])*(P[0] - ((s_V)))) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))) + (P[18]*(s_V + P[12])*(s_V - ((v_V_th)))));
     linear[0] = v_dI_dV;
     (void)time; (void)P; (void)PD; (void)F;
   }

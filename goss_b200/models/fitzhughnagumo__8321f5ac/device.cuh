@@ -12,6 +12,7 @@ struct Fitzhughnagumo {
   static constexpr int num_params = 11;
   static constexpr int num_field_params = 0;
   static constexpr int num_monitored = 2;
+  static constexpr int num_derived = 10;
 
   // values = f(y, time)
   template <typename T>
@@ -19,13 +20,31 @@ struct Fitzhughnagumo {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_V_amp = (P[0] - ((P[1])));
-    const T v_V_th = (P[1] + (v_V_amp*P[2]));
-    const T v_I = ((-(P[5]*s_s*(s_V - ((P[1])))/v_V_amp)) + (P[4]*(s_V - ((P[1])))*(s_V - ((v_V_th)))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)));
-    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp(((5.0*time) - ((5.0*PD[10]))))))))/(1.0 + exp(((5.0*time) - ((5.0*PD[8])) - ((5.0*PD[10]))))));
+    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     values[0] = (v_I + T(v_i_Stim));
-    values[1] = (P[3]*(s_V - ((P[1])) - ((P[6]*s_s))));
+    values[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
     (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // derived constants: parameter-only sub-expressions, evaluated once per
+  // launch on the host in FP64 and stored after the parameters
+  static void derived(const double* P, double* C)
+  {
+    const double v_V_amp = (P[0] - ((P[1])));
+    const double v_V_th = (P[1] + (v_V_amp*P[2]));
+    const double v_p_42 = 42.0;
+    C[0] = (-(P[1]));
+    C[1] = (-(P[5]/v_V_amp));
+    C[2] = (-(v_V_th));
+    C[3] = (P[4]/(v_V_amp*v_V_amp));
+    C[4] = ((-(5.0*P[8])) - ((5.0*P[10])));
+    C[5] = (-(5.0*P[10]));
+    C[6] = (-(P[6]));
+    C[7] = (-(P[3]*P[6]));
+    C[8] = (-(P[4]/(v_V_amp*v_V_amp)));
+    C[9] = v_p_42;
+    (void)P; (void)C;
   }
 
   // rhs = f(y, time), linear[i] = d f_i / d y_i
@@ -34,14 +53,12 @@ struct Fitzhughnagumo {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_V_amp = (P[0] - ((P[1])));
-    const T v_V_th = (P[1] + (v_V_amp*P[2]));
-    const T v_I = ((-(P[5]*s_s*(s_V - ((P[1])))/v_V_amp)) + (P[4]*(s_V - ((P[1])))*(s_V - ((v_V_th)))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)));
-    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp(((5.0*time) - ((5.0*PD[10]))))))))/(1.0 + exp(((5.0*time) - ((5.0*PD[8])) - ((5.0*PD[10]))))));
+    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     rhs[0] = (v_I + T(v_i_Stim));
-    rhs[1] = (P[3]*(s_V - ((P[1])) - ((P[6]*s_s))));
-    linear[1] = (-(P[3]*P[6]));
-    const T v_dI_dV = ((-(P[5]*s_s/v_V_amp)) + (P[4]*(s_V - ((P[1])))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)) + (P[4]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))/(v_V_amp*v_V_amp)) - ((P[4]*(s_V - ((P[1])))*(s_V - ((v_V_th)))/(v_V_amp*v_V_amp))));
+    rhs[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
+    linear[1] = P[18];
+    const T v_dI_dV = ((P[12]*s_s) + (P[14]*(s_V + P[11])*(P[0] - ((s_V)))) + (P[14]*(s_V + P[13])*(P[0] - ((s_V)))) + (P[19]*(s_V + P[11])*(s_V + P[13])));
     linear[0] = v_dI_dV;
     (void)time; (void)P; (void)PD; (void)F;
   }
@@ -51,9 +68,8 @@ struct Fitzhughnagumo {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_p_42 = T(42.0);
     const T v_p_V = s_V;
-    monitored[0] = v_p_42;
+    monitored[0] = P[20];
     monitored[1] = v_p_V;
     (void)time; (void)P; (void)PD; (void)F;
   }

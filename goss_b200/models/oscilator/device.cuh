@@ -12,6 +12,7 @@ struct Oscilator {
   static constexpr int num_params = 2;
   static constexpr int num_field_params = 0;
   static constexpr int num_monitored = 0;
+  static constexpr int num_derived = 1;
 
   // values = f(y, time)
   template <typename T>
@@ -19,9 +20,17 @@ struct Oscilator {
   {
     const T s_x = y[0];
     const T s_y = y[1];
-    values[0] = (-(P[0]*s_y));
+    values[0] = (P[2]*s_y);
     values[1] = (P[1]*s_x);
     (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // derived constants: parameter-only sub-expressions, evaluated once per
+  // launch on the host in FP64 and stored after the parameters
+  static void derived(const double* P, double* C)
+  {
+    C[0] = (-(P[0]));
+    (void)P; (void)C;
   }
 
   // rhs = f(y, time), linear[i] = d f_i / d y_i
@@ -30,7 +39,7 @@ struct Oscilator {
   {
     const T s_x = y[0];
     const T s_y = y[1];
-    rhs[0] = (-(P[0]*s_y));
+    rhs[0] = (P[2]*s_y);
     rhs[1] = (P[1]*s_x);
     linear[0] = T(0.0);
     linear[1] = T(0.0);

@@ -12,6 +12,7 @@ struct Oscilator {
   static constexpr int num_params = 2;
   static constexpr int num_field_params = 2;
   static constexpr int num_monitored = 0;
+  static constexpr int num_derived = 0;
 
   // values = f(y, time)
   template <typename T>
@@ -22,6 +23,13 @@ struct Oscilator {
     values[0] = (-(F[0]*s_y));
     values[1] = (F[1]*s_x);
     (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // derived constants: parameter-only sub-expressions, evaluated once per
+  // launch on the host in FP64 and stored after the parameters
+  static void derived(const double* P, double* C)
+  {
+    (void)P; (void)C;
   }
 
   // rhs = f(y, time), linear[i] = d f_i / d y_i

@@ -79,9 +79,12 @@ def test_eval_matches_oracle_tp06():
     lin, rhs = ode.linearized_eval_many(ys, ts)
     cpu = np.array([om.rhs(y, t) for y, t in zip(ys, ts)])
     cl = np.array([om.linearized(y, t)[0] for y, t in zip(ys, ts)])
-    np.testing.assert_allclose(gpu, cpu, rtol=1e-13, atol=1e-16)
-    np.testing.assert_allclose(rhs, cpu, rtol=1e-13, atol=1e-16)
-    np.testing.assert_allclose(lin, cl, rtol=1e-12, atol=1e-16)
+    # the device code folds parameter-only sub-expressions into constants,
+    # which re-associates a few operations: agreement to rounding, amplified
+    # only where terms of a sum cancel
+    np.testing.assert_allclose(gpu, cpu, rtol=1e-11, atol=1e-14)
+    np.testing.assert_allclose(rhs, cpu, rtol=1e-11, atol=1e-14)
+    np.testing.assert_allclose(lin, cl, rtol=1e-11, atol=1e-14)
 
 
 @pytest.mark.parametrize("Solver", goss.solvers.GOSSExplicitSolvers)
