@@ -202,6 +202,30 @@ def run_gpu(args, rank, world, dist):
     if not args.skip_fp64:
         s64 = make("double")
         fp64_ms, _ = timed(s64, args.steps, args.warmup)
+    # --- plain FP64 GPU path: one launch per internal step (states through HBM
+    #     every step, as goss's PyCUDA path launches one kernel per substep) ---
+    plain64 = None
+    if not args.skip_fp64:
+        sp = make("double")
+        t = 0.0
+        for _ in range(50):
+            sp.forward_async(t, LDT)
+            t += LDT
+        sp.synchronize()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        for _ in range(steps_per_call):
+            sp.forward_async(t, LDT)
+            t += LDT
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        sp.synchronize()
+        torch.cuda.synchronize()
+        plain64 = float(N) * steps_per_call / (e0.elapsed_time(e1) / 1e3)
+        del sp
+    out["fp64_plain_value"] = plain64
     # --- accuracy of FP32 against FP64 at the end of the run ----------------
     v32 = s32.states[:, iv]
     err = None
@@ -233,6 +257,8 @@ def run_gpu(args, rank, world, dist):
     e2e_s = time.perf_counter() - w0
     del e2e
 
+    out["batched"] = run_batched(args, dev) if not args.skip_fp64 else None
+
     times = torch.tensor([ms32, fp64_ms or 0.0, e2e_s], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
@@ -249,6 +275,44 @@ def run_gpu(args, rank, world, dist):
         model_time_ms=t_end,
     ))
     return out, md
+
+
+BATCH_POPS = [  # heterogeneous workload: model, field parameters, solver, nodes
+    ("fitzhughnagumo", ["a", "b"], "RK4", 3),
+    ("fitzhughnagumo", ["a", "b"], "RK4", 200_000),
+    ("oscilator", ["a", "b"], "RK4", 5_000),
+    ("tentusscher_2004_mcell", FIELDS, "GRL1", 700_000),
+    ("tentusscher_panfilov_2006_M_cell", FIELDS, "GRL1", 64_000),
+    ("tentusscher_panfilov_2006_M_cell", FIELDS, "GRL1", 1_000_000),
+]
+
+
+def run_batched(args, dev, steps=1000, dt=0.01, precision="single"):
+    """Six populations (1,969,003 nodes, 2/17/19 states, RK4 and GRL1) in one
+    persistent kernel per forward; 1000 forwards of dt = 0.01 ms captured in
+    one CUDA graph; launch configuration from the autotuner."""
+    import goss_b200 as goss
+    from goss_b200 import autotune
+
+    rng = np.random.default_rng(SEED)
+    systems = []
+    for model, fps, solver, n in BATCH_POPS:
+        ode = goss.ParameterizedODE(model, field_parameters=fps)
+        s = goss.solvers.solver_mapper[solver](ode)
+        s.internal_time_step = dt
+        sysm = goss.ODESystemSolver(n, s, ode, precision=precision, device=dev)
+        sysm.set_states(ode.get_ic()[None, :] * (1 + rng.uniform(-0.1, 0.1, (n, ode.num_states))))
+        sysm.field_parameters = sysm.field_parameters * (1 + rng.uniform(-0.1, 0.1, (n, len(fps))))
+        systems.append(sysm)
+    batch = goss.BatchSolver(systems)
+    tuned = autotune.tune_batch(batch, interval=dt, steps=20)
+    batch.time(0.0, dt, 10, use_graph=False)  # warm-up
+    ms = batch.time(0.0, dt, steps, use_graph=True)
+    nodes = batch.total_nodes
+    return {"value": nodes * steps / (ms / 1e3), "unit": "cell-steps/s", "nodes": nodes, "forwards": steps,
+            "ms": ms, "precision": precision, "graph": True,
+            "config": {k: tuned[k] for k in ("block", "grid", "schedule", "order")},
+            "populations": [f"{m}/{s}/{n}" for m, _, s, n in BATCH_POPS]}
 
 
 def roofline(md, value_fp32, ms_per_step, n_nodes):
@@ -391,8 +455,12 @@ def main():
                 "data": "synthetic (seeded)", "config": config, "roofline": rl, "cpu_baseline": cpu,
                 "e2e": res["e2e"], "gpu_launches": args.steps, "clocks": res["clocks"],
                 "fp64": {"value": res["fp64_value"], "fp32_over_fp64": res["fp32_over_fp64"],
+                         "plain_value": res["fp64_plain_value"],
+                         "fp32_over_plain_fp64": (res["value"] / world / res["fp64_plain_value"])
+                         if res["fp64_plain_value"] else None,
                          "v_max_rel_err_fp32_vs_fp64": res["v_max_rel_err_fp32_vs_fp64"]},
-                "state_max_rel_err_fp32_vs_fp64": res.get("state_max_rel_err_fp32_vs_fp64")}
+                "state_max_rel_err_fp32_vs_fp64": res.get("state_max_rel_err_fp32_vs_fp64"),
+                "batched_heterogeneous": res.get("batched")}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

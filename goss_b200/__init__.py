@@ -45,3 +45,7 @@ __all__ = [
     "has_openmp",
     "__version__",
 ]
+
+from .batch import BatchSolver  # noqa: E402
+
+__all__.append("BatchSolver")

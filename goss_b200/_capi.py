@@ -81,6 +81,18 @@ class ModelDesc(C.Structure):
     ]
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("name", C.c_char_p),
+        ("num_kinds", C.c_uint32),
+        ("kind_variants", C.POINTER(C.c_char_p)),
+        ("kind_solvers", C.POINTER(C.c_int32)),
+        ("kind_num_states", C.POINTER(C.c_uint32)),
+        ("launch", C.c_void_p),
+    ]
+
+
 _dp = C.POINTER(C.c_double)
 _u32p = C.POINTER(C.c_uint32)
 _i64p = C.POINTER(C.c_int64)
@@ -123,7 +135,19 @@ _PROTOS = {
     "goss_system_device_states": (C.c_int, [_sys, C.POINTER(_dp), C.POINTER(C.c_uint64)]),
     "goss_system_device_field_params": (C.c_int, [_sys, C.POINTER(_dp), C.POINTER(C.c_uint64)]),
     "goss_system_set_stream": (C.c_int, [_sys, C.c_void_p]),
-    "goss_model_eval_noalloc": (C.c_int, [_desc, C.c_int32, C.c_int32, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
+    "goss_system_capture": (C.c_int, [_sys, C.c_double, C.c_double, C.c_uint32]),
+    "goss_system_replay": (C.c_int, [_sys]),
+    "goss_batch_create": (C.c_int, [C.POINTER(BatchDesc), C.POINTER(C.c_void_p), C.POINTER(C.c_int32), C.c_uint32,
+                                    C.c_int32, C.POINTER(C.c_void_p)]),
+    "goss_batch_destroy": (C.c_int, [C.c_void_p]),
+    "goss_batch_set_config": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _u32p]),
+    "goss_batch_forward": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "goss_batch_capture": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_uint32]),
+    "goss_batch_replay": (C.c_int, [C.c_void_p]),
+    "goss_batch_time": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_uint32, C.c_int32,
+                                  C.POINTER(C.c_float)]),
+    "goss_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "goss_model_eval_noalloc":(C.c_int, [_desc, C.c_int32, C.c_int32, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_uint64, C.c_void_p, C.c_void_p]),
     "goss_model_eval_noalloc_capacity": (C.c_uint64, []),
     "goss_lu_factorize": (C.c_int, [C.c_uint32, _dp]),

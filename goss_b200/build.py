@@ -97,10 +97,34 @@ def build_variant(vdir: Path, force: bool = False, extra_flags: Optional[List[st
     return out
 
 
-def build_all(variant_dirs: Iterable[Path], force: bool = False, jobs: Optional[int] = None) -> List[Path]:
-    """Runtime plus every variant, variants compiled in parallel."""
+def batch_deps(bdir: Path) -> List[Path]:
+    import json
+
+    meta = json.loads((Path(bdir) / "batch.json").read_text())
+    deps = [Path(bdir) / "batch.cu", CSRC / "goss_batch.cuh", CSRC / "goss_kernels.cuh",
+            CSRC / "goss_device_math.cuh", INCLUDE / "goss_b200.h"]
+    deps += [PKG / v / "device.cuh" for v, _ in meta["kinds"]]
+    return deps
+
+
+def build_batch(bdir: Path, force: bool = False) -> Path:
+    """Compile one batch module directory into ``libgoss_batch.so``."""
+    bdir = Path(bdir)
+    out = bdir / "libgoss_batch.so"
+    flags = ["--use_fast_math"]
+    if force or _stale(out, batch_deps(bdir), flags):
+        tmp = out.with_suffix(f".so.{os.getpid()}.tmp")
+        _run([nvcc(), *ARCH, *COMMON, *flags, f"-I{PKG}", "-shared", str(bdir / "batch.cu"), "-o", str(tmp)])
+        os.replace(tmp, out)
+        _stamp(out, batch_deps(bdir), flags)
+    return out
+
+
+def build_all(variant_dirs: Iterable[Path], force: bool = False, jobs: Optional[int] = None,
+              batch_dirs: Iterable[Path] = ()) -> List[Path]:
+    """Runtime plus every variant and batch module, compiled in parallel."""
     build_runtime(force)
-    dirs = list(variant_dirs)
-    jobs = jobs or max(1, min(len(dirs), os.cpu_count() or 1))
+    jobs_list = [(build_variant, d) for d in variant_dirs] + [(build_batch, d) for d in batch_dirs]
+    jobs = jobs or max(1, min(len(jobs_list), os.cpu_count() or 1))
     with ThreadPoolExecutor(max_workers=jobs) as ex:
-        return list(ex.map(lambda d: build_variant(d, force), dirs))
+        return list(ex.map(lambda fd: fd[0](fd[1], force), jobs_list))

@@ -417,11 +417,12 @@ class ModelSource:
             pass
         return lines
 
-    def emit_device(self) -> str:
-        cls = model_class_name(self.name)
+    def emit_device(self, struct_name: str = None) -> str:
+        # one struct per variant, so several variants can share a translation unit
+        cls = struct_name or model_class_name(self.name)
         ns, npar, nfp = len(self.states), len(self.params), len(self.fparams)
         L = []
-        guard = self.ident.upper() + "_DEVICE_CUH"
+        guard = cls.upper() + "_DEVICE_CUH"
         L.append(f"// Generated by goss_b200.codegen from the '{self.name}' model; do not edit.")
         L.append("// Device-side model: rhs and linearised rhs templated on the arithmetic type T.")
         L.append(f"#ifndef {guard}")

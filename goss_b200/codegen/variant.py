@@ -62,9 +62,14 @@ def _num_list(ctype: str, name: str, items, fmt=str) -> str:
     return f"static const {ctype} {name}[{len(items)}] = {{" + ", ".join(fmt(v) for v in items) + "};"
 
 
+def device_struct(ident: str) -> str:
+    """Name of a variant's device model struct (unique per variant)."""
+    return f"M_{ident}"
+
+
 def emit_module(src: ModelSource, ident: str) -> str:
     md = src.metadata()
-    cls = model_class_name(src.name)
+    cls = device_struct(ident)
     from .printer import c_double
 
     lines = [
@@ -121,7 +126,7 @@ def write_variant(model: ODEModel, outdir: Path, field_parameters: Sequence[str]
               hash=model_hash(model, field_parameters, monitored, linearization),
               generator_version=GENERATOR_VERSION, class_name=model_class_name(model.name))
     files = {
-        "device.cuh": src.emit_device(),
+        "device.cuh": src.emit_device(device_struct(ident)),
         "module.cu": emit_module(src, ident),
         "oracle_model.c": src.emit_oracle_c(),
         "goss_plugin.h": src.emit_goss_plugin(),

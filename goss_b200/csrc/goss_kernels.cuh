@@ -177,13 +177,26 @@ struct Acc<float> {
     }
 };
 
+// Where one node's explicit solve reads and writes (shared by the
+// single-population kernel and the batched kernel of goss_batch.cuh).
+struct NodeIO {
+    double* states;         // [n][ld]
+    const double* fparams;  // [nfp][ld]
+    uint8_t* node_status;   // [ld]
+    uint32_t* flags;
+    uint64_t ld;
+    uint64_t nsteps;
+    double t;
+    double ldt;
+    double delta;
+};
+
+// Advance one node over nsteps internal steps of one explicit solver.
 template <class M, typename T, Explicit S>
-__global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ ExplicitArgs<M, T> a)
+__device__ __forceinline__ void explicit_node(const NodeIO& a, uint32_t node, const T* __restrict__ P,
+                                              const double* __restrict__ PD)
 {
     constexpr int n = M::num_states;
-    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= a.N)
-        return;
     Acc<T> y[n];
 #pragma unroll
     for (int i = 0; i < n; ++i)
@@ -204,7 +217,7 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
         if constexpr (S == Explicit::Euler) {
             // ExplicitEuler.cpp:80-81
             T f[n];
-            M::template rhs<T>(yt, lt, a.P, a.PD, F, f);
+            M::template rhs<T>(yt, lt, P, PD, F, f);
 #pragma unroll
             for (int i = 0; i < n; ++i)
                 y[i].add(h * f[i]);
@@ -212,25 +225,25 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
             // RK4.cpp:79-98 with RK4::axpy (RK4.h:70-74); the weighted sum is
             // accumulated in the order k1 + 2 k2 + 2 k3 + k4 of the reference.
             T k[n], sum[n], tmp[n];
-            M::template rhs<T>(yt, lt, a.P, a.PD, F, k);
+            M::template rhs<T>(yt, lt, P, PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = k[i];
                 tmp[i] = y[i].plus(hh * k[i]);
             }
-            M::template rhs<T>(tmp, lt + 0.5 * ldt, a.P, a.PD, F, k);
+            M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = sum[i] + T(2.0) * k[i];
                 tmp[i] = y[i].plus(hh * k[i]);
             }
-            M::template rhs<T>(tmp, lt + 0.5 * ldt, a.P, a.PD, F, k);
+            M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = sum[i] + T(2.0) * k[i];
                 tmp[i] = y[i].plus(h * k[i]);
             }
-            M::template rhs<T>(tmp, lt + ldt, a.P, a.PD, F, k);
+            M::template rhs<T>(tmp, lt + ldt, P, PD, F, k);
 #pragma unroll
             for (int i = 0; i < n; ++i) {
                 sum[i] = sum[i] + k[i];
@@ -239,7 +252,7 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
         } else if constexpr (S == Explicit::GRL1) {
             // GRL1.h:72-84
             T lin[n], rhs[n];
-            M::template linearized<T>(yt, lt, a.P, a.PD, F, lin, rhs);
+            M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
 #pragma unroll
             for (int i = 0; i < n; ++i)
                 y[i].add(grl_increment(lin[i], rhs[i], h, delta));
@@ -248,11 +261,11 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
             // self-initialised local (GRL2.cpp:67) whose -O3 build behaves as 0:
             // the exponential form is used whenever the linear term is non-zero.
             T lin[n], rhs[n], y2[n];
-            M::template linearized<T>(yt, lt, a.P, a.PD, F, lin, rhs);
+            M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
 #pragma unroll
             for (int i = 0; i < n; ++i)
                 y2[i] = y[i].plus(grl_increment(lin[i], rhs[i], hh, T(0)));
-            M::template linearized<T>(y2, lt, a.P, a.PD, F, lin, rhs);
+            M::template linearized<T>(y2, lt, P, PD, F, lin, rhs);
 #pragma unroll
             for (int i = 0; i < n; ++i)
                 y[i].add(grl_increment(lin[i], rhs[i], h, T(0)));
@@ -270,6 +283,16 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
         a.node_status[node] |= GOSS_FLAG_NONFINITE;
         atomicOr(a.flags, GOSS_FLAG_NONFINITE);
     }
+}
+
+template <class M, typename T, Explicit S>
+__global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ ExplicitArgs<M, T> a)
+{
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= a.N)
+        return;
+    const NodeIO io{a.states, a.fparams, a.node_status, a.flags, a.ld, a.nsteps, a.t, a.ldt, a.delta};
+    explicit_node<M, T, S>(io, node, a.P, a.PD);
 }
 
 // ---------------------------------------------------------------------------

@@ -138,6 +138,23 @@ struct goss_system {
     uint32_t block = 0;
     uint32_t num_threads = 0;
     uint32_t host_flags = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::string last_error;
+};
+
+struct goss_batch {
+    const goss_batch_desc* d = nullptr;
+    std::vector<goss_system*> systems;
+    std::vector<int32_t> kinds;
+    std::vector<uint32_t> order;
+    int32_t precision = 0;
+    int32_t device = 0;
+    uint32_t block = 128, grid = 0, schedule = 1;
+    uint32_t* d_counters = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
     std::string last_error;
 };
 
@@ -358,10 +375,311 @@ GOSS_API int goss_system_destroy(goss_system* s)
     cudaFree(s->d_stage);
     cudaFree(s->d_small);
     cudaFree(s->d_rows);
+    if (s->graph_exec)
+        cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph)
+        cudaGraphDestroy(s->graph);
     if (s->own_stream && s->stream)
         cudaStreamDestroy(s->stream);
     delete s;
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA graphs of forward loops
+// ---------------------------------------------------------------------------
+GOSS_API int goss_system_capture(goss_system* s, double t0, double interval, uint32_t num_steps)
+{
+    if (!s || num_steps == 0)
+        return fail(s ? &s->last_error : nullptr, GOSS_ERR_ARGUMENT, "capture needs a system and num_steps > 0");
+    int rc = set_device(s);
+    if (rc)
+        return rc;
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (s->graph_exec) {
+        cudaGraphExecDestroy(s->graph_exec);
+        s->graph_exec = nullptr;
+    }
+    if (s->graph) {
+        cudaGraphDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t k = 0; k < num_steps && !rc; ++k)
+        rc = launch_forward(s, t0 + k * interval, interval);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc) {
+        if (g)
+            cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess)
+        return fail(&s->last_error, GOSS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    s->graph = g;
+    CUDA_TRY(s, cudaGraphInstantiate(&s->graph_exec, s->graph, 0));
+    return 0;
+}
+
+GOSS_API int goss_system_replay(goss_system* s)
+{
+    if (!s || !s->graph_exec)
+        return fail(s ? &s->last_error : nullptr, GOSS_ERR_ARGUMENT, "no captured graph");
+    int rc = set_device(s);
+    if (rc)
+        return rc;
+    CUDA_TRY(s, cudaGraphLaunch(s->graph_exec, s->stream));
+    return check_flags(s);
+}
+
+// ---------------------------------------------------------------------------
+// heterogeneous batches
+// ---------------------------------------------------------------------------
+namespace {
+
+int batch_fail(goss_batch* b, int code, const char* msg)
+{
+    return fail(b ? &b->last_error : nullptr, code, "%s", msg);
+}
+
+int batch_launch(goss_batch* b, double t, double interval)
+{
+    std::vector<goss_batch_pop> pops(b->systems.size());
+    for (size_t i = 0; i < pops.size(); ++i) {
+        goss_system* s = b->systems[i];
+        goss_batch_pop& p = pops[i];
+        p.kind = b->kinds[i];
+        p.num_nodes = s->N;
+        p.ld = s->ld;
+        p.states = s->d_states;
+        p.field_params = s->d_fparams;
+        p.node_status = s->d_node_status;
+        p.flags = s->d_flags;
+        p.params = s->params.data();
+        p.solver_params = &s->sp;
+    }
+    goss_batch_launch L{};
+    L.precision = b->precision;
+    L.num_pops = (uint32_t)pops.size();
+    L.pops = pops.data();
+    L.order = b->order.empty() ? nullptr : b->order.data();
+    L.block = b->block;
+    L.grid = b->grid;
+    L.schedule = b->schedule;
+    L.counters = b->d_counters;
+    L.t = t;
+    L.interval = interval;
+    L.stream = b->stream;
+    const int rc = b->d->launch(&L);
+    if (rc)
+        return fail(&b->last_error, rc, "batch launch failed (%s)", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
+int batch_check(goss_batch* b)
+{
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess)
+        return fail(&b->last_error, GOSS_ERR_CUDA, "batch failed: %s", cudaGetErrorString(e));
+    for (goss_system* s : b->systems) {
+        const int rc = check_flags(s);
+        if (rc)
+            return fail(&b->last_error, rc, "%s", s->last_error.c_str());
+    }
+    return 0;
+}
+
+}  // namespace
+
+GOSS_API const char* goss_batch_last_error(const goss_batch* b) { return b ? b->last_error.c_str() : ""; }
+
+GOSS_API int goss_batch_create(const goss_batch_desc* d, goss_system* const* systems, const int32_t* kinds,
+                               uint32_t count, int32_t precision, goss_batch** out)
+{
+    if (!out || !d || (count && (!systems || !kinds)))
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (d->abi_version != GOSS_B200_ABI_VERSION)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "batch module built for another ABI version");
+    if (count > 16)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "a batch holds at most 16 populations");
+    if (precision != GOSS_FP64 && precision != GOSS_FP32)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "invalid precision %d", precision);
+    int device = count ? systems[0]->device : 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const goss_system* s = systems[i];
+        if (!s || kinds[i] < 0 || (uint32_t)kinds[i] >= d->num_kinds)
+            return fail(nullptr, GOSS_ERR_ARGUMENT, "population %u: invalid system or kind", i);
+        if (s->solver != d->kind_solvers[kinds[i]] || s->n != d->kind_num_states[kinds[i]])
+            return fail(nullptr, GOSS_ERR_ARGUMENT, "population %u: solver or model does not match kind %d (%s)", i,
+                        kinds[i], d->kind_variants[kinds[i]]);
+        if (s->device != device)
+            return fail(nullptr, GOSS_ERR_ARGUMENT, "all populations must live on one device");
+        for (uint32_t j = 0; j < i; ++j)
+            if (systems[j] == s)
+                return fail(nullptr, GOSS_ERR_ARGUMENT, "a system appears twice in the batch");
+    }
+    auto* b = new goss_batch();
+    b->d = d;
+    b->systems.assign(systems, systems + count);
+    b->kinds.assign(kinds, kinds + count);
+    b->precision = precision;
+    b->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_counters, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(uint32_t), b->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) {
+        goss_batch_destroy(b);
+        return fail(nullptr, GOSS_ERR_CUDA, "batch create: %s", cudaGetErrorString(e));
+    }
+    // the populations are about to be touched from the batch stream
+    for (goss_system* s : b->systems)
+        cudaStreamSynchronize(s->stream);
+    *out = b;
+    return 0;
+}
+
+GOSS_API int goss_batch_destroy(goss_batch* b)
+{
+    if (!b)
+        return 0;
+    cudaSetDevice(b->device);
+    if (b->stream)
+        cudaStreamSynchronize(b->stream);
+    if (b->graph_exec)
+        cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph)
+        cudaGraphDestroy(b->graph);
+    cudaFree(b->d_counters);
+    if (b->stream)
+        cudaStreamDestroy(b->stream);
+    delete b;
+    return 0;
+}
+
+GOSS_API int goss_batch_set_config(goss_batch* b, uint32_t block, uint32_t grid, uint32_t schedule,
+                                   const uint32_t* order)
+{
+    if (!b)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL batch");
+    if (block && (block % 32 || block > 128))
+        return batch_fail(b, GOSS_ERR_ARGUMENT, "block must be a multiple of 32 and at most 128");
+    if (schedule > 1)
+        return batch_fail(b, GOSS_ERR_ARGUMENT, "schedule must be 0 (round-robin) or 1 (dynamic)");
+    if (order) {
+        std::vector<uint32_t> o(order, order + b->systems.size());
+        std::vector<uint32_t> s(o);
+        std::sort(s.begin(), s.end());
+        for (size_t i = 0; i < s.size(); ++i)
+            if (s[i] != i)
+                return batch_fail(b, GOSS_ERR_ARGUMENT, "order must be a permutation of the populations");
+        b->order = o;
+    } else {
+        b->order.clear();
+    }
+    b->block = block ? block : 128;
+    b->grid = grid;
+    b->schedule = schedule;
+    return 0;
+}
+
+GOSS_API int goss_batch_forward(goss_batch* b, double t, double interval)
+{
+    if (!b)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL batch");
+    CUDA_TRY((goss_system*)nullptr, cudaSetDevice(b->device));
+    int rc = batch_launch(b, t, interval);
+    return rc ? rc : batch_check(b);
+}
+
+GOSS_API int goss_batch_capture(goss_batch* b, double t0, double interval, uint32_t num_steps)
+{
+    if (!b || num_steps == 0)
+        return fail(b ? &b->last_error : nullptr, GOSS_ERR_ARGUMENT, "capture needs a batch and num_steps > 0");
+    CUDA_TRY((goss_system*)nullptr, cudaSetDevice(b->device));
+    cudaStreamSynchronize(b->stream);
+    if (b->graph_exec) {
+        cudaGraphExecDestroy(b->graph_exec);
+        b->graph_exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess)
+        return fail(&b->last_error, GOSS_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    int rc = 0;
+    for (uint32_t k = 0; k < num_steps && !rc; ++k)
+        rc = batch_launch(b, t0 + k * interval, interval);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+        if (g)
+            cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess)
+        return fail(&b->last_error, GOSS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    b->graph = g;
+    e = cudaGraphInstantiate(&b->graph_exec, b->graph, 0);
+    if (e != cudaSuccess)
+        return fail(&b->last_error, GOSS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+GOSS_API int goss_batch_replay(goss_batch* b)
+{
+    if (!b || !b->graph_exec)
+        return fail(b ? &b->last_error : nullptr, GOSS_ERR_ARGUMENT, "no captured graph");
+    CUDA_TRY((goss_system*)nullptr, cudaSetDevice(b->device));
+    cudaError_t e = cudaGraphLaunch(b->graph_exec, b->stream);
+    if (e != cudaSuccess)
+        return fail(&b->last_error, GOSS_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+    return batch_check(b);
+}
+
+GOSS_API int goss_batch_time(goss_batch* b, double t0, double interval, uint32_t num_steps, int32_t use_graph,
+                             float* ms)
+{
+    if (!b || !ms || num_steps == 0)
+        return fail(b ? &b->last_error : nullptr, GOSS_ERR_ARGUMENT, "NULL argument or num_steps == 0");
+    CUDA_TRY((goss_system*)nullptr, cudaSetDevice(b->device));
+    int rc = 0;
+    if (use_graph) {
+        rc = goss_batch_capture(b, t0, interval, num_steps);
+        if (rc)
+            return rc;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, b->stream);
+    if (use_graph) {
+        cudaGraphLaunch(b->graph_exec, b->stream);
+    } else {
+        for (uint32_t k = 0; k < num_steps && !rc; ++k)
+            rc = batch_launch(b, t0 + k * interval, interval);
+    }
+    cudaEventRecord(e1, b->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float v = 0.f;
+    if (e == cudaSuccess)
+        e = cudaEventElapsedTime(&v, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc)
+        return rc;
+    if (e != cudaSuccess)
+        return fail(&b->last_error, GOSS_ERR_CUDA, "timing failed: %s", cudaGetErrorString(e));
+    *ms = v;
+    return batch_check(b);
 }
 
 GOSS_API int goss_system_set_solver_params(goss_system* s, const goss_solver_params* p)

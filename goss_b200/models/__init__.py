@@ -25,6 +25,8 @@ SHIPPED: List[Dict] = [
     dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode", field_parameters=["g_Kr", "g_CaL"]),
     dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode",
          field_parameters=["g_Kr", "g_Na", "g_Ks"]),
+    dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode",
+         field_parameters=["g_Kr", "g_Ks", "g_CaL", "g_to"]),
     dict(name="fitzhughnagumo", ode="tests/fitzhughnagumo.ode", field_parameters=[]),
     dict(name="fitzhughnagumo", ode="tests/fitzhughnagumo.ode", field_parameters=["a", "b"]),
     dict(name="fitzhughnagumo", ode="tests/fitzhughnagumo.ode", field_parameters=[], monitored=["p_42", "p_V"]),

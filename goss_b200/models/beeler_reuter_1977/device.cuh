@@ -1,12 +1,12 @@
 // Generated by goss_b200.codegen from the 'beeler_reuter_1977' model; do not edit.
 // Device-side model: rhs and linearised rhs templated on the arithmetic type T.
-#ifndef BEELER_REUTER_1977_DEVICE_CUH
-#define BEELER_REUTER_1977_DEVICE_CUH
+#ifndef M_BEELER_REUTER_1977_DEVICE_CUH
+#define M_BEELER_REUTER_1977_DEVICE_CUH
 #include "goss_device_math.cuh"
 
 namespace goss_b200 { namespace models {
 
-struct Beeler_reuter_1977 {
+struct M_beeler_reuter_1977 {
   static constexpr const char* name = "beeler_reuter_1977";
   static constexpr int num_states = 8;
   static constexpr int num_params = 10;

@@ -4,7 +4,7 @@
 #include "device.cuh"
 
 namespace {
-using Model = goss_b200::models::Beeler_reuter_1977;
+using Model = goss_b200::models::M_beeler_reuter_1977;
 static const char* const state_names[8] = {"m", "h", "j", "Cai", "d", "f", "x1", "V"};
 static const char* const parameter_names[10] = {"E_Na", "g_Na", "g_Nac", "g_s", "IstimAmplitude", "IstimEnd", "IstimPeriod", "IstimPulseDuration", "IstimStart", "C"};
 static const char* const field_parameter_names[1] = {nullptr};

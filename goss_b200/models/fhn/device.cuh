@@ -1,12 +1,12 @@
 // Generated by goss_b200.codegen from the 'fhn' model; do not edit.
 // Device-side model: rhs and linearised rhs templated on the arithmetic type T.
-#ifndef FHN_DEVICE_CUH
-#define FHN_DEVICE_CUH
+#ifndef M_FHN_DEVICE_CUH
+#define M_FHN_DEVICE_CUH
 #include "goss_device_math.cuh"
 
 namespace goss_b200 { namespace models {
 
-struct Fhn {
+struct M_fhn {
   static constexpr const char* name = "fhn";
   static constexpr int num_states = 2;
   static constexpr int num_params = 11;

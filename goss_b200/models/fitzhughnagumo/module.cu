@@ -4,7 +4,7 @@
 #include "device.cuh"
 
 namespace {
-using Model = goss_b200::models::Fitzhughnagumo;
+using Model = goss_b200::models::M_fitzhughnagumo;
 static const char* const state_names[2] = {"V", "s"};
 static const char* const parameter_names[11] = {"V_peak", "V_rest", "a", "b", "c_1", "c_2", "c_3", "stim_amplitude", "stim_duration", "stim_period", "stim_start"};
 static const char* const field_parameter_names[1] = {nullptr};

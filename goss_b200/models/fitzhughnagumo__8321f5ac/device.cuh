@@ -1,12 +1,12 @@
 // Generated by goss_b200.codegen from the 'fitzhughnagumo' model; do not edit.
 // Device-side model: rhs and linearised rhs templated on the arithmetic type T.
-#ifndef FITZHUGHNAGUMO_DEVICE_CUH
-#define FITZHUGHNAGUMO_DEVICE_CUH
+#ifndef M_FITZHUGHNAGUMO__8321F5AC_DEVICE_CUH
+#define M_FITZHUGHNAGUMO__8321F5AC_DEVICE_CUH
 #include "goss_device_math.cuh"
 
 namespace goss_b200 { namespace models {
 
-struct Fitzhughnagumo {
+struct M_fitzhughnagumo__8321f5ac {
   static constexpr const char* name = "fitzhughnagumo";
   static constexpr int num_states = 2;
   static constexpr int num_params = 11;

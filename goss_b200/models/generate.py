@@ -28,6 +28,20 @@ def main() -> int:
         md = write_variant(model, HERE / ident, field_parameters=entry["field_parameters"], monitored=mon)
         print(f"{ident}: {len(md['state_names'])} states, {len(md['parameter_names'])} parameters, "
               f"field parameters {md['field_parameter_names']}")
+    # batch modules over shipped variants
+    from ..batches import HERE as BATCHES, SHIPPED_BATCHES
+    from ..codegen.batchgen import write_batch
+    from . import find_variant
+
+    pkg = HERE.parent
+    for b in SHIPPED_BATCHES:
+        kinds = []
+        for name, fps, solver in b["kinds"]:
+            vdir = find_variant(name, fps)
+            assert vdir is not None, (name, fps)
+            kinds.append((vdir, solver))
+        write_batch(b["name"], kinds, BATCHES / b["name"], pkg)
+        print(f"batch {b['name']}: {[(k[0].name, k[1]) for k in kinds]}")
     return 0
 
 

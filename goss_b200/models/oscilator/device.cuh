@@ -1,12 +1,12 @@
 // Generated by goss_b200.codegen from the 'oscilator' model; do not edit.
 // Device-side model: rhs and linearised rhs templated on the arithmetic type T.
-#ifndef OSCILATOR_DEVICE_CUH
-#define OSCILATOR_DEVICE_CUH
+#ifndef M_OSCILATOR_DEVICE_CUH
+#define M_OSCILATOR_DEVICE_CUH
 #include "goss_device_math.cuh"
 
 namespace goss_b200 { namespace models {
 
-struct Oscilator {
+struct M_oscilator {
   static constexpr const char* name = "oscilator";
   static constexpr int num_states = 2;
   static constexpr int num_params = 2;

@@ -4,7 +4,7 @@
 #include "device.cuh"
 
 namespace {
-using Model = goss_b200::models::Oscilator;
+using Model = goss_b200::models::M_oscilator__5dc98ee0;
 static const char* const state_names[2] = {"x", "y"};
 static const char* const parameter_names[2] = {"a", "b"};
 static const char* const field_parameter_names[2] = {"a", "b"};

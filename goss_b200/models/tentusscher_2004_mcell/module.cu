@@ -4,7 +4,7 @@
 #include "device.cuh"
 
 namespace {
-using Model = goss_b200::models::Tentusscher_2004_mcell;
+using Model = goss_b200::models::M_tentusscher_2004_mcell;
 static const char* const state_names[17] = {"Xr1", "Xr2", "Xs", "m", "h", "j", "d", "f", "fCa", "s", "r", "g", "Ca_i", "Ca_SR", "Na_i", "V", "K_i"};
 static const char* const parameter_names[45] = {"P_kna", "g_K1", "g_Kr", "g_Ks", "g_Na", "g_bna", "g_CaL", "g_bca", "g_to", "K_mNa", "K_mk", "P_NaK", "K_NaCa", "K_sat", "Km_Ca", "Km_Nai", "alpha", "gamma", "K_pCa", "g_pCa", "g_pK", "Buf_c", "Buf_sr", "Ca_o", "K_buf_c", "K_buf_sr", "K_up", "V_leak", "V_sr", "Vmax_up", "a_rel", "b_rel", "c_rel", "tau_g", "Na_o", "Cm", "F", "R", "T", "V_c", "stim_amplitude", "stim_duration", "stim_period", "stim_start", "K_o"};
 static const char* const field_parameter_names[1] = {nullptr};

@@ -4,7 +4,7 @@
 #include "device.cuh"
 
 namespace {
-using Model = goss_b200::models::Tentusscher_panfilov_2006_m_cell;
+using Model = goss_b200::models::M_tentusscher_panfilov_2006_M_cell;
 static const char* const state_names[19] = {"Xr1", "Xr2", "Xs", "m", "h", "j", "d", "f", "f2", "fCass", "s", "r", "Ca_i", "R_prime", "Ca_SR", "Ca_ss", "Na_i", "V", "K_i"};
 static const char* const parameter_names[53] = {"P_kna", "g_K1", "g_Kr", "g_Ks", "g_Na", "g_bna", "g_CaL", "g_bca", "g_to", "K_mNa", "K_mk", "P_NaK", "K_NaCa", "K_sat", "Km_Ca", "Km_Nai", "alpha", "gamma", "K_pCa", "g_pCa", "g_pK", "Buf_c", "Buf_sr", "Buf_ss", "Ca_o", "EC", "K_buf_c", "K_buf_sr", "K_buf_ss", "K_up", "V_leak", "V_rel", "V_sr", "V_ss", "V_xfer", "Vmax_up", "k1_prime", "k2_prime", "k3", "k4", "max_sr", "min_sr", "Na_o", "Cm", "F", "R", "T", "V_c", "stim_amplitude", "stim_duration", "stim_period", "stim_start", "K_o"};
 static const char* const field_parameter_names[1] = {nullptr};

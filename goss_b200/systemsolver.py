@@ -221,6 +221,16 @@ class ODESystemSolver:
     def synchronize(self) -> None:
         _capi.check(self._L.goss_system_synchronize(self._h), self._h)
 
+    def capture(self, t0: float, interval: float, num_steps: int) -> None:
+        """Record num_steps forward(t0 + k*interval, interval) launches into a
+        CUDA graph (solver and model parameters as of now)."""
+        self._sync_params()
+        _capi.check(self._L.goss_system_capture(self._h, float(t0), float(interval), int(num_steps)), self._h)
+
+    def replay(self) -> None:
+        """Launch the captured graph and wait for it."""
+        _capi.check(self._L.goss_system_replay(self._h), self._h)
+
     def set_block_size(self, block: int) -> None:
         _capi.check(self._L.goss_system_set_block_size(self._h, int(block)), self._h)
 

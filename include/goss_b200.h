@@ -150,7 +150,49 @@ typedef struct goss_model_desc {
     const uint32_t* op_census_rhs;
 } goss_model_desc;
 
+/* One population of a heterogeneous batch (filled by the runtime). */
+typedef struct goss_batch_pop {
+    int32_t kind;            /* index into the batch module's kinds */
+    uint32_t num_nodes;
+    uint64_t ld;
+    double* states;          /* device [num_states][ld] */
+    const double* field_params;
+    uint8_t* node_status;
+    uint32_t* flags;
+    const double* params;    /* host [num_parameters] */
+    const goss_solver_params* solver_params; /* host */
+} goss_batch_pop;
+
+/* One launch of a batch module over all populations. */
+typedef struct goss_batch_launch {
+    int32_t precision;
+    uint32_t num_pops;
+    const goss_batch_pop* pops;
+    const uint32_t* order;   /* tile order of the populations (NULL: as given) */
+    uint32_t block;          /* nodes per tile = threads per block */
+    uint32_t grid;           /* persistent grid size (0: one block per tile) */
+    uint32_t schedule;       /* 0: round-robin tiles, 1: tiles claimed from an atomic counter */
+    uint32_t* counters;      /* device [2], zero before the first launch */
+    double t;
+    double interval;
+    void* stream;
+} goss_batch_launch;
+
+/* A compiled batch module: the kernels of several (model variant, explicit
+ * solver) kinds in one persistent kernel.  No counterpart in the reference,
+ * which runs one ODESystemSolver per population in sequence. */
+typedef struct goss_batch_desc {
+    uint32_t abi_version;
+    const char* name;
+    uint32_t num_kinds;
+    const char* const* kind_variants; /* model variant of each kind */
+    const int32_t* kind_solvers;      /* solver kind of each kind */
+    const uint32_t* kind_num_states;
+    int (*launch)(const goss_batch_launch* launch);
+} goss_batch_desc;
+
 typedef struct goss_system goss_system;
+typedef struct goss_batch goss_batch;
 
 /* ODESystemSolver(uint nodes, shared_ptr<ODESolver>, shared_ptr<ParameterizedODE>)
  * (ODESystemSolver.cpp:45-59): allocates device state, sets the initial
@@ -225,6 +267,32 @@ GOSS_API int goss_system_synchronize(goss_system* sys);
 GOSS_API int goss_model_eval(const goss_model_desc* model, int32_t what, int32_t precision, const double* params,
                              const double* states, const double* field_params, const double* times, uint64_t count,
                              double* out, int32_t device);
+
+/* CUDA graphs of forward loops.  goss_system_capture records num_steps
+ * consecutive forward(t0 + k*interval, interval) launches into a graph;
+ * goss_system_replay launches it (solver and model parameters are those at
+ * capture time) and synchronises; a new capture replaces the old graph. */
+GOSS_API int goss_system_capture(goss_system* sys, double t0, double interval, uint32_t num_steps);
+GOSS_API int goss_system_replay(goss_system* sys);
+
+/* Heterogeneous batches: the populations are existing systems (their states,
+ * field parameters, solver and model parameters); kinds[i] selects the
+ * batch module's kind for systems[i] (it must match the system's model
+ * variant name and solver).  One goss_batch_forward launches one kernel for
+ * all populations; capture/replay record num_steps forwards in a CUDA graph.
+ * goss_batch_time measures num_steps forwards (graph or direct launches)
+ * with CUDA events on the batch stream, leaving the states advanced. */
+GOSS_API int goss_batch_create(const goss_batch_desc* desc, goss_system* const* systems, const int32_t* kinds,
+                               uint32_t count, int32_t precision, goss_batch** out);
+GOSS_API int goss_batch_destroy(goss_batch* batch);
+GOSS_API int goss_batch_set_config(goss_batch* batch, uint32_t block, uint32_t grid, uint32_t schedule,
+                                   const uint32_t* order);
+GOSS_API int goss_batch_forward(goss_batch* batch, double t, double interval);
+GOSS_API int goss_batch_capture(goss_batch* batch, double t0, double interval, uint32_t num_steps);
+GOSS_API int goss_batch_replay(goss_batch* batch);
+GOSS_API int goss_batch_time(goss_batch* batch, double t0, double interval, uint32_t num_steps, int32_t use_graph,
+                             float* ms);
+GOSS_API const char* goss_batch_last_error(const goss_batch* batch);
 
 /* Batched model evaluation that allocates no device memory.  No counterpart
  * in the reference: it exists for callers that must not have a library call
