@@ -78,6 +78,35 @@ class ModelDesc(C.Structure):
         ("solver_state_rows", C.CFUNCTYPE(C.c_uint32, C.c_int32)),
         ("op_census_linearized", C.POINTER(C.c_uint32)),
         ("op_census_rhs", C.POINTER(C.c_uint32)),
+        ("adjoint", C.c_void_p),
+    ]
+
+
+class AdjointLaunch(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32),
+        ("solver", C.c_int32),
+        ("precision", C.c_int32),
+        ("num_nodes", C.c_uint32),
+        ("block", C.c_uint32),
+        ("ld", C.c_uint64),
+        ("states", C.c_void_p),
+        ("field_params", C.c_void_p),
+        ("params", C.POINTER(C.c_double)),
+        ("t0", C.c_double),
+        ("interval", C.c_double),
+        ("num_intervals", C.c_uint32),
+        ("steps_per_interval", C.c_uint32),
+        ("checkpoint_every", C.c_uint32),
+        ("trace_state", C.c_uint32),
+        ("checkpoints", C.c_void_p),
+        ("trace", C.c_void_p),
+        ("trace_bar", C.c_void_p),
+        ("scratch", C.c_void_p),
+        ("field_params_bar", C.c_void_p),
+        ("states_bar", C.c_void_p),
+        ("flags", C.c_void_p),
+        ("stream", C.c_void_p),
     ]
 
 

@@ -25,6 +25,7 @@ import sympy as sp
 
 from .ir import CONST, FIELD, STATE, TIME_CLS, Assign, ModelIR, Output, Program, count_ops
 from .odeparse import TIME
+from .ad import ReverseProgram
 from .hoist import ConstantFolder
 from .printer import CPrinter, c_double
 
@@ -323,6 +324,12 @@ class ModelSource:
                         return f"double(F[{j}])" if ctx_double else f"F[{j}]"
                     k = self.pindex[n]
                     return f"PD[{k}]" if ctx_double else f"P[{k}]"
+                if n.startswith("__seed_linear_"):
+                    return f"abar[{int(n[len('__seed_linear_'):])}]"
+                if n.startswith("__seed_rhs_"):
+                    return f"bbar[{int(n[len('__seed_rhs_'):])}]"
+                if n.startswith("__adj_"):
+                    return f"a_{n[len('__adj_'):]}"
                 if n.startswith("__c"):
                     # derived constant, stored after the parameters
                     k = len(self.params) + int(n[3:])
@@ -393,6 +400,41 @@ class ModelSource:
             else:
                 body.append(Output(b.array, b.index, f(b.expr)))
         return Program(prog.name, body, None)
+
+    def _dev_vjp_lines(self, lin_full: Program) -> List[str]:
+        """Body of linearized_vjp: forward sweep, then the reverse sweep."""
+        folded = self._fold(lin_full)
+        inter = {n: self.model.sym(n) for n in self.model.intermediates}
+        rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
+                            [self.model.sym(p) for p in self.fparams], inter)
+        prT, prD = self._dev_printers()
+        lines = []
+        for b in rp.forward:
+            t = "double" if b.cls == TIME_CLS else "T"
+            pr = prD if b.cls == TIME_CLS else prT
+            lines.append(f"const {t} v_{b.name} = {pr(b.expr)};")
+        # the values themselves, then the caller's cotangents for them
+        n = len(self.states)
+        lines.append(f"T lin_v[{n}], rhs_v[{n}], abar[{n}], bbar[{n}];")
+        for o in folded.body:
+            if isinstance(o, Output):
+                arr = "lin_v" if o.array == "linear" else "rhs_v"
+                lines.append(f"{arr}[{o.index}] = {prT(o.expr)};")
+        for i, lt in enumerate(self.linear_terms):
+            pass
+        for i in range(n):
+            if not any(isinstance(o, Output) and o.array == "linear" and o.index == i for o in folded.body):
+                lines.append(f"lin_v[{i}] = T(0.0);")
+            if not any(isinstance(o, Output) and o.array == "rhs" and o.index == i for o in folded.body):
+                lines.append(f"rhs_v[{i}] = T(0.0);")
+        lines.append("seed(lin_v, rhs_v, abar, bbar);")
+        for adj, e in rp.reverse:
+            lines.append(f"const T a_{adj.name[len('__adj_'):]} = {prT(e)};")
+        for i, e in enumerate(rp.state_bar):
+            lines.append(f"ybar[{i}] = {prT(e) if e != 0 else 'T(0.0)'};")
+        for k, e in enumerate(rp.field_bar):
+            lines.append(f"Fbar[{k}] = {prT(e) if e != 0 else 'T(0.0)'};")
+        return lines
 
     def _derived_host_lines(self) -> List[str]:
         """Host code filling C[k] with the derived constants from P."""
@@ -470,6 +512,17 @@ class ModelSource:
         L.append("  {")
         L += ["    " + x for x in head + self._dev_body(lin_full)]
         L.append("    (void)time; (void)P; (void)PD; (void)F;")
+        L.append("  }")
+        L.append("")
+        L.append("  // vector-Jacobian product of linearized (reverse mode, generated): after the forward")
+        L.append("  // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then")
+        L.append("  // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters")
+        L.append("  template <typename T, class Seed>")
+        L.append(f"  __device__ static __forceinline__ void linearized_vjp({sig}, Seed&& seed,")
+        L.append("      T* __restrict__ ybar, T* __restrict__ Fbar)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_vjp_lines(lin_full)]
+        L.append("    (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;")
         L.append("  }")
         if self.mon is not None:
             L.append("")

@@ -1,0 +1,333 @@
+// Adjoint of GRL1 trajectories with checkpointing (one thread per node).
+//
+// Forward (record_kernel): the reference's user loop
+//     for j in 0..J-1:  forward(t0 + j*interval, interval)   (S internal GRL1
+//                       steps, GRL1.cpp:61-82)  and sample the traced state
+// storing the traced state after every interval (the trace) and the full
+// state every K internal steps (checkpoints; K a multiple of S).
+//
+// Backward (adjoint_kernel): given the cotangent of the trace, walk the
+// checkpoint segments from last to first; recompute each segment's K states
+// into per-node scratch, then apply the transposed Jacobian of every GRL1 step
+// in reverse,
+//     Phi_i(y) = y_i + b_i h phi1(a_i h),   (a, b) = linearized(y, t)
+//     lambda  <- lambda + [abar^T d a/dy + bbar^T d b/dy]
+//     abar_i = lambda_i b_i h^2 phi1'(a_i h),  bbar_i = lambda_i h phi1(a_i h)
+// (the reverse sweep of linearized comes from the generated linearized_vjp),
+// adding the trace cotangent to the traced state's lambda at every sample and
+// accumulating the field-parameter gradient.  phi1(x) = (e^x - 1)/x is the
+// same function as the reference's b/a (e^{a h} - 1); the derivative uses
+// the smooth phi1 form.
+#ifndef GOSS_ADJOINT_CUH
+#define GOSS_ADJOINT_CUH
+
+#include "goss_kernels.cuh"
+
+namespace goss_b200 {
+
+// phi1(x) = (e^x - 1)/x and phi1'(x) = (e^x (x - 1) + 1)/x^2 in FP64:
+// Taylor series sum_k x^k/(k+1)! and sum_k (k+1) x^k/(k+2)! for |x| < 0.1
+// (truncation below 1e-17 relative), closed forms otherwise.
+__device__ __forceinline__ double phi1d(double x)
+{
+    if (fabs(x) < 0.1) {
+        double p = 1.0 / 362880.0;
+        p = fma(p, x, 1.0 / 40320.0);
+        p = fma(p, x, 1.0 / 5040.0);
+        p = fma(p, x, 1.0 / 720.0);
+        p = fma(p, x, 1.0 / 120.0);
+        p = fma(p, x, 1.0 / 24.0);
+        p = fma(p, x, 1.0 / 6.0);
+        p = fma(p, x, 0.5);
+        p = fma(p, x, 1.0);
+        return p;
+    }
+    return expm1(x) / x;
+}
+
+__device__ __forceinline__ double dphi1d(double x)
+{
+    if (fabs(x) < 0.1) {
+        // sum_{k=0}^{8} (k+1) x^k / (k+2)!
+        double p = 9.0 / 39916800.0;
+        p = fma(p, x, 8.0 / 3628800.0);
+        p = fma(p, x, 7.0 / 362880.0);
+        p = fma(p, x, 6.0 / 40320.0);
+        p = fma(p, x, 5.0 / 5040.0);
+        p = fma(p, x, 4.0 / 720.0);
+        p = fma(p, x, 3.0 / 120.0);
+        p = fma(p, x, 2.0 / 24.0);
+        p = fma(p, x, 1.0 / 6.0);
+        p = fma(p, x, 0.5);
+        return p;
+    }
+    return (exp(x) * (x - 1.0) + 1.0) / (x * x);
+}
+
+// FP32: Taylor series to x^6 for |x| < 1/4 (truncation < 2e-9), closed forms otherwise
+__device__ __forceinline__ float dphi1f(float x)
+{
+    if (fabsf(x) < 0.25f) {
+        float p = 7.0f / 362880.0f;
+        p = fmaf(p, x, 6.0f / 40320.0f);
+        p = fmaf(p, x, 5.0f / 5040.0f);
+        p = fmaf(p, x, 4.0f / 720.0f);
+        p = fmaf(p, x, 3.0f / 120.0f);
+        p = fmaf(p, x, 2.0f / 24.0f);
+        p = fmaf(p, x, 1.0f / 6.0f);
+        p = fmaf(p, x, 0.5f);
+        return p;
+    }
+    return __fdividef(__expf(x) * (x - 1.0f) + 1.0f, x * x);
+}
+
+__device__ __forceinline__ double phi1t(double x) { return phi1d(x); }
+__device__ __forceinline__ float phi1t(float x) { return phi1f(x); }
+__device__ __forceinline__ double dphi1t(double x) { return dphi1d(x); }
+__device__ __forceinline__ float dphi1t(float x) { return dphi1f(x); }
+
+template <class M, typename T>
+struct AdjointArgs {
+    double* states;            // [n][ld] in: initial, out: final (record)
+    const double* fparams;     // [nfp][ld]
+    void* checkpoints;         // [C][2n][ld] float (FP32: hi, lo) or [C][n][ld] double
+    double* trace;             // [J][ld]
+    const double* trace_bar;   // [J][ld]
+    T* scratch;                // [K][n][ld]
+    double* fparams_bar;       // [nfp][ld]
+    double* states_bar;        // [n][ld]
+    uint32_t* flags;
+    uint64_t ld;
+    uint32_t N;
+    uint32_t num_intervals;    // J
+    uint32_t steps_per_interval;  // S
+    uint32_t checkpoint_every;    // K (multiple of S)
+    uint32_t trace_state;
+    double t0;
+    double interval;
+    T P[Dims<M>::np];
+    double PD[Dims<M>::np];
+};
+
+// checkpoint I/O for the accumulators
+__device__ __forceinline__ void cp_store(void* cp, uint64_t idx_hi, uint64_t idx_lo, const Acc<double>& a)
+{
+    static_cast<double*>(cp)[idx_hi] = a.y;
+    (void)idx_lo;
+}
+__device__ __forceinline__ void cp_store(void* cp, uint64_t idx_hi, uint64_t idx_lo, const Acc<float>& a)
+{
+    static_cast<float*>(cp)[idx_hi] = a.hi;
+    static_cast<float*>(cp)[idx_lo] = a.lo;
+}
+__device__ __forceinline__ void cp_load(const void* cp, uint64_t idx_hi, uint64_t idx_lo, Acc<double>& a)
+{
+    a.y = static_cast<const double*>(cp)[idx_hi];
+    (void)idx_lo;
+}
+__device__ __forceinline__ void cp_load(const void* cp, uint64_t idx_hi, uint64_t idx_lo, Acc<float>& a)
+{
+    a.hi = static_cast<const float*>(cp)[idx_hi];
+    a.lo = static_cast<const float*>(cp)[idx_lo];
+}
+
+template <typename T>
+__host__ __device__ constexpr int cp_rows(int n)
+{
+    return sizeof(T) == 4 ? 2 * n : n;
+}
+
+// one GRL1 step of the adjoint solver's forward (same update as explicit_node)
+template <class M, typename T>
+__device__ __forceinline__ void grl1_step(Acc<T>* y, double lt, T h, const T* P, const double* PD, const T* F)
+{
+    constexpr int n = M::num_states;
+    T yt[n], lin[n], rhs[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+        yt[i] = y[i].value();
+    M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+        y[i].add(grl_increment(lin[i], rhs[i], h, T(1e-8)));
+}
+
+template <class M, typename T>
+__global__ void __launch_bounds__(128) record_kernel(const __grid_constant__ AdjointArgs<M, T> a)
+{
+    constexpr int n = M::num_states;
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= a.N)
+        return;
+    Acc<T> y[n];
+    for (int i = 0; i < n; ++i)
+        y[i].load(a.states[i * a.ld + node]);
+    T F[Dims<M>::nfp];
+    load_field<M, T>(a.fparams, a.ld, node, F);
+    const uint32_t S = a.steps_per_interval, K = a.checkpoint_every;
+    const double ldt = a.interval / S;
+    const T h = T(ldt);
+    constexpr int rows = cp_rows<T>(n);
+    for (uint32_t j = 0; j < a.num_intervals; ++j) {
+        const uint64_t g = (uint64_t)j * S;
+        if (g % K == 0) {
+            const uint64_t c = g / K;
+            for (int i = 0; i < n; ++i)
+                cp_store(a.checkpoints, ((c * rows) + i) * a.ld + node, ((c * rows) + n + i) * a.ld + node, y[i]);
+        }
+        double lt = a.t0 + j * a.interval;
+        for (uint32_t s = 0; s < S; ++s) {
+            grl1_step<M, T>(y, lt, h, a.P, a.PD, F);
+            lt += ldt;
+        }
+        a.trace[(uint64_t)j * a.ld + node] = y[a.trace_state].store();
+    }
+    bool finite = true;
+    for (int i = 0; i < n; ++i) {
+        const double v = y[i].store();
+        a.states[i * a.ld + node] = v;
+        finite = finite && isfinite(v);
+    }
+    if (!finite)
+        atomicOr(a.flags, GOSS_FLAG_NONFINITE);
+}
+
+template <class M, typename T>
+__global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
+{
+    constexpr int n = M::num_states;
+    constexpr int nfp = Dims<M>::nfp;
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ double s_time[];  // time of every step of a segment (same for all nodes)
+    const uint32_t S = a.steps_per_interval, K = a.checkpoint_every;
+    const double ldt = a.interval / S;
+    const T h = T(ldt);
+    const bool active = node < a.N;
+    T F[nfp];
+    if (active)
+        load_field<M, T>(a.fparams, a.ld, node, F);
+    Acc<T> lam[n];
+    for (int i = 0; i < n; ++i)
+        lam[i].load(0.0);
+    double gF[nfp];
+    for (int k = 0; k < nfp; ++k)
+        gF[k] = 0.0;
+    const uint64_t total = (uint64_t)a.num_intervals * S;
+    const uint32_t num_cp = (uint32_t)((total + K - 1) / K);
+    constexpr int rows = cp_rows<T>(n);
+    for (int c = (int)num_cp - 1; c >= 0; --c) {
+        const uint64_t g0 = (uint64_t)c * K;
+        const uint32_t len = (uint32_t)((g0 + K <= total) ? K : total - g0);
+        // times of the segment's steps, exactly as the forward accumulated them
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double lt = 0.0;
+            for (uint32_t k = 0; k < len; ++k) {
+                const uint64_t g = g0 + k;
+                if (g % S == 0)
+                    lt = a.t0 + (g / S) * a.interval;
+                s_time[k] = lt;
+                lt += ldt;
+            }
+        }
+        __syncthreads();
+        if (!active)
+            continue;
+        // recompute the segment, keeping the model input of every step
+        Acc<T> y[n];
+        for (int i = 0; i < n; ++i)
+            cp_load(a.checkpoints, ((uint64_t)c * rows + i) * a.ld + node, ((uint64_t)c * rows + n + i) * a.ld + node,
+                    y[i]);
+        for (uint32_t k = 0; k < len; ++k) {
+            for (int i = 0; i < n; ++i)
+                a.scratch[((uint64_t)k * n + i) * a.ld + node] = y[i].value();
+            if (k + 1 < len)
+                grl1_step<M, T>(y, s_time[k], h, a.P, a.PD, F);
+        }
+        // reverse through the segment
+        for (int k = (int)len - 1; k >= 0; --k) {
+            const uint64_t g = g0 + k;  // step g maps state g to state g+1
+            if ((g + 1) % S == 0) {
+                const uint64_t j = (g + 1) / S - 1;
+                lam[a.trace_state].add(T(a.trace_bar[j * a.ld + node]));
+            }
+            T yt[n], lv[n], ybar[n], Fbar[nfp];
+            for (int i = 0; i < n; ++i) {
+                yt[i] = a.scratch[((uint64_t)k * n + i) * a.ld + node];
+                lv[i] = lam[i].value();
+            }
+            auto seed = [&](const T* lin, const T* rhs, T* abar, T* bbar) {
+#pragma unroll
+                for (int i = 0; i < n; ++i) {
+                    const T x = lin[i] * h;
+                    bbar[i] = lv[i] * h * phi1t(x);
+                    abar[i] = lv[i] * rhs[i] * h * h * dphi1t(x);
+                }
+            };
+            M::template linearized_vjp<T>(yt, s_time[k], a.P, a.PD, F, seed, ybar, Fbar);
+            for (int i = 0; i < n; ++i)
+                lam[i].add(ybar[i]);
+            for (int q = 0; q < M::num_field_params; ++q)
+                gF[q] += double(Fbar[q]);
+        }
+    }
+    if (!active)
+        return;
+    for (int q = 0; q < M::num_field_params; ++q)
+        a.fparams_bar[(uint64_t)q * a.ld + node] = gF[q];
+    for (int i = 0; i < n; ++i)
+        a.states_bar[(uint64_t)i * a.ld + node] = lam[i].store();
+}
+
+template <class M, typename T>
+inline int launch_adjoint_t(const goss_adjoint_launch* L)
+{
+    AdjointArgs<M, T> a;
+    a.states = L->states;
+    a.fparams = L->field_params;
+    a.checkpoints = L->checkpoints;
+    a.trace = L->trace;
+    a.trace_bar = L->trace_bar;
+    a.scratch = static_cast<T*>(L->scratch);
+    a.fparams_bar = L->field_params_bar;
+    a.states_bar = L->states_bar;
+    a.flags = L->flags;
+    a.ld = L->ld;
+    a.N = L->num_nodes;
+    a.num_intervals = L->num_intervals;
+    a.steps_per_interval = L->steps_per_interval;
+    a.checkpoint_every = L->checkpoint_every;
+    a.trace_state = L->trace_state;
+    a.t0 = L->t0;
+    a.interval = L->interval;
+    parameter_block<M>(L->params, a.PD);
+    for (int i = 0; i < Dims<M>::np; ++i)
+        a.P[i] = T(a.PD[i]);
+    if (a.steps_per_interval == 0 || a.checkpoint_every == 0 || a.checkpoint_every % a.steps_per_interval ||
+        a.trace_state >= (uint32_t)M::num_states)
+        return GOSS_ERR_ARGUMENT;
+    const unsigned block = L->block ? L->block : 128;
+    const unsigned grid = (L->num_nodes + block - 1) / block;
+    if (grid == 0)
+        return 0;
+    if (L->mode == 0) {
+        record_kernel<M, T><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    } else {
+        const size_t shm = sizeof(double) * a.checkpoint_every;
+        if (shm > 48 * 1024)
+            return GOSS_ERR_ARGUMENT;
+        adjoint_kernel<M, T><<<grid, block, shm, (cudaStream_t)L->stream>>>(a);
+    }
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
+}
+
+template <class M>
+inline int launch_adjoint(const goss_adjoint_launch* L)
+{
+    if (L->solver != GOSS_GRL1)
+        return GOSS_ERR_UNSUPPORTED;
+    return L->precision == GOSS_FP32 ? launch_adjoint_t<M, float>(L) : launch_adjoint_t<M, double>(L);
+}
+
+}  // namespace goss_b200
+#endif

@@ -128,6 +128,103 @@ struct M_beeler_reuter_1977 {
     linear[7] = ((P[16]*v_di_K1_dV) + (P[16]*v_di_Na_dV) + (P[16]*v_di_s_dV) + (P[16]*v_di_x1_dV));
     (void)time; (void)P; (void)PD; (void)F;
   }
+
+  // vector-Jacobian product of linearized (reverse mode, generated): after the forward
+  // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
+  // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters
+  template <typename T, class Seed>
+  __device__ static __forceinline__ void linearized_vjp(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, Seed&& seed,
+      T* __restrict__ ybar, T* __restrict__ Fbar)
+  {
+    const T s_m = y[0];
+    const T s_h = y[1];
+    const T s_j = y[2];
+    const T s_Cai = y[3];
+    const T s_d = y[4];
+    const T s_f = y[5];
+    const T s_x1 = y[6];
+    const T s_V = y[7];
+    const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
+    const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
+    const T v_alpha_m = (((-T(47.0)) - ((s_V)))/((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0)))));
+    const T v_beta_m = (T(0.7095526727489909)*gexp((-(T(0.056)*s_V))));
+    const T v_alpha_h = (T(5.497962438709065e-10)*gexp((-(T(0.25)*s_V))));
+    const T v_beta_h = (T(1.7)/(T(1.0) + (T(0.1580253208896478)*gexp((-(T(0.082)*s_V))))));
+    const T v_alpha_j = (T(1.8690473007222892e-10)*gexp((-(T(0.25)*s_V)))/(T(1.0) + (T(1.6788275299956603e-07)*gexp((-(T(0.2)*s_V))))));
+    const T v_beta_j = (T(0.3)/(T(1.0) + (T(0.040762203978366204)*gexp((-(T(0.1)*s_V))))));
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*glog((T(0.001)*s_Cai)))));
+    const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
+    const T v_alpha_d = (T(0.095)*gexp((T(0.05) - ((T(0.01)*s_V))))/(T(1.0) + (T(1.4332881385696572)*gexp((-(T(0.07199424046076314)*s_V))))));
+    const T v_beta_d = (T(0.07)*gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))))/(T(1.0) + gexp((T(2.2) + (T(0.05)*s_V)))));
+    const T v_alpha_f = (T(0.012)*gexp(((-T(0.224)) - ((T(0.008)*s_V))))/(T(1.0) + (T(66.5465065250986)*gexp((T(0.14992503748125938)*s_V)))));
+    const T v_beta_f = (T(0.0065)*gexp(((-T(0.6)) - ((T(0.02)*s_V))))/(T(1.0) + gexp(((-T(6.0)) - ((T(0.2)*s_V))))));
+    const T v_i_x1 = (T(0.0019727757115328517)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))));
+    const T v_alpha_x1 = (T(0.031158410986342627)*gexp((T(0.08264462809917356)*s_V))/(T(1.0) + (T(17.41170806332765)*gexp((T(0.05714285714285714)*s_V)))));
+    const T v_beta_x1 = (T(0.0003916464405623223)*gexp((-(T(0.05998800239952009)*s_V)))/(T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V))))));
+    const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
+    const T v_i_K1 = ((T(0.0035)*(T(4.6000000000000005) + (T(0.2)*s_V))/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))));
+    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
+    const T v_dE_s_dCai = (-(T(13.0287)/s_Cai));
+    const T v_di_s_dCai = (P[15]*s_d*v_dE_s_dCai*s_f);
+    const T v_dV_eff_1_dV = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0));
+    const T v_di_K1_dV = ((T(0.0007000000000000001)/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.016779896026542326)*gexp((T(0.04)*s_V))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))*((-(T(0.3332454995075077)*gexp((T(0.04)*s_V)))) - ((T(5.552628147100417)*gexp((T(0.08)*s_V)))))/(((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V)))))) - ((T(0.00028000000000000003)*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V))*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))))));
+    const T v_di_Na_dV = (P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)));
+    const T v_di_s_dV = (s_d*s_f*P[3]);
+    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))))));
+    T lin_v[8], rhs_v[8], abar[8], bbar[8];
+    rhs_v[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
+    rhs_v[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
+    rhs_v[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
+    rhs_v[3] = (T(7.000000000000001e-06) - ((T(0.07)*s_Cai)) - ((T(0.01)*v_i_s)));
+    rhs_v[4] = ((v_alpha_d*(T(1.0) - ((s_d)))) - ((v_beta_d*s_d)));
+    rhs_v[5] = ((v_alpha_f*(T(1.0) - ((s_f)))) - ((v_beta_f*s_f)));
+    rhs_v[6] = ((v_alpha_x1*(T(1.0) - ((s_x1)))) - ((v_beta_x1*s_x1)));
+    rhs_v[7] = (P[14]*(T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1))));
+    lin_v[0] = ((-(v_alpha_m)) - ((v_beta_m)));
+    lin_v[1] = ((-(v_alpha_h)) - ((v_beta_h)));
+    lin_v[2] = ((-(v_alpha_j)) - ((v_beta_j)));
+    lin_v[4] = ((-(v_alpha_d)) - ((v_beta_d)));
+    lin_v[5] = ((-(v_alpha_f)) - ((v_beta_f)));
+    lin_v[6] = ((-(v_alpha_x1)) - ((v_beta_x1)));
+    lin_v[3] = ((-T(0.07)) - ((T(0.01)*v_di_s_dCai)));
+    lin_v[7] = ((P[16]*v_di_K1_dV) + (P[16]*v_di_Na_dV) + (P[16]*v_di_s_dV) + (P[16]*v_di_x1_dV));
+    seed(lin_v, rhs_v, abar, bbar);
+    const T a_di_x1_dV = (P[16]*abar[7]);
+    const T a_di_s_dV = (P[16]*abar[7]);
+    const T a_di_Na_dV = (P[16]*abar[7]);
+    const T a_di_K1_dV = (P[16]*abar[7]);
+    const T a_dV_eff_1_dV = (-(T(0.00028000000000000003)*a_di_K1_dV*(T(4.6000000000000005) + (T(0.2)*s_V))*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1)))))))));
+    const T a_di_s_dCai = (-(T(0.01)*abar[3]));
+    const T a_dE_s_dCai = (a_di_s_dCai*P[15]*s_d*s_f);
+    const T a_i_K1 = (-(P[14]*bbar[7]));
+    const T a_V_eff_1 = ((a_di_K1_dV*((-(T(2.8000000000000003e-05)*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))))) + (T(1.1200000000000001e-05)*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V))*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1)))))))) + (T(2.2400000000000002e-05)*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V))*gexp((-(T(0.08)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1)))))))))) - ((T(0.00014000000000000001)*a_i_K1*(T(4.6000000000000005) + (T(0.2)*s_V))*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))))));
+    const T a_beta_x1 = ((-(abar[6])) - ((bbar[6]*s_x1)));
+    const T a_alpha_x1 = ((-(abar[6])) + (bbar[6]*(T(1.0) - ((s_x1)))));
+    const T a_i_x1 = (-(P[14]*bbar[7]));
+    const T a_beta_f = ((-(abar[5])) - ((bbar[5]*s_f)));
+    const T a_alpha_f = ((-(abar[5])) + (bbar[5]*(T(1.0) - ((s_f)))));
+    const T a_beta_d = ((-(abar[4])) - ((bbar[4]*s_d)));
+    const T a_alpha_d = ((-(abar[4])) + (bbar[4]*(T(1.0) - ((s_d)))));
+    const T a_i_s = ((-(T(0.01)*bbar[3])) - ((P[14]*bbar[7])));
+    const T a_E_s = (-(a_i_s*s_d*s_f*P[3]));
+    const T a_beta_j = ((-(abar[2])) - ((bbar[2]*s_j)));
+    const T a_alpha_j = ((-(abar[2])) + (bbar[2]*(T(1.0) - ((s_j)))));
+    const T a_beta_h = ((-(abar[1])) - ((bbar[1]*s_h)));
+    const T a_alpha_h = ((-(abar[1])) + (bbar[1]*(T(1.0) - ((s_h)))));
+    const T a_beta_m = ((-(abar[0])) - ((bbar[0]*s_m)));
+    const T a_alpha_m = ((-(abar[0])) + (bbar[0]*(T(1.0) - ((s_m)))));
+    const T a_V_eff_0 = (T(0.1)*a_alpha_m*((-T(47.0)) - ((s_V)))*gexp((-(T(0.1)*v_V_eff_0)))/(((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0))))*((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0))))));
+    const T a_i_Na = (-(P[14]*bbar[7]));
+    ybar[0] = ((bbar[0]*((-(v_alpha_m)) - ((v_beta_m)))) + (T(3.0)*a_di_Na_dV*P[1]*s_h*s_j*(s_m*s_m)) + (T(3.0)*a_i_Na*P[1]*s_h*s_j*(s_m*s_m)*(s_V + P[10])));
+    ybar[1] = ((bbar[1]*((-(v_alpha_h)) - ((v_beta_h)))) + (a_di_Na_dV*P[1]*s_j*(s_m*s_m*s_m)) + (a_i_Na*P[1]*s_j*(s_m*s_m*s_m)*(s_V + P[10])));
+    ybar[2] = ((bbar[2]*((-(v_alpha_j)) - ((v_beta_j)))) + (a_di_Na_dV*P[1]*s_h*(s_m*s_m*s_m)) + (a_i_Na*P[1]*s_h*(s_m*s_m*s_m)*(s_V + P[10])));
+    ybar[3] = ((-(T(0.07)*bbar[3])) + (T(13.0287)*a_dE_s_dCai/(s_Cai*s_Cai)) - ((T(13.0287)*a_E_s/s_Cai)));
+    ybar[4] = ((bbar[4]*((-(v_alpha_d)) - ((v_beta_d)))) + (a_di_s_dV*s_f*P[3]) + (a_di_s_dCai*P[15]*v_dE_s_dCai*s_f) + (a_i_s*s_f*P[3]*(s_V - ((v_E_s)))));
+    ybar[5] = ((bbar[5]*((-(v_alpha_f)) - ((v_beta_f)))) + (a_di_s_dV*s_d*P[3]) + (a_di_s_dCai*P[15]*s_d*v_dE_s_dCai) + (a_i_s*s_d*P[3]*(s_V - ((v_E_s)))));
+    ybar[6] = ((a_di_x1_dV*(T(0.0017169779107590322) - ((T(7.891102846131407e-05)*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))))))) + (bbar[6]*((-(v_alpha_x1)) - ((v_beta_x1)))) + (T(0.0019727757115328517)*a_i_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V)))));
+    ybar[7] = ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_alpha_d*((-(T(0.00095)*gexp((T(0.05) - ((T(0.01)*s_V))))/(T(1.0) + (T(1.4332881385696572)*gexp((-(T(0.07199424046076314)*s_V))))))) + (T(0.009802906635285633)*gexp((-(T(0.07199424046076314)*s_V)))*gexp((T(0.05) - ((T(0.01)*s_V))))/((T(1.0) + (T(1.4332881385696572)*gexp((-(T(0.07199424046076314)*s_V)))))*(T(1.0) + (T(1.4332881385696572)*gexp((-(T(0.07199424046076314)*s_V))))))))) + (a_alpha_f*((-(T(9.6e-05)*gexp(((-T(0.224)) - ((T(0.008)*s_V))))/(T(1.0) + (T(66.5465065250986)*gexp((T(0.14992503748125938)*s_V)))))) - ((T(0.11972384982026733)*gexp((T(0.14992503748125938)*s_V))*gexp(((-T(0.224)) - ((T(0.008)*s_V))))/((T(1.0) + (T(66.5465065250986)*gexp((T(0.14992503748125938)*s_V))))*(T(1.0) + (T(66.5465065250986)*gexp((T(0.14992503748125938)*s_V))))))))) + (a_alpha_j*((T(6.275616126633314e-18)*gexp((-(T(0.45)*s_V)))/((T(1.0) + (T(1.6788275299956603e-07)*gexp((-(T(0.2)*s_V)))))*(T(1.0) + (T(1.6788275299956603e-07)*gexp((-(T(0.2)*s_V))))))) - ((T(4.672618251805723e-11)*gexp((-(T(0.25)*s_V)))/(T(1.0) + (T(1.6788275299956603e-07)*gexp((-(T(0.2)*s_V))))))))) + (a_alpha_x1*((T(0.0025750752881274898)*gexp((T(0.08264462809917356)*s_V))/(T(1.0) + (T(17.41170806332765)*gexp((T(0.05714285714285714)*s_V))))) - ((T(0.031001208903507358)*gexp((T(0.1397874852420307)*s_V))/((T(1.0) + (T(17.41170806332765)*gexp((T(0.05714285714285714)*s_V))))*(T(1.0) + (T(17.41170806332765)*gexp((T(0.05714285714285714)*s_V))))))))) + (a_beta_d*((-(T(0.0011864406779661019)*gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))))/(T(1.0) + gexp((T(2.2) + (T(0.05)*s_V)))))) - ((T(0.0035000000000000005)*gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))))*gexp((T(2.2) + (T(0.05)*s_V)))/((T(1.0) + gexp((T(2.2) + (T(0.05)*s_V))))*(T(1.0) + gexp((T(2.2) + (T(0.05)*s_V))))))))) + (a_beta_f*((-(T(0.00013)*gexp(((-T(0.6)) - ((T(0.02)*s_V))))/(T(1.0) + gexp(((-T(6.0)) - ((T(0.2)*s_V))))))) + (T(0.0013)*gexp(((-T(6.0)) - ((T(0.2)*s_V))))*gexp(((-T(0.6)) - ((T(0.02)*s_V))))/((T(1.0) + gexp(((-T(6.0)) - ((T(0.2)*s_V)))))*(T(1.0) + gexp(((-T(6.0)) - ((T(0.2)*s_V))))))))) + (a_beta_x1*((-(T(2.3494087616216093e-05)*gexp((-(T(0.05998800239952009)*s_V)))/(T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V))))))) + (T(1.5665857622492893e-05)*gexp((-(T(0.05998800239952009)*s_V)))*gexp(((-T(0.8)) - ((T(0.04)*s_V))))/((T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V)))))*(T(1.0) + gexp(((-T(0.8)) - ((T(0.04)*s_V))))))))) + (a_di_K1_dV*((T(0.000671195841061693)*gexp((T(0.04)*s_V))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))) + (T(0.03355979205308465)*((-(T(0.3332454995075077)*gexp((T(0.04)*s_V)))) - ((T(5.552628147100417)*gexp((T(0.08)*s_V)))))*gexp((T(0.04)*s_V))/(((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V)))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))*((-(T(0.013329819980300308)*gexp((T(0.04)*s_V)))) - ((T(0.44421025176803336)*gexp((T(0.08)*s_V)))))/(((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V)))))) - ((T(5.6000000000000006e-05)*v_dV_eff_1_dV*gexp((-(T(0.04)*v_V_eff_1)))/((T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))*(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))*((-(T(0.3332454995075077)*gexp((T(0.04)*s_V)))) - ((T(5.552628147100417)*gexp((T(0.08)*s_V)))))*((-(T(0.6664909990150154)*gexp((T(0.04)*s_V)))) - ((T(11.105256294200833)*gexp((T(0.08)*s_V)))))/(((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V)))))))) + (a_di_x1_dV*((-(T(6.867911643036128e-05)*s_x1)) + (T(3.156441138452563e-06)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V)))))) + (a_i_K1*((T(0.0007000000000000001)/(T(1.0) - ((gexp((-(T(0.04)*v_V_eff_1))))))) + (T(0.016779896026542326)*gexp((T(0.04)*s_V))/((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))) + (T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*gexp((T(0.04)*s_V))))*((-(T(0.3332454995075077)*gexp((T(0.04)*s_V)))) - ((T(5.552628147100417)*gexp((T(0.08)*s_V)))))/(((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V))))*((T(8.331137487687693)*gexp((T(0.04)*s_V))) + (T(69.4078518387552)*gexp((T(0.08)*s_V)))))))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) + (a_i_x1*((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*s_x1*((-T(1.0)) + (T(21.75840239619708)*gexp((T(0.04)*s_V))))*gexp((-(T(0.04)*s_V))))))) - ((a_alpha_m/((-T(1.0)) + gexp((-(T(0.1)*v_V_eff_0)))))) - ((T(0.03973494967394349)*a_beta_m*gexp((-(T(0.056)*s_V))))) - ((T(1.3744906096772661e-10)*a_alpha_h*gexp((-(T(0.25)*s_V))))) + (T(0.001222866119350986)*a_beta_j*gexp((-(T(0.1)*s_V)))/((T(1.0) + (T(0.040762203978366204)*gexp((-(T(0.1)*s_V)))))*(T(1.0) + (T(0.040762203978366204)*gexp((-(T(0.1)*s_V))))))) + (T(0.022028729732016906)*a_beta_h*gexp((-(T(0.082)*s_V)))/((T(1.0) + (T(0.1580253208896478)*gexp((-(T(0.082)*s_V)))))*(T(1.0) + (T(0.1580253208896478)*gexp((-(T(0.082)*s_V))))))) + (a_i_s*s_d*s_f*P[3]));
+    (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
+  }
 };
 
 }}  // namespace goss_b200::models

@@ -60,6 +60,31 @@ struct M_fhn {
     linear[0] = v_dI_dv;
     (void)time; (void)P; (void)PD; (void)F;
   }
+
+  // vector-Jacobian product of linearized (reverse mode, generated): after the forward
+  // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
+  // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters
+  template <typename T, class Seed>
+  __device__ static __forceinline__ void linearized_vjp(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, Seed&& seed,
+      T* __restrict__ ybar, T* __restrict__ Fbar)
+  {
+    const T s_v = y[0];
+    const T s_s = y[1];
+    const T v_I = ((P[12]*s_s*(P[11] + s_v)) + (P[14]*(P[11] + s_v)*(P[13] + s_v)*(P[9] - ((s_v)))));
+    const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+    const T v_dI_dv = ((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) + (P[19]*(P[11] + s_v)*(P[13] + s_v)));
+    T lin_v[2], rhs_v[2], abar[2], bbar[2];
+    rhs_v[0] = (v_I + T(v_i_Stim));
+    rhs_v[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
+    lin_v[1] = P[18];
+    lin_v[0] = v_dI_dv;
+    seed(lin_v, rhs_v, abar, bbar);
+    const T a_dI_dv = abar[0];
+    const T a_I = bbar[0];
+    ybar[0] = ((a_I*((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) - ((P[14]*(P[11] + s_v)*(P[13] + s_v))))) + (a_dI_dv*((P[19]*(P[11] + s_v)) + (P[19]*(P[13] + s_v)) - ((P[14]*(P[11] + s_v))) - ((P[14]*(P[13] + s_v))) + (T(2.0)*P[14]*(P[9] - ((s_v)))))) + (bbar[1]*P[1]));
+    ybar[1] = ((a_dI_dv*P[12]) + (a_I*P[12]*(P[11] + s_v)) + (P[17]*bbar[1]*P[1]));
+    (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
+  }
 };
 
 }}  // namespace goss_b200::models

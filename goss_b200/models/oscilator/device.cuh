@@ -45,6 +45,26 @@ struct M_oscilator {
     linear[1] = T(0.0);
     (void)time; (void)P; (void)PD; (void)F;
   }
+
+  // vector-Jacobian product of linearized (reverse mode, generated): after the forward
+  // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
+  // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters
+  template <typename T, class Seed>
+  __device__ static __forceinline__ void linearized_vjp(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, Seed&& seed,
+      T* __restrict__ ybar, T* __restrict__ Fbar)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    T lin_v[2], rhs_v[2], abar[2], bbar[2];
+    rhs_v[0] = (P[2]*s_y);
+    rhs_v[1] = (P[1]*s_x);
+    lin_v[0] = T(0.0);
+    lin_v[1] = T(0.0);
+    seed(lin_v, rhs_v, abar, bbar);
+    ybar[0] = (bbar[1]*P[1]);
+    ybar[1] = (P[2]*bbar[0]);
+    (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
+  }
 };
 
 }}  // namespace goss_b200::models

@@ -1,5 +1,6 @@
 // Generated by goss_b200.codegen for model 'oscilator' (variant oscilator); do not edit.
 // sm_100a solver kernels instantiated for this model and its goss_model_desc factory.
+#include "goss_adjoint.cuh"
 #include "goss_kernels.cuh"
 #include "device.cuh"
 
@@ -17,6 +18,7 @@ static const uint32_t op_rhs[9] = {0, 3, 0, 0, 0, 0, 0, 0, 0};
 int launch(const goss_launch* L) { return goss_b200::launch_solver<Model>(L); }
 int eval(const goss_eval_launch* L) { return goss_b200::launch_eval<Model>(L); }
 uint32_t rows(int32_t s) { return goss_b200::solver_state_rows<Model>(s); }
+int adjoint(const goss_adjoint_launch* L) { return goss_b200::launch_adjoint<Model>(L); }
 }  // namespace
 
 extern "C" GOSS_API const goss_model_desc* goss_b200_model_oscilator(void)
@@ -28,7 +30,7 @@ extern "C" GOSS_API const goss_model_desc* goss_b200_model_oscilator(void)
         state_names, parameter_names, field_parameter_names, field_parameter_indices,
         initial_conditions, default_parameters, linear_terms,
         (1u << GOSS_NUM_SOLVERS) - 1u,
-        launch, eval, rows, op_lin, op_rhs,
+        launch, eval, rows, op_lin, op_rhs, adjoint,
     };
     return &d;
 }

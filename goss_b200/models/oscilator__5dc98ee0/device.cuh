@@ -44,6 +44,28 @@ struct M_oscilator__5dc98ee0 {
     linear[1] = T(0.0);
     (void)time; (void)P; (void)PD; (void)F;
   }
+
+  // vector-Jacobian product of linearized (reverse mode, generated): after the forward
+  // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
+  // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters
+  template <typename T, class Seed>
+  __device__ static __forceinline__ void linearized_vjp(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, Seed&& seed,
+      T* __restrict__ ybar, T* __restrict__ Fbar)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    T lin_v[2], rhs_v[2], abar[2], bbar[2];
+    rhs_v[0] = (-(F[0]*s_y));
+    rhs_v[1] = (F[1]*s_x);
+    lin_v[0] = T(0.0);
+    lin_v[1] = T(0.0);
+    seed(lin_v, rhs_v, abar, bbar);
+    ybar[0] = (bbar[1]*F[1]);
+    ybar[1] = (-(bbar[0]*F[0]));
+    Fbar[0] = (-(bbar[0]*s_y));
+    Fbar[1] = (bbar[1]*s_x);
+    (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
+  }
 };
 
 }}  // namespace goss_b200::models

@@ -122,6 +122,43 @@ typedef struct goss_eval_launch {
     void* stream;
 } goss_eval_launch;
 
+/* Adjoint of a GRL1 trajectory (no counterpart in the reference).  The
+ * trajectory is the reference's user loop: for j < num_intervals,
+ * forward(t0 + j*interval, interval) with steps_per_interval GRL1 steps, the
+ * state trace_state sampled after every interval.
+ *   mode 0 (record): states (in: initial, out: final) -> trace [J][ld] and a
+ *     checkpoint every checkpoint_every steps (a multiple of
+ *     steps_per_interval) in checkpoints: FP32 [C][2n][ld] floats (hi, lo),
+ *     FP64 [C][n][ld] doubles, C = ceil(J*S/K).
+ *   mode 1 (backward): trace_bar [J][ld] = dLoss/dtrace -> field_params_bar
+ *     [nfp][ld] = dLoss/dfield_params and states_bar [n][ld] = dLoss/dstates
+ *     (initial); scratch holds [K][n][ld] values of the arithmetic type. */
+typedef struct goss_adjoint_launch {
+    int32_t mode;
+    int32_t solver;           /* GOSS_GRL1 */
+    int32_t precision;
+    uint32_t num_nodes;
+    uint32_t block;
+    uint64_t ld;
+    double* states;
+    const double* field_params;
+    const double* params;     /* host [num_parameters] */
+    double t0;
+    double interval;
+    uint32_t num_intervals;
+    uint32_t steps_per_interval;
+    uint32_t checkpoint_every;
+    uint32_t trace_state;
+    void* checkpoints;
+    double* trace;
+    const double* trace_bar;
+    void* scratch;
+    double* field_params_bar;
+    double* states_bar;
+    uint32_t* flags;
+    void* stream;
+} goss_adjoint_launch;
+
 /* A compiled model: produced by the code generator for one .ode model and one
  * choice of field parameters; replaces the goss::ParameterizedODE plugin and
  * its extern "C" create_<Name>() factory (python/goss/codegeneration.py:109-112). */
@@ -148,6 +185,8 @@ typedef struct goss_model_desc {
      * evaluation: add, mul, div, exp, log, sqrt, pow, cmp, misc */
     const uint32_t* op_census_linearized;
     const uint32_t* op_census_rhs;
+    /* GRL1 trajectory adjoint (goss_adjoint_launch) */
+    int (*adjoint)(const goss_adjoint_launch* launch);
 } goss_model_desc;
 
 /* One population of a heterogeneous batch (filled by the runtime). */
