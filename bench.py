@@ -258,6 +258,7 @@ def run_gpu(args, rank, world, dist):
     del e2e
 
     out["batched"] = run_batched(args, dev) if not args.skip_fp64 else None
+    out["adjoint"] = run_adjoint(dev) if not args.skip_fp64 else None
 
     times = torch.tensor([ms32, fp64_ms or 0.0, e2e_s], dtype=torch.float64, device="cuda")
     if dist:
@@ -313,6 +314,101 @@ def run_batched(args, dev, steps=1000, dt=0.01, precision="single"):
             "ms": ms, "precision": precision, "graph": True,
             "config": {k: tuned[k] for k in ("block", "grid", "schedule", "order")},
             "populations": [f"{m}/{s}/{n}" for m, _, s, n in BATCH_POPS]}
+
+
+def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, checkpoint_every=100):
+    """Gradient of a V-trace misfit w.r.t. four conductance fields (adjoint).
+
+    TP06 M-cell, GRL1 dt = 0.01 ms, 65,536 nodes, 400 ms (40,000 steps), V
+    sampled every 1 ms; fields lognormal sigma 0.2 (seed A), the target trace
+    from an FP64 solve with seed-B fields; loss = sum (V - V_target)^2;
+    checkpoints every 100 steps.  Times (CUDA events on the launch stream)
+    the FP32 recording forward, the FP32 adjoint and, for the cost ratio, one
+    plain FP32 forward solve of the same 400 ms loop through ODESystemSolver;
+    the FP32 gradient is compared with the FP64 adjoint's (itself checked
+    against the FP64 tangent-linear reference in the tests)."""
+    import torch
+
+    import goss_b200 as goss
+    from goss_b200.adjoint import GRL1Trace
+
+    ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS)
+    defaults = np.array([ode.get_parameter(p) for p in FIELDS])
+    rng_a, rng_b = np.random.default_rng(SEED + 1), np.random.default_rng(SEED + 2)
+    fp_a = defaults[None, :] * np.exp(0.2 * rng_a.standard_normal((nodes, 4)))
+    fp_b = defaults[None, :] * np.exp(0.2 * rng_b.standard_normal((nodes, 4)))
+    y0 = ode.get_ic()[None, :] * (1 + rng_a.uniform(-0.02, 0.02, (nodes, ode.num_states)))
+    cuda = torch.device("cuda", dev)
+    fa, fb, y0t = (torch.tensor(x, device=cuda) for x in (fp_a, fp_b, y0))
+    interval = steps_per_interval * LDT
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def grad(tr, warm=True):
+        if warm:  # one untimed forward + backward
+            v = tr.run_forward(fa, y0t)
+            tr.run_backward(2 * (v - target))
+        torch.cuda.synchronize()
+        s = torch.cuda.current_stream(cuda)
+        e0, e1 = events()
+        e2, e3 = events()
+        e0.record(s)
+        v = tr.run_forward(fa, y0t)
+        e1.record(s)
+        tb = 2 * (v - target)
+        e2.record(s)
+        g, _ = tr.run_backward(tb)
+        e3.record(s)
+        torch.cuda.synchronize()
+        return g.cpu().numpy(), e0.elapsed_time(e1), e2.elapsed_time(e3), float(((v - target) ** 2).sum())
+
+    tr64 = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="double")
+    target = tr64.run_forward(fb, y0t).clone()
+    g64, fwd64, bwd64, loss64 = grad(tr64, warm=False)
+    del tr64
+    tr32 = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="single")
+    g32, fwd32, bwd32, loss32 = grad(tr32)
+    cp_bytes = tr32._checkpoints.numel() * tr32._checkpoints.element_size()
+    del tr32
+
+    # one plain FP32 forward solve of the same loop (ODESystemSolver, persistent kernel per interval)
+    solver = goss.solvers.GRL1(ode)
+    solver.internal_time_step = LDT
+    system = goss.ODESystemSolver(nodes, solver, ode, precision="single", device=dev)
+    system.set_states(y0)
+    system.field_parameters = fp_a
+    system.forward(0.0, interval)  # warm-up
+    system.set_states(y0)
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream(cuda)
+    system.set_stream(s.cuda_stream)
+    e0, e1 = events()
+    e0.record(s)
+    for j in range(num_intervals):
+        system.forward_async(j * interval, interval)
+    e1.record(s)
+    system.synchronize()
+    torch.cuda.synchronize()
+    plain = e0.elapsed_time(e1)
+
+    den = np.maximum(np.abs(g64).max(axis=0), 1e-300)
+    col_err = np.abs(g32 - g64).max(axis=0) / den
+    elem = np.abs(g32 - g64) / np.maximum(np.abs(g64), 1e-12 * den)
+    return {
+        "workload": f"TP06 GRL1 dt=0.01ms, {nodes} nodes, {num_intervals} ms ({num_intervals * steps_per_interval} "
+                    f"steps), V every 1 ms, 4 lognormal conductance fields, checkpoints every {checkpoint_every} "
+                    "steps",
+        "fp32": {"forward_record_ms": fwd32, "backward_ms": bwd32, "loss": loss32},
+        "fp64": {"forward_record_ms": fwd64, "backward_ms": bwd64, "loss": loss64},
+        "plain_forward_fp32_ms": plain,
+        "backward_over_plain_forward": bwd32 / plain,
+        "gradient_over_plain_forward": (fwd32 + bwd32) / plain,
+        "checkpoint_bytes_fp32": int(cp_bytes),
+        "grad_rel_err_fp32_vs_fp64": {"per_field_scaled_max": {f: float(e) for f, e in zip(FIELDS, col_err)},
+                                      "elementwise_median": float(np.median(elem)),
+                                      "elementwise_p99": float(np.quantile(elem, 0.99))},
+    }
 
 
 def roofline(md, value_fp32, ms_per_step, n_nodes):
@@ -460,7 +556,7 @@ def main():
                          if res["fp64_plain_value"] else None,
                          "v_max_rel_err_fp32_vs_fp64": res["v_max_rel_err_fp32_vs_fp64"]},
                 "state_max_rel_err_fp32_vs_fp64": res.get("state_max_rel_err_fp32_vs_fp64"),
-                "batched_heterogeneous": res.get("batched")}
+                "batched_heterogeneous": res.get("batched"), "adjoint": res.get("adjoint")}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -81,7 +81,7 @@ def build_runtime(force: bool = False) -> Path:
 
 def variant_deps(vdir: Path) -> List[Path]:
     return [vdir / "module.cu", vdir / "device.cuh", CSRC / "goss_kernels.cuh", CSRC / "goss_device_math.cuh",
-            INCLUDE / "goss_b200.h"]
+            CSRC / "goss_adjoint.cuh", INCLUDE / "goss_b200.h"]
 
 
 def build_variant(vdir: Path, force: bool = False, extra_flags: Optional[List[str]] = None) -> Path:

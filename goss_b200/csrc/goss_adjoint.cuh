@@ -48,16 +48,16 @@ __device__ __forceinline__ double phi1d(double x)
 __device__ __forceinline__ double dphi1d(double x)
 {
     if (fabs(x) < 0.1) {
-        // sum_{k=0}^{8} (k+1) x^k / (k+2)!
-        double p = 9.0 / 39916800.0;
-        p = fma(p, x, 8.0 / 3628800.0);
-        p = fma(p, x, 7.0 / 362880.0);
-        p = fma(p, x, 6.0 / 40320.0);
-        p = fma(p, x, 5.0 / 5040.0);
-        p = fma(p, x, 4.0 / 720.0);
-        p = fma(p, x, 3.0 / 120.0);
-        p = fma(p, x, 2.0 / 24.0);
-        p = fma(p, x, 1.0 / 6.0);
+        // sum_{k=0}^{9} (k+1) x^k / (k+2)!
+        double p = 10.0 / 39916800.0;
+        p = fma(p, x, 9.0 / 3628800.0);
+        p = fma(p, x, 8.0 / 362880.0);
+        p = fma(p, x, 7.0 / 40320.0);
+        p = fma(p, x, 6.0 / 5040.0);
+        p = fma(p, x, 5.0 / 720.0);
+        p = fma(p, x, 4.0 / 120.0);
+        p = fma(p, x, 3.0 / 24.0);
+        p = fma(p, x, 2.0 / 6.0);
         p = fma(p, x, 0.5);
         return p;
     }
@@ -68,13 +68,14 @@ __device__ __forceinline__ double dphi1d(double x)
 __device__ __forceinline__ float dphi1f(float x)
 {
     if (fabsf(x) < 0.25f) {
-        float p = 7.0f / 362880.0f;
-        p = fmaf(p, x, 6.0f / 40320.0f);
-        p = fmaf(p, x, 5.0f / 5040.0f);
-        p = fmaf(p, x, 4.0f / 720.0f);
-        p = fmaf(p, x, 3.0f / 120.0f);
-        p = fmaf(p, x, 2.0f / 24.0f);
-        p = fmaf(p, x, 1.0f / 6.0f);
+        // sum_{k=0}^{7} (k+1) x^k / (k+2)!
+        float p = 8.0f / 362880.0f;
+        p = fmaf(p, x, 7.0f / 40320.0f);
+        p = fmaf(p, x, 6.0f / 5040.0f);
+        p = fmaf(p, x, 5.0f / 720.0f);
+        p = fmaf(p, x, 4.0f / 120.0f);
+        p = fmaf(p, x, 3.0f / 24.0f);
+        p = fmaf(p, x, 2.0f / 6.0f);
         p = fmaf(p, x, 0.5f);
         return p;
     }

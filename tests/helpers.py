@@ -70,3 +70,28 @@ def parity(a, b, rtol=1e-10, atol=1e-12):
         return float("inf")
     m = np.isfinite(b)
     return float(np.max(np.abs(a[m] - b[m]) / (atol + rtol * np.abs(b[m])))) if m.any() else 0.0
+
+
+def oracle_grl1_traces(name, field_parameters, fp, y0, interval, steps_per_interval, num_intervals, state_index,
+                       t0=0.0):
+    """Oracle (reference semantics) GRL1 traces [J, nodes] of one state: the
+    loop forward(t0 + j*interval, interval), sampled after every interval."""
+    om = oracle_model(name, tuple(field_parameters))
+    y0 = np.atleast_2d(np.asarray(y0, dtype=np.float64))
+    o = pyoracle.OracleSystem(om, "GRL1", y0.shape[0], ldt=interval / steps_per_interval)
+    o.states[:] = y0
+    if om.nfp:
+        o.field_params[:] = fp
+    out = np.zeros((num_intervals, y0.shape[0]))
+    for j in range(num_intervals):
+        o.forward(t0 + j * interval, interval)
+        out[j] = o.states[:, state_index]
+    return out
+
+
+def column_rel_err(a, b):
+    """max over rows of |a-b| / max |b| per column, worst column: the error of
+    a gradient [nodes, inputs] relative to each input's gradient scale."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.max(np.abs(a - b).max(axis=0) / np.maximum(np.abs(b).max(axis=0), 1e-300)))

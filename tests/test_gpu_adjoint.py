@@ -1,15 +1,19 @@
-"""Adjoint of GRL1 traces (goss_b200.adjoint) against finite differences.
+"""Adjoint of GRL1 traces (goss_b200.adjoint) against the FP64 tangent-linear reference.
 
 The trace is the reference's user loop (forward(t0 + j*interval, interval),
 V sampled after each interval); the loss a trace misfit.  Checks:
 
 * the FP64 record kernel reproduces the oracle's trace (the reference's
   GRL1 semantics) to 1e-10;
-* FP64 adjoint gradients w.r.t. the four conductance fields equal central
-  finite differences (relative step 1e-6) of the ORACLE's FP64 loss;
-* the same against GPU FP64 central differences on every node;
+* FP64 adjoint gradients w.r.t. the four conductance fields and the 19
+  initial states equal the FP64 forward-mode tangent-linear reference
+  (oracle/tangent) on every node;
+* they equal central finite differences of the ORACLE's loss as far as
+  finite differences resolve this model (1e-4 for the median over three
+  steps: the sodium-gate rates switch branches discontinuously at V = -40 mV
+  and the upstroke amplifies rounding);
 * checkpoint spacing does not change the gradient;
-* the FP32 adjoint against the FP64 adjoint.
+* the FP32 adjoint against the FP64 tangent-linear reference.
 """
 from __future__ import annotations
 
@@ -19,7 +23,7 @@ import pytest
 import goss_b200 as goss
 import pyoracle
 from goss_b200.adjoint import GRL1Trace, trace
-from helpers import oracle_model, parity
+from helpers import column_rel_err, oracle_grl1_traces, parity
 
 pytestmark = pytest.mark.gpu
 
@@ -42,29 +46,29 @@ def setup(precision="double", K=400, seed=2):
     return ode, tr, fp, y0, target
 
 
-def loss_grad(tr, fp, y0, target):
+def loss_grad(tr, fp, y0, target, with_states=False):
     import torch
 
     p = torch.tensor(fp, device="cuda", requires_grad=True)
-    v = trace(tr, p, torch.tensor(y0, device="cuda"))
+    y = torch.tensor(y0, device="cuda", requires_grad=with_states)
+    v = trace(tr, p, y)
     loss = ((v - target) ** 2).sum()
     loss.backward()
+    if with_states:
+        return float(loss), p.grad.cpu().numpy(), y.grad.cpu().numpy()
     return float(loss), p.grad.cpu().numpy(), v.detach().cpu().numpy()
+
+
+def tangent_grad(ode, fp, y0, target, dirs):
+    """Loss gradient along `dirs` from the FP64 tangent-linear reference."""
+    tl = pyoracle.TangentGRL1(ode.module.dir)
+    tr, jac = tl.trace(y0, fp, ode._params, 0.0, INTERVAL, S, J, ode.state_names.index("V"), dirs)
+    return np.einsum("jn,jnk->nk", 2 * (tr - target), jac)
 
 
 def oracle_traces(ode, fp, y0):
     """Oracle (reference semantics) traces of V for every row of fp."""
-    om = oracle_model(MODEL, tuple(F4))
-    n_sys = fp.shape[0]
-    o = pyoracle.OracleSystem(om, "GRL1", n_sys, ldt=INTERVAL / S)
-    o.states[:] = y0
-    o.field_params[:] = fp
-    iv = ode.state_names.index("V")
-    out = np.zeros((J, n_sys))
-    for j in range(J):
-        o.forward(j * INTERVAL, INTERVAL)
-        out[j] = o.states[:, iv]
-    return out
+    return oracle_grl1_traces(MODEL, F4, fp, y0, INTERVAL, S, J, ode.state_names.index("V"))
 
 
 def test_record_trace_matches_oracle():
@@ -76,37 +80,35 @@ def test_record_trace_matches_oracle():
     assert parity(v, ref, rtol=1e-10, atol=1e-12) <= 1.0
 
 
+def test_fp64_adjoint_matches_tangent_linear():
+    ode, tr, fp, y0, target = setup()
+    _, gfp, gy0 = loss_grad(tr, fp, y0, target, with_states=True)
+    n = ode.num_states
+    ref = tangent_grad(ode, fp, y0, target.cpu().numpy(), list(range(n + 4)))
+    assert column_rel_err(gfp, ref[:, n:]) < 1e-9
+    assert column_rel_err(gy0, ref[:, :n]) < 1e-9
+
+
 def test_adjoint_matches_oracle_central_differences():
     ode, tr, fp, y0, target = setup()
     _, grad, _ = loss_grad(tr, fp, y0, target)
     tgt = target.cpu().numpy()
     nodes = [0, 5, 11, 23]
-    h = 1e-6
-    for k in range(4):
-        fpp, fpm = fp[nodes].copy(), fp[nodes].copy()
-        fpp[:, k] *= 1 + h
-        fpm[:, k] *= 1 - h
-        lp = ((oracle_traces(ode, fpp, y0[nodes]) - tgt[:, nodes]) ** 2).sum(axis=0)
-        lm = ((oracle_traces(ode, fpm, y0[nodes]) - tgt[:, nodes]) ** 2).sum(axis=0)
-        fd = (lp - lm) / (2 * h * fp[nodes, k])
-        np.testing.assert_allclose(grad[nodes, k], fd, rtol=2e-5, atol=1e-9 * np.abs(fd).max())
-
-
-def test_adjoint_matches_gpu_central_differences_all_nodes():
-    import torch
-
-    ode, tr, fp, y0, target = setup()
-    _, grad, _ = loss_grad(tr, fp, y0, target)
-    y0t = torch.tensor(y0, device="cuda")
-    h = 1e-6
-    for k in range(4):
-        fpp, fpm = fp.copy(), fp.copy()
-        fpp[:, k] *= 1 + h
-        fpm[:, k] *= 1 - h
-        lp = ((tr.run_forward(torch.tensor(fpp, device="cuda"), y0t) - target) ** 2).sum(0).cpu().numpy()
-        lm = ((tr.run_forward(torch.tensor(fpm, device="cuda"), y0t) - target) ** 2).sum(0).cpu().numpy()
-        fd = (lp - lm) / (2 * h * fp[:, k])
-        np.testing.assert_allclose(grad[:, k], fd, rtol=2e-5, atol=1e-9 * np.abs(fd).max())
+    iv = ode.state_names.index("V")
+    # a single step is either swamped by rounding amplified through the
+    # upstroke (small h) or crosses a branch switch (large h) for some entry;
+    # the median over three steps is robust to one bad estimate
+    steps = (1e-4, 1e-5, 1e-6)
+    fd = np.zeros((len(steps), len(nodes), 4))
+    for i, h in enumerate(steps):
+        for k in range(4):
+            fpp, fpm = fp[nodes].copy(), fp[nodes].copy()
+            fpp[:, k] *= 1 + h
+            fpm[:, k] *= 1 - h
+            lp = ((oracle_grl1_traces(MODEL, F4, fpp, y0[nodes], INTERVAL, S, J, iv) - tgt[:, nodes]) ** 2).sum(0)
+            lm = ((oracle_grl1_traces(MODEL, F4, fpm, y0[nodes], INTERVAL, S, J, iv) - tgt[:, nodes]) ** 2).sum(0)
+            fd[i, :, k] = (lp - lm) / (2 * h * fp[nodes, k])
+    assert column_rel_err(grad[nodes], np.median(fd, axis=0)) < 1e-4
 
 
 def test_checkpoint_spacing_does_not_change_gradient():
@@ -114,13 +116,14 @@ def test_checkpoint_spacing_does_not_change_gradient():
     _, ga, _ = loss_grad(tr_a, fp, y0, target)
     _, tr_b, _, _, _ = setup(K=800)
     _, gb, _ = loss_grad(tr_b, fp, y0, target)
-    assert np.array_equal(ga, gb)
+    # the recomputed segments are the recorded trajectory up to rounding
+    assert np.abs(ga - gb).max() <= 1e-10 * np.abs(ga).max()
 
 
-def test_fp32_adjoint_close_to_fp64():
+def test_fp32_adjoint_close_to_tangent_linear():
     ode, tr64, fp, y0, target = setup("double")
-    _, g64, _ = loss_grad(tr64, fp, y0, target)
+    ref = tangent_grad(ode, fp, y0, target.cpu().numpy(), [ode.num_states + k for k in range(4)])
     _, tr32, _, _, _ = setup("single")
     _, g32, _ = loss_grad(tr32, fp, y0, target)
-    rel = np.abs(g32 - g64).max() / np.abs(g64).max()
+    rel = column_rel_err(g32, ref)
     assert rel < 1e-3, rel
