@@ -72,7 +72,7 @@ class GRL1Trace:
         rows = 2 * self.n if self.precision == _capi.GOSS_FP32 else self.n
         dev = self.device
         self._checkpoints = torch.zeros((self.num_checkpoints, rows, self.ld), dtype=cp_dtype, device=dev)
-        self._scratch = torch.zeros((self.K, self.n, self.ld), dtype=cp_dtype, device=dev)
+        self._scratch = torch.zeros((self.K, self.n, (self.N + 255) // 256 * 256), dtype=cp_dtype, device=dev)
         self._states = torch.zeros((self.n, self.ld), dtype=torch.float64, device=dev)
         self._fp = torch.zeros((max(self.nfp, 1), self.ld), dtype=torch.float64, device=dev)
         self._trace = torch.zeros((self.J, self.ld), dtype=torch.float64, device=dev)
@@ -80,6 +80,7 @@ class GRL1Trace:
         self._fn = _AdjointFn(ode.module.desc.contents.adjoint)
         if not ode.module.desc.contents.adjoint:
             raise _capi.ExtensionMissingError("the model module has no adjoint kernels")
+        self.block = 0  # backward threads per block (0: the module's compiled default)
         self.final_states: Optional[object] = None
 
     def _launch(self, mode: int, trace_bar=None, fp_bar=None, states_bar=None) -> None:
@@ -90,7 +91,7 @@ class GRL1Trace:
         L.solver = _capi.GOSS_GRL1
         L.precision = self.precision
         L.num_nodes = self.N
-        L.block = 128
+        L.block = self.block
         L.ld = self.ld
         L.states = self._states.data_ptr()
         L.field_params = self._fp.data_ptr()

@@ -13,57 +13,193 @@ forward sweep that recomputes the program's values:
     reverse sweep:  a_j = sum_{k reads v_j} a_k * d f_k / d v_j   (j = J..1)
     results:        ybar_m = sum over statements reading state m, likewise F
 
-Partial derivatives are sympy derivatives of each statement with respect to
-its direct inputs (intermediates as independent symbols), with floor
-derivatives 0 and |x|' = sign(x) as a Piecewise.
+With ``elementary=True`` (the default) the active statements are first split
+so that every transcendental operation is a statement of its own: each
+``exp(u)``, ``log(u)``, ``sqrt(u)``, ``u**p`` (p not an integer) and each
+denominator of a product (one reciprocal ``1/(d_1 d_2 ...)`` per product)
+becomes a value ``__t<k>`` computed once in the forward sweep, shared by all
+statements with the same operand.  Their partial derivatives are written in
+terms of those values -- d exp(u) = exp(u) du, d(1/D) = -(1/D)^2 dD,
+d log(u) = (1/u) du, d sqrt(u) = du / (2 sqrt(u)) -- so the reverse sweep is
+multiplications and additions only; the transcendental work of a VJP is that
+of one forward evaluation.  Conditionals (``Piecewise``) are kept whole.
+
+Partial derivatives of the remaining statements are sympy derivatives with
+respect to their direct inputs (intermediates as independent symbols), with
+floor derivatives 0 and |x|' = sign(x) as a Piecewise.
 """
 from __future__ import annotations
 
-from collections import OrderedDict, defaultdict
+from collections import defaultdict
 from typing import Dict, List, Sequence, Set, Tuple
 
 import sympy as sp
 
-from .ir import CONST, TIME_CLS, Assign, Output, Program, clean
+from .ir import CONST, STATE, TIME_CLS, Assign, Output, Program, clean
+
+
+class _Splitter:
+    """Rewrites active expressions so that transcendental operations are
+    separate values (see the module docstring), recording their partials."""
+
+    def __init__(self, active: Set[sp.Symbol]):
+        self.active = active
+        self.memo: Dict[sp.Expr, sp.Symbol] = {}
+        self.nodes: List[Tuple[sp.Symbol, sp.Expr, Dict[sp.Symbol, sp.Expr]]] = []
+        self._count = 0
+
+    def _is_active(self, e: sp.Expr) -> bool:
+        return bool(e.free_symbols & self.active)
+
+    def _node(self, expr: sp.Expr, partials) -> sp.Symbol:
+        s = self.memo.get(expr)
+        if s is not None:
+            return s
+        s = sp.Symbol(f"__t{self._count}", real=True)
+        self._count += 1
+        self.memo[expr] = s
+        slot = len(self.nodes)
+        self.nodes.append((s, expr, {}))
+        self.active.add(s)
+        self.nodes[slot] = (s, expr, partials(s))
+        return s
+
+    def _chain(self, outer: sp.Expr, u: sp.Expr) -> Dict[sp.Symbol, sp.Expr]:
+        """{x: outer * du/dx} over the active symbols x of u."""
+        out = {}
+        for x in sorted(u.free_symbols & self.active, key=lambda q: q.name):
+            d = clean(sp.diff(u, x))
+            if d != 0:
+                out[x] = outer * d
+        return out
+
+    def recip(self, d: sp.Expr) -> sp.Symbol:
+        return self._node(sp.Pow(d, -1, evaluate=False), lambda r: self._chain(-r * r, d))
+
+    def exp(self, u: sp.Expr) -> sp.Symbol:
+        return self._node(sp.exp(u), lambda e: self._chain(e, u))
+
+    def log(self, u: sp.Expr) -> sp.Symbol:
+        return self._node(sp.log(u), lambda l: self._chain(self.recip(u), u))
+
+    def sqrt(self, u: sp.Expr) -> sp.Symbol:
+        return self._node(sp.Pow(u, sp.Rational(1, 2), evaluate=False),
+                          lambda s: self._chain(sp.Rational(1, 2) * self.recip(s), u))
+
+    def power(self, b: sp.Expr, p: sp.Expr) -> sp.Symbol:
+        """b**p with an inactive, non-integer exponent."""
+        return self._node(sp.Pow(b, p, evaluate=False), lambda q: self._chain(p * q * self.recip(b), b))
+
+    def _positive_power(self, b: sp.Expr, p: sp.Expr) -> sp.Expr:
+        """Transformed b**p for an active base b and an inactive exponent p."""
+        if p.is_Integer:
+            return b ** p if p > 0 else self.recip(b ** (-p))
+        if p == sp.Rational(1, 2):
+            return self.sqrt(b)
+        if p == sp.Rational(-1, 2):
+            return self.recip(self.sqrt(b))
+        return self.power(b, p)
+
+    def tx(self, e: sp.Expr) -> sp.Expr:
+        if e.is_Atom or not self._is_active(e) or isinstance(e, sp.Piecewise):
+            return e
+        if isinstance(e, sp.Mul):
+            num, den = [], []
+            for f in e.args:
+                if f.is_Pow and self._is_active(f.base) and f.exp.is_Number and f.exp < 0:
+                    den.append(self._positive_power(self.tx(f.base), -f.exp))
+                else:
+                    num.append(self.tx(f))
+            if den:
+                num.append(self.recip(sp.Mul(*den)))
+            return sp.Mul(*num)
+        if isinstance(e, sp.Pow):
+            b, p = e.base, e.exp
+            if b is sp.E:
+                return self.exp(self.tx(p))
+            if self._is_active(p):
+                return e.func(self.tx(b), self.tx(p))
+            if not self._is_active(b):
+                return e
+            return self._positive_power(self.tx(b), p)
+        if isinstance(e, sp.exp):
+            return self.exp(self.tx(e.args[0]))
+        if isinstance(e, sp.log) and len(e.args) == 1:
+            return self.log(self.tx(e.args[0]))
+        return e.func(*[self.tx(a) for a in e.args])
 
 
 class ReverseProgram:
-    """Statements of the forward sweep and the reverse sweep."""
+    """Statements of the forward sweep and the reverse sweep.
+
+    ``forward``: the forward sweep's assignments in order (with the split
+    values when ``elementary``); ``outputs``: the program's outputs in terms
+    of them; ``seeds``: (symbol, array, index) of the output cotangents;
+    ``reverse``: (adjoint symbol, value) in evaluation order; ``state_bar`` and
+    ``field_bar``: the VJP's results.
+    """
 
     def __init__(self, prog: Program, state_syms: Sequence[sp.Symbol], field_syms: Sequence[sp.Symbol],
-                 inter_syms: Dict[str, sp.Symbol]):
-        self.forward: List[Assign] = [b for b in prog.body if isinstance(b, Assign)]
-        outputs = [b for b in prog.body if isinstance(b, Output)]
+                 inter_syms: Dict[str, sp.Symbol], elementary: bool = True):
         self.state_syms = list(state_syms)
         self.field_syms = list(field_syms)
         sym_of = dict(inter_syms)
         active: Set[sp.Symbol] = set(self.state_syms) | set(self.field_syms)
+        splitter = _Splitter(active) if elementary else None
+        node_partials: Dict[sp.Symbol, Dict[sp.Symbol, sp.Expr]] = {}
+        self.forward: List[Assign] = []
         self.active_assigns: List[Tuple[sp.Symbol, Assign]] = []
-        for b in self.forward:
-            s = sym_of.get(b.name) or sp.Symbol(b.name, real=True)
-            if b.cls in (CONST, TIME_CLS):
+
+        def split(expr: sp.Expr, cls: int) -> sp.Expr:
+            if splitter is None:
+                return expr
+            start = len(splitter.nodes)
+            expr = splitter.tx(expr)
+            for ns, ne, part in splitter.nodes[start:]:
+                nb = Assign(ns.name, ne, cls)
+                self.forward.append(nb)
+                self.active_assigns.append((ns, nb))
+                node_partials[ns] = part
+            return expr
+
+        for b in prog.body:
+            if not isinstance(b, Assign):
                 continue
-            if b.expr.free_symbols & active:
-                active.add(s)
-                self.active_assigns.append((s, b))
+            s = sym_of.get(b.name) or sp.Symbol(b.name, real=True)
+            if b.cls in (CONST, TIME_CLS) or not (b.expr.free_symbols & active):
+                self.forward.append(b)
+                continue
+            nb = Assign(b.name, split(b.expr, b.cls), b.cls)
+            active.add(s)
+            self.forward.append(nb)
+            self.active_assigns.append((s, nb))
+        self.outputs: List[Output] = []
+        for o in prog.body:
+            if isinstance(o, Output):
+                expr = split(o.expr, STATE) if (o.expr.free_symbols & active) else o.expr
+                self.outputs.append(Output(o.array, o.index, expr))
         self.active = active
-        # contributions[u] = list of (adjoint expression, partial expression)
+        # contributions[u] = adjoint-weighted partials of the statements reading u
         contrib: Dict[sp.Symbol, List[sp.Expr]] = defaultdict(list)
         self.seeds = []
-        for o in outputs:
+        for o in self.outputs:
             seed = sp.Symbol(f"__seed_{o.array}_{o.index}", real=True)
             self.seeds.append((seed, o.array, o.index))
             for u in sorted(o.expr.free_symbols & active, key=lambda q: q.name):
                 d = clean(sp.diff(o.expr, u))
                 if d != 0:
                     contrib[u].append(seed * d)
-        self.reverse: List[Tuple[sp.Symbol, sp.Expr]] = []  # (adjoint symbol, value)
+        self.reverse: List[Tuple[sp.Symbol, sp.Expr]] = []
         for s, b in reversed(self.active_assigns):
             terms = contrib.pop(s, [])
             if not terms:
                 continue
             adj = sp.Symbol(f"__adj_{s.name}", real=True)
             self.reverse.append((adj, sp.Add(*terms)))
+            if s in node_partials:
+                for u, d in node_partials[s].items():
+                    contrib[u].append(adj * d)
+                continue
             for u in sorted(b.expr.free_symbols & active, key=lambda q: q.name):
                 d = clean(sp.diff(b.expr, u))
                 if d != 0:

@@ -416,16 +416,13 @@ class ModelSource:
         # the values themselves, then the caller's cotangents for them
         n = len(self.states)
         lines.append(f"T lin_v[{n}], rhs_v[{n}], abar[{n}], bbar[{n}];")
-        for o in folded.body:
-            if isinstance(o, Output):
-                arr = "lin_v" if o.array == "linear" else "rhs_v"
-                lines.append(f"{arr}[{o.index}] = {prT(o.expr)};")
-        for i, lt in enumerate(self.linear_terms):
-            pass
+        for o in rp.outputs:
+            arr = "lin_v" if o.array == "linear" else "rhs_v"
+            lines.append(f"{arr}[{o.index}] = {prT(o.expr)};")
         for i in range(n):
-            if not any(isinstance(o, Output) and o.array == "linear" and o.index == i for o in folded.body):
+            if not any(o.array == "linear" and o.index == i for o in rp.outputs):
                 lines.append(f"lin_v[{i}] = T(0.0);")
-            if not any(isinstance(o, Output) and o.array == "rhs" and o.index == i for o in folded.body):
+            if not any(o.array == "rhs" and o.index == i for o in rp.outputs):
                 lines.append(f"rhs_v[{i}] = T(0.0);")
         lines.append("seed(lin_v, rhs_v, abar, bbar);")
         for adj, e in rp.reverse:

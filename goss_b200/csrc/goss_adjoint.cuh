@@ -23,6 +23,26 @@
 
 #include "goss_kernels.cuh"
 
+// Launch shape of the adjoint kernel: threads per block (at most 256, a
+// power of two) and the minimum resident blocks per SM it is compiled for
+// (its register cap is 65536 / (threads * blocks)).  With GOSS_ADJOINT_LOCKSTEP
+// the warps of a block synchronise after every step of the recompute and
+// reverse loops, so they walk the large straight-line step code together and
+// share instruction-cache lines.  Measured on B200 (ten Tusscher-Panfilov,
+// FP32, 65,536 nodes x 2,000 steps): 256 threads x 1 block in lockstep
+// 43.5 ms; 256 x 1 without lockstep 46.8 ms; 128 x 2 in lockstep 47.7 ms,
+// without 50.4 ms; register caps of 168 or 128 (3 or 4 blocks of 128) spill
+// more than the extra warps gain (65-67 ms).
+#ifndef GOSS_ADJOINT_BLOCK
+#define GOSS_ADJOINT_BLOCK 256
+#endif
+#ifndef GOSS_ADJOINT_MIN_BLOCKS
+#define GOSS_ADJOINT_MIN_BLOCKS 1
+#endif
+#ifndef GOSS_ADJOINT_LOCKSTEP
+#define GOSS_ADJOINT_LOCKSTEP 1
+#endif
+
 namespace goss_b200 {
 
 // phi1(x) = (e^x - 1)/x and phi1'(x) = (e^x (x - 1) + 1)/x^2 in FP64:
@@ -94,11 +114,12 @@ struct AdjointArgs {
     void* checkpoints;         // [C][2n][ld] float (FP32: hi, lo) or [C][n][ld] double
     double* trace;             // [J][ld]
     const double* trace_bar;   // [J][ld]
-    T* scratch;                // [K][n][ld]
+    T* scratch;                // [K][n][sld], sld = num_nodes rounded up to 256
     double* fparams_bar;       // [nfp][ld]
     double* states_bar;        // [n][ld]
     uint32_t* flags;
     uint64_t ld;
+    uint64_t sld;              // scratch row stride (>= grid * block)
     uint32_t N;
     uint32_t num_intervals;    // J
     uint32_t steps_per_interval;  // S
@@ -194,19 +215,22 @@ __global__ void __launch_bounds__(128) record_kernel(const __grid_constant__ Adj
 }
 
 template <class M, typename T>
-__global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
+__global__ void __launch_bounds__(GOSS_ADJOINT_BLOCK, GOSS_ADJOINT_MIN_BLOCKS)
+adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
 {
     constexpr int n = M::num_states;
     constexpr int nfp = Dims<M>::nfp;
+    // Every thread runs every loop (block-wide barriers below); threads past
+    // the last node shadow it (reads only) and keep their own scratch column.
     const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = node < a.N;
+    const uint32_t src = active ? node : a.N - 1;
     extern __shared__ double s_time[];  // time of every step of a segment (same for all nodes)
     const uint32_t S = a.steps_per_interval, K = a.checkpoint_every;
     const double ldt = a.interval / S;
     const T h = T(ldt);
-    const bool active = node < a.N;
     T F[nfp];
-    if (active)
-        load_field<M, T>(a.fparams, a.ld, node, F);
+    load_field<M, T>(a.fparams, a.ld, src, F);
     Acc<T> lam[n];
     for (int i = 0; i < n; ++i)
         lam[i].load(0.0);
@@ -216,6 +240,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ Ad
     const uint64_t total = (uint64_t)a.num_intervals * S;
     const uint32_t num_cp = (uint32_t)((total + K - 1) / K);
     constexpr int rows = cp_rows<T>(n);
+    T* const scratch = a.scratch + node;
     for (int c = (int)num_cp - 1; c >= 0; --c) {
         const uint64_t g0 = (uint64_t)c * K;
         const uint32_t len = (uint32_t)((g0 + K <= total) ? K : total - g0);
@@ -232,29 +257,30 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ Ad
             }
         }
         __syncthreads();
-        if (!active)
-            continue;
         // recompute the segment, keeping the model input of every step
         Acc<T> y[n];
         for (int i = 0; i < n; ++i)
-            cp_load(a.checkpoints, ((uint64_t)c * rows + i) * a.ld + node, ((uint64_t)c * rows + n + i) * a.ld + node,
+            cp_load(a.checkpoints, ((uint64_t)c * rows + i) * a.ld + src, ((uint64_t)c * rows + n + i) * a.ld + src,
                     y[i]);
         for (uint32_t k = 0; k < len; ++k) {
             for (int i = 0; i < n; ++i)
-                a.scratch[((uint64_t)k * n + i) * a.ld + node] = y[i].value();
+                scratch[((uint64_t)k * n + i) * a.sld] = y[i].value();
             if (k + 1 < len)
                 grl1_step<M, T>(y, s_time[k], h, a.P, a.PD, F);
+#if GOSS_ADJOINT_LOCKSTEP
+            __syncthreads();
+#endif
         }
         // reverse through the segment
         for (int k = (int)len - 1; k >= 0; --k) {
             const uint64_t g = g0 + k;  // step g maps state g to state g+1
             if ((g + 1) % S == 0) {
                 const uint64_t j = (g + 1) / S - 1;
-                lam[a.trace_state].add(T(a.trace_bar[j * a.ld + node]));
+                lam[a.trace_state].add(T(a.trace_bar[j * a.ld + src]));
             }
             T yt[n], lv[n], ybar[n], Fbar[nfp];
             for (int i = 0; i < n; ++i) {
-                yt[i] = a.scratch[((uint64_t)k * n + i) * a.ld + node];
+                yt[i] = scratch[((uint64_t)k * n + i) * a.sld];
                 lv[i] = lam[i].value();
             }
             auto seed = [&](const T* lin, const T* rhs, T* abar, T* bbar) {
@@ -270,6 +296,9 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ Ad
                 lam[i].add(ybar[i]);
             for (int q = 0; q < M::num_field_params; ++q)
                 gF[q] += double(Fbar[q]);
+#if GOSS_ADJOINT_LOCKSTEP
+            __syncthreads();
+#endif
         }
     }
     if (!active)
@@ -307,13 +336,19 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
     if (a.steps_per_interval == 0 || a.checkpoint_every == 0 || a.checkpoint_every % a.steps_per_interval ||
         a.trace_state >= (uint32_t)M::num_states)
         return GOSS_ERR_ARGUMENT;
-    const unsigned block = L->block ? L->block : 128;
-    const unsigned grid = (L->num_nodes + block - 1) / block;
-    if (grid == 0)
+    a.sld = ((uint64_t)L->num_nodes + 255) / 256 * 256;
+    if (L->num_nodes == 0)
         return 0;
     if (L->mode == 0) {
+        const unsigned block = 128;
+        const unsigned grid = (L->num_nodes + block - 1) / block;
         record_kernel<M, T><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
     } else {
+        // power-of-two blocks up to the compiled bound keep grid * block <= sld
+        unsigned block = L->block ? L->block : GOSS_ADJOINT_BLOCK;
+        if (block > GOSS_ADJOINT_BLOCK || block < 32 || (block & (block - 1)))
+            return GOSS_ERR_ARGUMENT;
+        const unsigned grid = (L->num_nodes + block - 1) / block;
         const size_t shm = sizeof(double) * a.checkpoint_every;
         if (shm > 48 * 1024)
             return GOSS_ERR_ARGUMENT;

@@ -222,13 +222,37 @@ class TangentGRL1:
         self.num_params = self.lib.tangent_num_params()
         self.num_derived = self.lib.tangent_num_derived()
 
+    def _pvec(self, params):
+        P = np.zeros(self.num_params + self.num_derived)
+        P[: self.num_params] = params
+        return P
+
+    def jvp(self, y, F, params, time, ydot, Fdot):
+        """(linear, rhs, linear_dot, rhs_dot) of one evaluation along (ydot, Fdot)."""
+        f64 = lambda a, n: np.ascontiguousarray(np.resize(np.asarray(a, dtype=np.float64), max(n, 1)))
+        y, ydot = f64(y, self.n), f64(ydot, self.n)
+        F, Fdot = f64(F if self.nfp else [0.0], self.nfp), f64(Fdot if self.nfp else [0.0], self.nfp)
+        out = [np.zeros(self.n) for _ in range(4)]
+        self.lib.tangent_jvp(_ptr(y), _ptr(F), _ptr(self._pvec(params)), C.c_double(time), _ptr(ydot), _ptr(Fdot),
+                             *[_ptr(o) for o in out])
+        return tuple(out)
+
+    def vjp(self, y, F, params, time, abar, bbar):
+        """(ybar, Fbar) of one evaluation from the generated reverse sweep."""
+        f64 = lambda a, n: np.ascontiguousarray(np.resize(np.asarray(a, dtype=np.float64), max(n, 1)))
+        y, abar, bbar = f64(y, self.n), f64(abar, self.n), f64(bbar, self.n)
+        F = f64(F if self.nfp else [0.0], self.nfp)
+        ybar, Fbar = np.zeros(self.n), np.zeros(max(self.nfp, 1))
+        self.lib.tangent_vjp(_ptr(y), _ptr(F), _ptr(self._pvec(params)), C.c_double(time), _ptr(abar), _ptr(bbar),
+                             _ptr(ybar), _ptr(Fbar))
+        return ybar, Fbar[: self.nfp]
+
     def trace(self, states0, field_params, params, t0, interval, steps_per_interval, num_intervals, trace_state,
               dirs, delta=1e-8):
         y0 = np.ascontiguousarray(states0, dtype=np.float64).reshape(-1, self.n)
         N = y0.shape[0]
         fp = np.ascontiguousarray(field_params if self.nfp else np.zeros((N, 1)), dtype=np.float64)
-        P = np.zeros(self.num_params + self.num_derived)
-        P[: self.num_params] = params
+        P = self._pvec(params)
         d = np.ascontiguousarray(dirs, dtype=np.uint32)
         tr = np.zeros((num_intervals, N))
         jac = np.zeros((num_intervals, N, len(d)))

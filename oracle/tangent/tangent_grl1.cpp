@@ -133,3 +133,68 @@ __attribute__((visibility("default"))) int tangent_grl1_trace(
 }
 
 }  // extern "C"
+
+// Single-evaluation checks of the generated model code (one state, one time):
+//   tangent_jvp: (linear, rhs) and their directional derivatives along
+//                (ydot, Fdot), by dual numbers through `linearized`;
+//   tangent_vjp: ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar, by
+//                the generated reverse sweep `linearized_vjp` in FP64.
+// A dot-product test <abar, lin_dot> + <bbar, rhs_dot> = <ybar, ydot> +
+// <Fbar, Fdot> then checks the reverse sweep against forward mode.
+// params as for tangent_grl1_trace (derived constants filled in here).
+extern "C" {
+
+__attribute__((visibility("default"))) int tangent_jvp(const double* y, const double* F, double* params,
+                                                       double time, const double* ydot, const double* Fdot,
+                                                       double* lin, double* rhs, double* lin_dot, double* rhs_dot)
+{
+    using T = Dual<1>;
+    Model::derived(params, params + Model::num_params);
+    std::vector<T> P(kParams);
+    for (int i = 0; i < kParams; ++i)
+        P[i] = T(params[i]);
+    T yd[kStates], Fd[kFields], l[kStates], r[kStates];
+    for (int i = 0; i < kStates; ++i) {
+        yd[i] = T(y[i]);
+        yd[i].d[0] = ydot[i];
+        l[i] = T(0.0);
+        r[i] = T(0.0);
+    }
+    for (int f = 0; f < Model::num_field_params; ++f) {
+        Fd[f] = T(F[f]);
+        Fd[f].d[0] = Fdot[f];
+    }
+    Model::template linearized<T>(yd, time, P.data(), params, Fd, l, r);
+    for (int i = 0; i < kStates; ++i) {
+        lin[i] = l[i].v;
+        rhs[i] = r[i].v;
+        lin_dot[i] = l[i].d[0];
+        rhs_dot[i] = r[i].d[0];
+    }
+    return 0;
+}
+
+__attribute__((visibility("default"))) int tangent_vjp(const double* y, const double* F, double* params,
+                                                       double time, const double* abar, const double* bbar,
+                                                       double* ybar, double* Fbar)
+{
+    Model::derived(params, params + Model::num_params);
+    double Fl[kFields] = {0.0};
+    for (int f = 0; f < Model::num_field_params; ++f)
+        Fl[f] = F[f];
+    double yb[kStates], Fb[kFields];
+    auto seed = [&](const double*, const double*, double* ab, double* bb) {
+        for (int i = 0; i < kStates; ++i) {
+            ab[i] = abar[i];
+            bb[i] = bbar[i];
+        }
+    };
+    Model::template linearized_vjp<double>(y, time, params, params, Fl, seed, yb, Fb);
+    for (int i = 0; i < kStates; ++i)
+        ybar[i] = yb[i];
+    for (int f = 0; f < Model::num_field_params; ++f)
+        Fbar[f] = Fb[f];
+    return 0;
+}
+
+}  // extern "C"

@@ -89,3 +89,36 @@ def test_bad_arguments_raise():
         tl.trace(y0, fp, params, 0.0, 1.0, 10, 2, 0, [om.n + 2])     # no such field
     with pytest.raises(ValueError):
         tl.trace(y0, fp, params, 0.0, 1.0, 10, 2, 0, list(range(33)) )
+
+
+FIELD_VARIANTS = [("fitzhughnagumo", ["a", "b"]), ("oscilator", ["a", "b"]),
+                  ("tentusscher_2004_mcell", ["g_Kr", "g_CaL"]),
+                  ("tentusscher_2004_mcell", ["g_Kr", "g_Na", "g_Ks"]),
+                  ("tentusscher_2004_mcell", ["g_Kr", "g_Ks", "g_CaL", "g_to"]),
+                  ("tentusscher_panfilov_2006_M_cell", ["g_Kr", "g_Ks", "g_CaL", "g_to"])]
+
+
+@pytest.mark.parametrize("name,fields", FIELD_VARIANTS, ids=lambda v: v if isinstance(v, str) else "-".join(v))
+def test_generated_vjp_dot_product(name, fields):
+    """The generated reverse sweep (linearized_vjp, compiled for the host in
+    FP64) is the transpose of the forward-mode derivative of `linearized`:
+    <abar, lin_dot> + <bbar, rhs_dot> = <ybar, ydot> + <Fbar, Fdot> for random
+    directions and cotangents, at states on both sides of V = -40 mV."""
+    tl, om, md, params, fp, y0 = _setup(name, fields, 6, seed=11)
+    rng = np.random.default_rng(5)
+    names = md["state_names"]
+    worst = 0.0
+    for node in range(6):
+        y = y0[node].copy()
+        if "V" in names:
+            y[names.index("V")] = (-85.0, -60.0, -39.0, -20.0, 5.0, 30.0)[node]
+        ydot = rng.standard_normal(om.n) * np.maximum(np.abs(y), 1e-3)
+        Fdot = rng.standard_normal(len(fields)) * fp[node]
+        abar, bbar = rng.standard_normal(om.n), rng.standard_normal(om.n)
+        lin, rhs, lin_dot, rhs_dot = tl.jvp(y, fp[node], params, 12.5, ydot, Fdot)
+        ybar, Fbar = tl.vjp(y, fp[node], params, 12.5, abar, bbar)
+        lhs = abar @ lin_dot + bbar @ rhs_dot
+        rhs_ = ybar @ ydot + Fbar @ Fdot
+        scale = np.abs(abar * lin_dot).sum() + np.abs(bbar * rhs_dot).sum()
+        worst = max(worst, abs(lhs - rhs_) / scale)
+    assert worst < 1e-12, worst
