@@ -1,13 +1,14 @@
-"""Gradients of GRL1 traces with respect to per-node field parameters.
+"""Gradients of GRL1 and RK4 traces with respect to per-node field parameters.
 
-``GRL1Trace`` runs the reference's user loop -- ``forward(t0 + j*interval,
-interval)`` for ``j < num_intervals`` with GRL1, sampling one state (``V``
-by default) after every interval -- on the GPU and records a checkpoint of
-the full state every ``checkpoint_every`` internal steps.  Its backward pass
-is a hand-written adjoint kernel (``goss_b200/csrc/goss_adjoint.cuh``) that
-recomputes each checkpoint segment and applies the transposed GRL1 step
-Jacobians in reverse, using the generated reverse-mode sweep of the model's
-linearised right-hand side.
+``GRL1Trace`` / ``RK4Trace`` run the reference's user loop --
+``forward(t0 + j*interval, interval)`` for ``j < num_intervals``, sampling
+one state (``V`` by default) after every interval -- on the GPU and record a
+checkpoint of the full state every ``checkpoint_every`` internal steps.  The
+backward pass is a hand-written adjoint kernel
+(``goss_b200/csrc/goss_adjoint.cuh``) that recomputes each checkpoint
+segment and applies the transposed step Jacobians in reverse, using the
+generated reverse-mode sweeps of the model's linearised right-hand side
+(GRL1) or right-hand side (RK4).
 
 :func:`trace` wraps it in a ``torch.autograd.Function``: any loss built from
 the trace (for example a misfit ``((trace - target)**2).sum()``) can be
@@ -32,23 +33,28 @@ def _ld(n: int) -> int:
     return (max(n, 1) + 31) // 32 * 32
 
 
-class GRL1Trace:
-    """Trace of a GRL1 solve over many nodes, with its adjoint.
+class SolverTrace:
+    """Trace of an explicit solve (GRL1 or RK4) over many nodes, with its adjoint.
 
     Parameters
     ----------
     ode : ParameterizedODE  (its field parameters are the differentiated inputs)
-    num_nodes, interval (ms), steps_per_interval (internal GRL1 steps per
+    num_nodes, interval (ms), steps_per_interval (internal steps per
     interval), num_intervals, checkpoint_every (internal steps; a multiple of
     steps_per_interval), trace_state (state name), precision ("single" or
-    "double"), t0, device.
+    "double"), t0, device, solver ("GRL1" or "RK4").
     """
+
+    SOLVERS = {"GRL1": _capi.GOSS_GRL1, "RK4": _capi.GOSS_RK4}
 
     def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
                  num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
-                 t0: float = 0.0, device: int = 0):
+                 t0: float = 0.0, device: int = 0, solver: str = "GRL1"):
         import torch
 
+        if solver not in self.SOLVERS:
+            raise ValueError(f"no adjoint for solver {solver!r}; choose one of {sorted(self.SOLVERS)}")
+        self.solver = solver
         if checkpoint_every % steps_per_interval:
             raise ValueError("checkpoint_every must be a multiple of steps_per_interval")
         if trace_state not in ode.state_names:
@@ -88,7 +94,7 @@ class GRL1Trace:
 
         L = _capi.AdjointLaunch()
         L.mode = mode
-        L.solver = _capi.GOSS_GRL1
+        L.solver = self.SOLVERS[self.solver]
         L.precision = self.precision
         L.num_nodes = self.N
         L.block = self.block
@@ -147,12 +153,32 @@ class GRL1Trace:
         return fpb[: self.nfp, : self.N].t().clone(), sb[:, : self.N].t().clone()
 
 
+class GRL1Trace(SolverTrace):
+    """:class:`SolverTrace` of the GRL1 solver."""
+
+    def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
+                 num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
+                 t0: float = 0.0, device: int = 0):
+        super().__init__(ode, num_nodes, interval, steps_per_interval, num_intervals, checkpoint_every,
+                         trace_state, precision, t0, device, solver="GRL1")
+
+
+class RK4Trace(SolverTrace):
+    """:class:`SolverTrace` of the RK4 solver."""
+
+    def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
+                 num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
+                 t0: float = 0.0, device: int = 0):
+        super().__init__(ode, num_nodes, interval, steps_per_interval, num_intervals, checkpoint_every,
+                         trace_state, precision, t0, device, solver="RK4")
+
+
 def _function():
     import torch
 
     class _TraceFn(torch.autograd.Function):
         @staticmethod
-        def forward(ctx, field_params, states0, solver: GRL1Trace):
+        def forward(ctx, field_params, states0, solver: SolverTrace):
             ctx.solver = solver
             return solver.run_forward(field_params.detach(), states0.detach())
 
@@ -167,7 +193,7 @@ def _function():
 _TRACE_FN = None
 
 
-def trace(solver: GRL1Trace, field_params, states0=None):
+def trace(solver: SolverTrace, field_params, states0=None):
     """Differentiable trace: ``solver``'s GRL1 loop as a torch function of the
     field parameters [N, nfp] and the initial states [N, n]."""
     import torch

@@ -19,7 +19,7 @@ from __future__ import annotations
 
 import json
 import re
-from typing import Dict, List, Sequence
+from typing import Dict, List, Sequence, Tuple
 
 import sympy as sp
 
@@ -328,6 +328,8 @@ class ModelSource:
                     return f"abar[{int(n[len('__seed_linear_'):])}]"
                 if n.startswith("__seed_rhs_"):
                     return f"bbar[{int(n[len('__seed_rhs_'):])}]"
+                if n.startswith("__seed_values_"):
+                    return f"bbar[{int(n[len('__seed_values_'):])}]"
                 if n.startswith("__adj_"):
                     return f"a_{n[len('__adj_'):]}"
                 if n.startswith("__c"):
@@ -401,9 +403,12 @@ class ModelSource:
                 body.append(Output(b.array, b.index, f(b.expr)))
         return Program(prog.name, body, None)
 
-    def _dev_vjp_lines(self, lin_full: Program) -> List[str]:
-        """Body of linearized_vjp: forward sweep, then the reverse sweep."""
-        folded = self._fold(lin_full)
+    def _dev_vjp_lines(self, prog: Program, arrays: Dict[str, Tuple[str, str]], seed_call: str) -> List[str]:
+        """Body of a VJP: forward sweep, the caller's seed, the reverse sweep.
+
+        arrays maps each output array of ``prog`` to (value array, cotangent
+        array) names; ``seed_call`` hands both to the caller's seed."""
+        folded = self._fold(prog)
         inter = {n: self.model.sym(n) for n in self.model.intermediates}
         rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
                             [self.model.sym(p) for p in self.fparams], inter)
@@ -415,16 +420,15 @@ class ModelSource:
             lines.append(f"const {t} v_{b.name} = {pr(b.expr)};")
         # the values themselves, then the caller's cotangents for them
         n = len(self.states)
-        lines.append(f"T lin_v[{n}], rhs_v[{n}], abar[{n}], bbar[{n}];")
+        decl = ", ".join(f"{v}[{n}], {c}[{n}]" for v, c in arrays.values())
+        lines.append(f"T {decl};")
         for o in rp.outputs:
-            arr = "lin_v" if o.array == "linear" else "rhs_v"
-            lines.append(f"{arr}[{o.index}] = {prT(o.expr)};")
-        for i in range(n):
-            if not any(o.array == "linear" and o.index == i for o in rp.outputs):
-                lines.append(f"lin_v[{i}] = T(0.0);")
-            if not any(o.array == "rhs" and o.index == i for o in rp.outputs):
-                lines.append(f"rhs_v[{i}] = T(0.0);")
-        lines.append("seed(lin_v, rhs_v, abar, bbar);")
+            lines.append(f"{arrays[o.array][0]}[{o.index}] = {prT(o.expr)};")
+        for arr, (val, _) in arrays.items():
+            for i in range(n):
+                if not any(o.array == arr and o.index == i for o in rp.outputs):
+                    lines.append(f"{val}[{i}] = T(0.0);")
+        lines.append(seed_call)
         for adj, e in rp.reverse:
             lines.append(f"const T a_{adj.name[len('__adj_'):]} = {prT(e)};")
         for i, e in enumerate(rp.state_bar):
@@ -518,8 +522,21 @@ class ModelSource:
         L.append(f"  __device__ static __forceinline__ void linearized_vjp({sig}, Seed&& seed,")
         L.append("      T* __restrict__ ybar, T* __restrict__ Fbar)")
         L.append("  {")
-        L += ["    " + x for x in head + self._dev_vjp_lines(lin_full)]
+        L += ["    " + x for x in head + self._dev_vjp_lines(
+            lin_full, {"linear": ("lin_v", "abar"), "rhs": ("rhs_v", "bbar")}, "seed(lin_v, rhs_v, abar, bbar);")]
         L.append("    (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;")
+        L.append("  }")
+        L.append("")
+        L.append("  // vector-Jacobian product of rhs (reverse mode, generated): after the forward sweep")
+        L.append("  // seed(values, bbar) supplies the cotangents of the values, then ybar = bbar^T df/dy")
+        L.append("  // and Fbar = bbar^T df/dF")
+        L.append("  template <typename T, class Seed>")
+        L.append(f"  __device__ static __forceinline__ void rhs_vjp({sig}, Seed&& seed,")
+        L.append("      T* __restrict__ ybar, T* __restrict__ Fbar)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_vjp_lines(self.rhs, {"values": ("f_v", "bbar")},
+                                                             "seed(f_v, bbar);")]
+        L.append("    (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;")
         L.append("  }")
         if self.mon is not None:
             L.append("")

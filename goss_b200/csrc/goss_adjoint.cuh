@@ -1,23 +1,32 @@
-// Adjoint of GRL1 trajectories with checkpointing (one thread per node).
+// Adjoint of GRL1 and RK4 trajectories with checkpointing (one thread per node).
 //
 // Forward (record_kernel): the reference's user loop
-//     for j in 0..J-1:  forward(t0 + j*interval, interval)   (S internal GRL1
-//                       steps, GRL1.cpp:61-82)  and sample the traced state
+//     for j in 0..J-1:  forward(t0 + j*interval, interval)   (S internal
+//                       steps, GRL1.cpp:61-82 / RK4.cpp:68-102)
 // storing the traced state after every interval (the trace) and the full
-// state every K internal steps (checkpoints; K a multiple of S).
+// state every K internal steps (checkpoints; K a multiple of S).  Each step
+// is explicit_step of goss_kernels.cuh, the solver kernels' own arithmetic.
 //
 // Backward (adjoint_kernel): given the cotangent of the trace, walk the
 // checkpoint segments from last to first; recompute each segment's K states
-// into per-node scratch, then apply the transposed Jacobian of every GRL1 step
-// in reverse,
-//     Phi_i(y) = y_i + b_i h phi1(a_i h),   (a, b) = linearized(y, t)
-//     lambda  <- lambda + [abar^T d a/dy + bbar^T d b/dy]
+// into per-node scratch, then apply the transposed Jacobian of every step in
+// reverse, adding the trace cotangent to the traced state's lambda at every
+// sample and accumulating the field-parameter gradient.
+//
+// GRL1:  Phi_i(y) = y_i + b_i h phi1(a_i h),   (a, b) = linearized(y, t)
+//     lambda <- lambda + [abar^T d a/dy + bbar^T d b/dy]
 //     abar_i = lambda_i b_i h^2 phi1'(a_i h),  bbar_i = lambda_i h phi1(a_i h)
-// (the reverse sweep of linearized comes from the generated linearized_vjp),
-// adding the trace cotangent to the traced state's lambda at every sample and
-// accumulating the field-parameter gradient.  phi1(x) = (e^x - 1)/x is the
-// same function as the reference's b/a (e^{a h} - 1); the derivative uses
-// the smooth phi1 form.
+// with the generated linearized_vjp for the bracket.  phi1(x) = (e^x - 1)/x
+// is the same function as the reference's b/a (e^{a h} - 1); the derivative
+// uses the smooth phi1 form.
+//
+// RK4:   y' = y + h/6 (k1 + 2 k2 + 2 k3 + k4),  k_s = f(u_s, t_s),
+//        u_1 = y, u_2 = y + h/2 k1, u_3 = y + h/2 k2, u_4 = y + h k3
+// reversed stage by stage with the generated rhs_vjp:
+//     kbar_4 = h/6 lambda;  ubar_s = (df/du)(u_s)^T kbar_s;
+//     kbar_{s-1} = w_{s-1} lambda + c_s ubar_s  (w = h/6, h/3, h/3; c = h/2, h/2, h)
+//     lambda <- lambda + sum_s ubar_s
+// after recomputing k1..k3 from the step's input state.
 #ifndef GOSS_ADJOINT_CUH
 #define GOSS_ADJOINT_CUH
 
@@ -153,28 +162,16 @@ __device__ __forceinline__ void cp_load(const void* cp, uint64_t idx_hi, uint64_
     a.lo = static_cast<const float*>(cp)[idx_lo];
 }
 
+// GRL1 threshold of the reference (GRL1.h:39) used by the traces
+constexpr double kGrlDelta = 1e-8;
+
 template <typename T>
 __host__ __device__ constexpr int cp_rows(int n)
 {
     return sizeof(T) == 4 ? 2 * n : n;
 }
 
-// one GRL1 step of the adjoint solver's forward (same update as explicit_node)
-template <class M, typename T>
-__device__ __forceinline__ void grl1_step(Acc<T>* y, double lt, T h, const T* P, const double* PD, const T* F)
-{
-    constexpr int n = M::num_states;
-    T yt[n], lin[n], rhs[n];
-#pragma unroll
-    for (int i = 0; i < n; ++i)
-        yt[i] = y[i].value();
-    M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
-#pragma unroll
-    for (int i = 0; i < n; ++i)
-        y[i].add(grl_increment(lin[i], rhs[i], h, T(1e-8)));
-}
-
-template <class M, typename T>
+template <class M, typename T, Explicit S>
 __global__ void __launch_bounds__(128) record_kernel(const __grid_constant__ AdjointArgs<M, T> a)
 {
     constexpr int n = M::num_states;
@@ -186,20 +183,19 @@ __global__ void __launch_bounds__(128) record_kernel(const __grid_constant__ Adj
         y[i].load(a.states[i * a.ld + node]);
     T F[Dims<M>::nfp];
     load_field<M, T>(a.fparams, a.ld, node, F);
-    const uint32_t S = a.steps_per_interval, K = a.checkpoint_every;
-    const double ldt = a.interval / S;
-    const T h = T(ldt);
+    const uint32_t S_ = a.steps_per_interval, K = a.checkpoint_every;
+    const double ldt = a.interval / S_;
     constexpr int rows = cp_rows<T>(n);
     for (uint32_t j = 0; j < a.num_intervals; ++j) {
-        const uint64_t g = (uint64_t)j * S;
+        const uint64_t g = (uint64_t)j * S_;
         if (g % K == 0) {
             const uint64_t c = g / K;
             for (int i = 0; i < n; ++i)
                 cp_store(a.checkpoints, ((c * rows) + i) * a.ld + node, ((c * rows) + n + i) * a.ld + node, y[i]);
         }
         double lt = a.t0 + j * a.interval;
-        for (uint32_t s = 0; s < S; ++s) {
-            grl1_step<M, T>(y, lt, h, a.P, a.PD, F);
+        for (uint32_t s = 0; s < S_; ++s) {
+            explicit_step<M, T, S>(y, lt, ldt, a.P, a.PD, F, T(kGrlDelta));
             lt += ldt;
         }
         a.trace[(uint64_t)j * a.ld + node] = y[a.trace_state].store();
@@ -214,7 +210,91 @@ __global__ void __launch_bounds__(128) record_kernel(const __grid_constant__ Adj
         atomicOr(a.flags, GOSS_FLAG_NONFINITE);
 }
 
+// lambda <- lambda + (dPhi/dy)(y)^T lambda - lambda for one GRL1 step, and the
+// field-parameter part into gF
 template <class M, typename T>
+__device__ __forceinline__ void reverse_step_grl1(const T* yt, double lt, double ldt, const T* P, const double* PD,
+                                                  const T* F, Acc<T>* lam, double* gF)
+{
+    constexpr int n = M::num_states;
+    constexpr int nfp = Dims<M>::nfp;
+    const T h = T(ldt);
+    T lv[n], ybar[n], Fbar[nfp];
+    for (int i = 0; i < n; ++i)
+        lv[i] = lam[i].value();
+    auto seed = [&](const T* lin, const T* rhs, T* abar, T* bbar) {
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            const T x = lin[i] * h;
+            bbar[i] = lv[i] * h * phi1t(x);
+            abar[i] = lv[i] * rhs[i] * h * h * dphi1t(x);
+        }
+    };
+    M::template linearized_vjp<T>(yt, lt, P, PD, F, seed, ybar, Fbar);
+    for (int i = 0; i < n; ++i)
+        lam[i].add(ybar[i]);
+    for (int q = 0; q < M::num_field_params; ++q)
+        gF[q] += double(Fbar[q]);
+}
+
+// the same for one RK4 step; the stage loops are not unrolled, so rhs and
+// rhs_vjp are instantiated once.  The stage inputs are formed from the step's
+// input value (in FP32 its high word; the forward adds the low word as well,
+// a difference of at most half an FP32 ulp of the state).
+template <class M, typename T>
+__device__ __forceinline__ void reverse_step_rk4(const T* yt, double lt, double ldt, const T* P, const double* PD,
+                                                 const T* F, Acc<T>* lam, double* gF)
+{
+    constexpr int n = M::num_states;
+    constexpr int nfp = Dims<M>::nfp;
+    const T h = T(ldt), hh = T(0.5 * ldt);
+    T k1[n], k2[n], k3[n], u[n];
+#pragma unroll 1
+    for (int st = 0; st < 3; ++st) {
+        const double ts = st == 0 ? lt : lt + 0.5 * ldt;
+        for (int i = 0; i < n; ++i)
+            u[i] = st == 0 ? yt[i] : yt[i] + hh * (st == 1 ? k1[i] : k2[i]);
+        T k[n];
+        M::template rhs<T>(u, ts, P, PD, F, k);
+        for (int i = 0; i < n; ++i) {
+            k1[i] = st == 0 ? k[i] : k1[i];
+            k2[i] = st == 1 ? k[i] : k2[i];
+            k3[i] = st == 2 ? k[i] : k3[i];
+        }
+    }
+    T lv[n], kb[n], ysum[n];
+    const T w6 = h / T(6.0), w3 = h / T(3.0);
+    for (int i = 0; i < n; ++i) {
+        lv[i] = lam[i].value();
+        kb[i] = w6 * lv[i];
+        ysum[i] = T(0.0);
+    }
+#pragma unroll 1
+    for (int st = 3; st >= 0; --st) {
+        const T c = st == 3 ? h : hh;
+        const double ts = st == 3 ? lt + ldt : (st == 0 ? lt : lt + 0.5 * ldt);
+        for (int i = 0; i < n; ++i)
+            u[i] = st == 0 ? yt[i] : yt[i] + c * (st == 3 ? k3[i] : st == 2 ? k2[i] : k1[i]);
+        T ub[n], Fb[nfp];
+        auto seed = [&](const T*, T* bbar) {
+#pragma unroll
+            for (int i = 0; i < n; ++i)
+                bbar[i] = kb[i];
+        };
+        M::template rhs_vjp<T>(u, ts, P, PD, F, seed, ub, Fb);
+        const T w = st == 1 ? w6 : w3;
+        for (int i = 0; i < n; ++i) {
+            ysum[i] = ysum[i] + ub[i];
+            kb[i] = w * lv[i] + c * ub[i];
+        }
+        for (int q = 0; q < M::num_field_params; ++q)
+            gF[q] += double(Fb[q]);
+    }
+    for (int i = 0; i < n; ++i)
+        lam[i].add(ysum[i]);
+}
+
+template <class M, typename T, Explicit S>
 __global__ void __launch_bounds__(GOSS_ADJOINT_BLOCK, GOSS_ADJOINT_MIN_BLOCKS)
 adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
 {
@@ -226,9 +306,8 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
     const bool active = node < a.N;
     const uint32_t src = active ? node : a.N - 1;
     extern __shared__ double s_time[];  // time of every step of a segment (same for all nodes)
-    const uint32_t S = a.steps_per_interval, K = a.checkpoint_every;
-    const double ldt = a.interval / S;
-    const T h = T(ldt);
+    const uint32_t S_ = a.steps_per_interval, K = a.checkpoint_every;
+    const double ldt = a.interval / S_;
     T F[nfp];
     load_field<M, T>(a.fparams, a.ld, src, F);
     Acc<T> lam[n];
@@ -237,7 +316,7 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
     double gF[nfp];
     for (int k = 0; k < nfp; ++k)
         gF[k] = 0.0;
-    const uint64_t total = (uint64_t)a.num_intervals * S;
+    const uint64_t total = (uint64_t)a.num_intervals * S_;
     const uint32_t num_cp = (uint32_t)((total + K - 1) / K);
     constexpr int rows = cp_rows<T>(n);
     T* const scratch = a.scratch + node;
@@ -250,14 +329,14 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
             double lt = 0.0;
             for (uint32_t k = 0; k < len; ++k) {
                 const uint64_t g = g0 + k;
-                if (g % S == 0)
-                    lt = a.t0 + (g / S) * a.interval;
+                if (g % S_ == 0)
+                    lt = a.t0 + (g / S_) * a.interval;
                 s_time[k] = lt;
                 lt += ldt;
             }
         }
         __syncthreads();
-        // recompute the segment, keeping the model input of every step
+        // recompute the segment, keeping the input state of every step
         Acc<T> y[n];
         for (int i = 0; i < n; ++i)
             cp_load(a.checkpoints, ((uint64_t)c * rows + i) * a.ld + src, ((uint64_t)c * rows + n + i) * a.ld + src,
@@ -266,7 +345,7 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
             for (int i = 0; i < n; ++i)
                 scratch[((uint64_t)k * n + i) * a.sld] = y[i].value();
             if (k + 1 < len)
-                grl1_step<M, T>(y, s_time[k], h, a.P, a.PD, F);
+                explicit_step<M, T, S>(y, s_time[k], ldt, a.P, a.PD, F, T(kGrlDelta));
 #if GOSS_ADJOINT_LOCKSTEP
             __syncthreads();
 #endif
@@ -274,28 +353,17 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
         // reverse through the segment
         for (int k = (int)len - 1; k >= 0; --k) {
             const uint64_t g = g0 + k;  // step g maps state g to state g+1
-            if ((g + 1) % S == 0) {
-                const uint64_t j = (g + 1) / S - 1;
+            if ((g + 1) % S_ == 0) {
+                const uint64_t j = (g + 1) / S_ - 1;
                 lam[a.trace_state].add(T(a.trace_bar[j * a.ld + src]));
             }
-            T yt[n], lv[n], ybar[n], Fbar[nfp];
-            for (int i = 0; i < n; ++i) {
-                yt[i] = scratch[((uint64_t)k * n + i) * a.sld];
-                lv[i] = lam[i].value();
-            }
-            auto seed = [&](const T* lin, const T* rhs, T* abar, T* bbar) {
-#pragma unroll
-                for (int i = 0; i < n; ++i) {
-                    const T x = lin[i] * h;
-                    bbar[i] = lv[i] * h * phi1t(x);
-                    abar[i] = lv[i] * rhs[i] * h * h * dphi1t(x);
-                }
-            };
-            M::template linearized_vjp<T>(yt, s_time[k], a.P, a.PD, F, seed, ybar, Fbar);
+            T yt[n];
             for (int i = 0; i < n; ++i)
-                lam[i].add(ybar[i]);
-            for (int q = 0; q < M::num_field_params; ++q)
-                gF[q] += double(Fbar[q]);
+                yt[i] = scratch[((uint64_t)k * n + i) * a.sld];
+            if constexpr (S == Explicit::GRL1)
+                reverse_step_grl1<M, T>(yt, s_time[k], ldt, a.P, a.PD, F, lam, gF);
+            else
+                reverse_step_rk4<M, T>(yt, s_time[k], ldt, a.P, a.PD, F, lam, gF);
 #if GOSS_ADJOINT_LOCKSTEP
             __syncthreads();
 #endif
@@ -309,7 +377,7 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
         a.states_bar[(uint64_t)i * a.ld + node] = lam[i].store();
 }
 
-template <class M, typename T>
+template <class M, typename T, Explicit S>
 inline int launch_adjoint_t(const goss_adjoint_launch* L)
 {
     AdjointArgs<M, T> a;
@@ -342,7 +410,7 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
     if (L->mode == 0) {
         const unsigned block = 128;
         const unsigned grid = (L->num_nodes + block - 1) / block;
-        record_kernel<M, T><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+        record_kernel<M, T, S><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
     } else {
         // power-of-two blocks up to the compiled bound keep grid * block <= sld
         unsigned block = L->block ? L->block : GOSS_ADJOINT_BLOCK;
@@ -352,7 +420,7 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
         const size_t shm = sizeof(double) * a.checkpoint_every;
         if (shm > 48 * 1024)
             return GOSS_ERR_ARGUMENT;
-        adjoint_kernel<M, T><<<grid, block, shm, (cudaStream_t)L->stream>>>(a);
+        adjoint_kernel<M, T, S><<<grid, block, shm, (cudaStream_t)L->stream>>>(a);
     }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
 }
@@ -360,9 +428,15 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
 template <class M>
 inline int launch_adjoint(const goss_adjoint_launch* L)
 {
-    if (L->solver != GOSS_GRL1)
+    const bool f32 = L->precision == GOSS_FP32;
+    switch (L->solver) {
+    case GOSS_GRL1:
+        return f32 ? launch_adjoint_t<M, float, Explicit::GRL1>(L) : launch_adjoint_t<M, double, Explicit::GRL1>(L);
+    case GOSS_RK4:
+        return f32 ? launch_adjoint_t<M, float, Explicit::RK4>(L) : launch_adjoint_t<M, double, Explicit::RK4>(L);
+    default:
         return GOSS_ERR_UNSUPPORTED;
-    return L->precision == GOSS_FP32 ? launch_adjoint_t<M, float>(L) : launch_adjoint_t<M, double>(L);
+    }
 }
 
 }  // namespace goss_b200

@@ -191,6 +191,78 @@ struct NodeIO {
     double delta;
 };
 
+// One internal step of an explicit solver at time lt with step ldt, in place
+// on the accumulated states (shared by the solver kernels and the adjoint
+// kernels' record and recompute passes, so all take identical arithmetic).
+template <class M, typename T, Explicit S>
+__device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const double ldt, const T* __restrict__ P,
+                                              const double* __restrict__ PD, const T* __restrict__ F, const T delta)
+{
+    constexpr int n = M::num_states;
+    const T h = T(ldt);
+    const T hh = T(0.5 * ldt);
+    T yt[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+        yt[i] = y[i].value();
+    if constexpr (S == Explicit::Euler) {
+        // ExplicitEuler.cpp:80-81
+        T f[n];
+        M::template rhs<T>(yt, lt, P, PD, F, f);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y[i].add(h * f[i]);
+    } else if constexpr (S == Explicit::RK4) {
+        // RK4.cpp:79-98 with RK4::axpy (RK4.h:70-74); the weighted sum is
+        // accumulated in the order k1 + 2 k2 + 2 k3 + k4 of the reference.
+        T k[n], sum[n], tmp[n];
+        M::template rhs<T>(yt, lt, P, PD, F, k);
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            sum[i] = k[i];
+            tmp[i] = y[i].plus(hh * k[i]);
+        }
+        M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            sum[i] = sum[i] + T(2.0) * k[i];
+            tmp[i] = y[i].plus(hh * k[i]);
+        }
+        M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            sum[i] = sum[i] + T(2.0) * k[i];
+            tmp[i] = y[i].plus(h * k[i]);
+        }
+        M::template rhs<T>(tmp, lt + ldt, P, PD, F, k);
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+            sum[i] = sum[i] + k[i];
+            y[i].add(h * sum[i] / T(6.0));
+        }
+    } else if constexpr (S == Explicit::GRL1) {
+        // GRL1.h:72-84
+        T lin[n], rhs[n];
+        M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y[i].add(grl_increment(lin[i], rhs[i], h, delta));
+    } else {
+        // GRL2: GRL2.cpp:78-82.  The reference's branch threshold is a
+        // self-initialised local (GRL2.cpp:67) whose -O3 build behaves as 0:
+        // the exponential form is used whenever the linear term is non-zero.
+        T lin[n], rhs[n], y2[n];
+        M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y2[i] = y[i].plus(grl_increment(lin[i], rhs[i], hh, T(0)));
+        M::template linearized<T>(y2, lt, P, PD, F, lin, rhs);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y[i].add(grl_increment(lin[i], rhs[i], h, T(0)));
+    }
+}
+
 // Advance one node over nsteps internal steps of one explicit solver.
 template <class M, typename T, Explicit S>
 __device__ __forceinline__ void explicit_node(const NodeIO& a, uint32_t node, const T* __restrict__ P,
@@ -205,71 +277,10 @@ __device__ __forceinline__ void explicit_node(const NodeIO& a, uint32_t node, co
     load_field<M, T>(a.fparams, a.ld, node, F);
 
     const double ldt = a.ldt;
-    const T h = T(ldt);
-    const T hh = T(0.5 * ldt);
     const T delta = T(a.delta);
     double lt = a.t;
     for (uint64_t step = 0; step < a.nsteps; ++step) {
-        T yt[n];
-#pragma unroll
-        for (int i = 0; i < n; ++i)
-            yt[i] = y[i].value();
-        if constexpr (S == Explicit::Euler) {
-            // ExplicitEuler.cpp:80-81
-            T f[n];
-            M::template rhs<T>(yt, lt, P, PD, F, f);
-#pragma unroll
-            for (int i = 0; i < n; ++i)
-                y[i].add(h * f[i]);
-        } else if constexpr (S == Explicit::RK4) {
-            // RK4.cpp:79-98 with RK4::axpy (RK4.h:70-74); the weighted sum is
-            // accumulated in the order k1 + 2 k2 + 2 k3 + k4 of the reference.
-            T k[n], sum[n], tmp[n];
-            M::template rhs<T>(yt, lt, P, PD, F, k);
-#pragma unroll
-            for (int i = 0; i < n; ++i) {
-                sum[i] = k[i];
-                tmp[i] = y[i].plus(hh * k[i]);
-            }
-            M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
-#pragma unroll
-            for (int i = 0; i < n; ++i) {
-                sum[i] = sum[i] + T(2.0) * k[i];
-                tmp[i] = y[i].plus(hh * k[i]);
-            }
-            M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
-#pragma unroll
-            for (int i = 0; i < n; ++i) {
-                sum[i] = sum[i] + T(2.0) * k[i];
-                tmp[i] = y[i].plus(h * k[i]);
-            }
-            M::template rhs<T>(tmp, lt + ldt, P, PD, F, k);
-#pragma unroll
-            for (int i = 0; i < n; ++i) {
-                sum[i] = sum[i] + k[i];
-                y[i].add(h * sum[i] / T(6.0));
-            }
-        } else if constexpr (S == Explicit::GRL1) {
-            // GRL1.h:72-84
-            T lin[n], rhs[n];
-            M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
-#pragma unroll
-            for (int i = 0; i < n; ++i)
-                y[i].add(grl_increment(lin[i], rhs[i], h, delta));
-        } else {
-            // GRL2: GRL2.cpp:78-82.  The reference's branch threshold is a
-            // self-initialised local (GRL2.cpp:67) whose -O3 build behaves as 0:
-            // the exponential form is used whenever the linear term is non-zero.
-            T lin[n], rhs[n], y2[n];
-            M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
-#pragma unroll
-            for (int i = 0; i < n; ++i)
-                y2[i] = y[i].plus(grl_increment(lin[i], rhs[i], hh, T(0)));
-            M::template linearized<T>(y2, lt, P, PD, F, lin, rhs);
-#pragma unroll
-            for (int i = 0; i < n; ++i)
-                y[i].add(grl_increment(lin[i], rhs[i], h, T(0)));
-        }
+        explicit_step<M, T, S>(y, lt, ldt, P, PD, F, delta);
         lt += ldt;
     }
     bool finite = true;

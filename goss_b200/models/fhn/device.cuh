@@ -73,7 +73,7 @@ struct M_fhn {
     const T v_I = ((P[12]*s_s*(P[11] + s_v)) + (P[14]*(P[11] + s_v)*(P[13] + s_v)*(P[9] - ((s_v)))));
     const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     const T v_dI_dv = ((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) + (P[19]*(P[11] + s_v)*(P[13] + s_v)));
-    T lin_v[2], rhs_v[2], abar[2], bbar[2];
+    T lin_v[2], abar[2], rhs_v[2], bbar[2];
     rhs_v[0] = (v_I + T(v_i_Stim));
     rhs_v[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
     lin_v[1] = P[18];
@@ -84,6 +84,27 @@ struct M_fhn {
     ybar[0] = ((a_I*((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) - ((P[14]*(P[11] + s_v)*(P[13] + s_v))))) + (a_dI_dv*((P[19]*(P[11] + s_v)) + (P[19]*(P[13] + s_v)) - ((P[14]*(P[11] + s_v))) - ((P[14]*(P[13] + s_v))) + (T(2.0)*P[14]*(P[9] - ((s_v)))))) + (bbar[1]*P[1]));
     ybar[1] = ((a_dI_dv*P[12]) + (a_I*P[12]*(P[11] + s_v)) + (P[17]*bbar[1]*P[1]));
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
+  }
+
+  // vector-Jacobian product of rhs (reverse mode, generated): after the forward sweep
+  // seed(values, bbar) supplies the cotangents of the values, then ybar = bbar^T df/dy
+  // and Fbar = bbar^T df/dF
+  template <typename T, class Seed>
+  __device__ static __forceinline__ void rhs_vjp(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, Seed&& seed,
+      T* __restrict__ ybar, T* __restrict__ Fbar)
+  {
+    const T s_v = y[0];
+    const T s_s = y[1];
+    const T v_I = ((P[12]*s_s*(P[11] + s_v)) + (P[14]*(P[11] + s_v)*(P[13] + s_v)*(P[9] - ((s_v)))));
+    const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+    T f_v[2], bbar[2];
+    f_v[0] = (v_I + T(v_i_Stim));
+    f_v[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
+    seed(f_v, bbar);
+    const T a_I = bbar[0];
+    ybar[0] = ((a_I*((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) - ((P[14]*(P[11] + s_v)*(P[13] + s_v))))) + (bbar[1]*P[1]));
+    ybar[1] = ((a_I*P[12]*(P[11] + s_v)) + (P[17]*bbar[1]*P[1]));
+    (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;
   }
 };
 

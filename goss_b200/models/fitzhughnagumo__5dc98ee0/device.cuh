@@ -74,7 +74,7 @@ struct M_fitzhughnagumo__5dc98ee0 {
     const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     const T v_dI_dV = ((P[13]*s_s) + (P[14]*(s_V + P[12])*(P[0] - ((s_V)))) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))) + (P[18]*(s_V + P[12])*(s_V - ((v_V_th)))));
-    T lin_v[2], rhs_v[2], abar[2], bbar[2];
+    T lin_v[2], abar[2], rhs_v[2], bbar[2];
     rhs_v[0] = (v_I + T(v_i_Stim));
     rhs_v[1] = (F[1]*(s_V + P[12] + (P[17]*s_s)));
     lin_v[1] = (P[17]*F[1]);
@@ -88,6 +88,31 @@ struct M_fitzhughnagumo__5dc98ee0 {
     Fbar[0] = (a_V_th*P[11]);
     Fbar[1] = ((P[17]*abar[1]) + (bbar[1]*(s_V + P[12] + (P[17]*s_s))));
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
+  }
+
+  // vector-Jacobian product of rhs (reverse mode, generated): after the forward sweep
+  // seed(values, bbar) supplies the cotangents of the values, then ybar = bbar^T df/dy
+  // and Fbar = bbar^T df/dF
+  template <typename T, class Seed>
+  __device__ static __forceinline__ void rhs_vjp(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, Seed&& seed,
+      T* __restrict__ ybar, T* __restrict__ Fbar)
+  {
+    const T s_V = y[0];
+    const T s_s = y[1];
+    const T v_V_th = (P[1] + (P[11]*F[0]));
+    const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+    T f_v[2], bbar[2];
+    f_v[0] = (v_I + T(v_i_Stim));
+    f_v[1] = (F[1]*(s_V + P[12] + (P[17]*s_s)));
+    seed(f_v, bbar);
+    const T a_I = bbar[0];
+    const T a_V_th = (-(a_I*P[14]*(s_V + P[12])*(P[0] - ((s_V)))));
+    ybar[0] = ((a_I*((P[13]*s_s) + (P[14]*(s_V + P[12])*(P[0] - ((s_V)))) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))) - ((P[14]*(s_V + P[12])*(s_V - ((v_V_th))))))) + (bbar[1]*F[1]));
+    ybar[1] = ((a_I*P[13]*(s_V + P[12])) + (P[17]*bbar[1]*F[1]));
+    Fbar[0] = (a_V_th*P[11]);
+    Fbar[1] = (bbar[1]*(s_V + P[12] + (P[17]*s_s)));
+    (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;
   }
 };
 

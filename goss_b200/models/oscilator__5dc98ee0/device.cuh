@@ -54,7 +54,7 @@ struct M_oscilator__5dc98ee0 {
   {
     const T s_x = y[0];
     const T s_y = y[1];
-    T lin_v[2], rhs_v[2], abar[2], bbar[2];
+    T lin_v[2], abar[2], rhs_v[2], bbar[2];
     rhs_v[0] = (-(F[0]*s_y));
     rhs_v[1] = (F[1]*s_x);
     lin_v[0] = T(0.0);
@@ -65,6 +65,26 @@ struct M_oscilator__5dc98ee0 {
     Fbar[0] = (-(bbar[0]*s_y));
     Fbar[1] = (bbar[1]*s_x);
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
+  }
+
+  // vector-Jacobian product of rhs (reverse mode, generated): after the forward sweep
+  // seed(values, bbar) supplies the cotangents of the values, then ybar = bbar^T df/dy
+  // and Fbar = bbar^T df/dF
+  template <typename T, class Seed>
+  __device__ static __forceinline__ void rhs_vjp(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, Seed&& seed,
+      T* __restrict__ ybar, T* __restrict__ Fbar)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    T f_v[2], bbar[2];
+    f_v[0] = (-(F[0]*s_y));
+    f_v[1] = (F[1]*s_x);
+    seed(f_v, bbar);
+    ybar[0] = (bbar[1]*F[1]);
+    ybar[1] = (-(bbar[0]*F[0]));
+    Fbar[0] = (-(bbar[0]*s_y));
+    Fbar[1] = (bbar[1]*s_x);
+    (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;
   }
 };
 

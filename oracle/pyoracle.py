@@ -184,38 +184,39 @@ TANGENT = HERE / "tangent"
 
 
 def build_tangent(variant_dir: Path, force: bool = False) -> Path:
-    """Compile tangent/tangent_grl1.cpp over a variant's generated device.cuh."""
+    """Compile tangent/tangent_trace.cpp over a variant's generated device.cuh."""
     import json
 
     variant_dir = Path(variant_dir).resolve()
     struct = "M_" + json.loads((variant_dir / "model.json").read_text())["variant"]
     out = BUILD / "tangent" / variant_dir.name / "libtangent.so"
-    deps = [variant_dir / "device.cuh", TANGENT / "tangent_grl1.cpp", TANGENT / "goss_device_math.cuh"]
+    deps = [variant_dir / "device.cuh", TANGENT / "tangent_trace.cpp", TANGENT / "goss_device_math.cuh"]
     if not force and out.exists() and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return out
     out.parent.mkdir(parents=True, exist_ok=True)
     tmp = out.with_suffix(f".so.{os.getpid()}.tmp")
     subprocess.run([_cc("g++"), "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", f"-I{TANGENT}",
-                    f"-I{variant_dir}", f"-DGOSS_TANGENT_MODEL={struct}", str(TANGENT / "tangent_grl1.cpp"),
+                    f"-I{variant_dir}", f"-DGOSS_TANGENT_MODEL={struct}", str(TANGENT / "tangent_trace.cpp"),
                     "-o", str(tmp)], check=True)
     os.replace(tmp, out)
     return out
 
 
-class TangentGRL1:
-    """FP64 forward-mode tangent-linear GRL1 traces of one model variant.
+class TangentTrace:
+    """FP64 forward-mode tangent-linear GRL1 / RK4 traces of one model variant.
 
     ``trace(states0 [N, n], field_params [N, nfp], params, t0, interval,
-    steps_per_interval, num_intervals, trace_state, dirs)`` returns the trace
-    [J, N] and its Jacobian [J, N, len(dirs)] with respect to the inputs
-    ``dirs`` (index < n: an initial state; else field parameter index - n).
+    steps_per_interval, num_intervals, trace_state, dirs, solver="GRL1")``
+    returns the trace [J, N] and its Jacobian [J, N, len(dirs)] with respect
+    to the inputs ``dirs`` (index < n: an initial state; else field parameter
+    index - n).
     """
 
     def __init__(self, variant_dir: Path):
         self.lib = C.CDLL(str(build_tangent(variant_dir)))
-        self.lib.tangent_grl1_trace.restype = C.c_int
-        self.lib.tangent_grl1_trace.argtypes = [
-            C.c_uint32, _dp, _dp, _dp, C.c_double, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+        self.lib.tangent_trace.restype = C.c_int
+        self.lib.tangent_trace.argtypes = [
+            C.c_int, C.c_uint32, _dp, _dp, _dp, C.c_double, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
             C.POINTER(C.c_uint32), C.c_double, _dp, _dp]
         self.n = self.lib.tangent_num_states()
         self.nfp = self.lib.tangent_num_field_params()
@@ -248,7 +249,7 @@ class TangentGRL1:
         return ybar, Fbar[: self.nfp]
 
     def trace(self, states0, field_params, params, t0, interval, steps_per_interval, num_intervals, trace_state,
-              dirs, delta=1e-8):
+              dirs, solver="GRL1", delta=1e-8):
         y0 = np.ascontiguousarray(states0, dtype=np.float64).reshape(-1, self.n)
         N = y0.shape[0]
         fp = np.ascontiguousarray(field_params if self.nfp else np.zeros((N, 1)), dtype=np.float64)
@@ -256,11 +257,11 @@ class TangentGRL1:
         d = np.ascontiguousarray(dirs, dtype=np.uint32)
         tr = np.zeros((num_intervals, N))
         jac = np.zeros((num_intervals, N, len(d)))
-        rc = self.lib.tangent_grl1_trace(N, _ptr(y0), _ptr(fp), _ptr(P), t0, interval, steps_per_interval,
+        rc = self.lib.tangent_trace({"GRL1": 0, "RK4": 1}[solver], N, _ptr(y0), _ptr(fp), _ptr(P), t0, interval, steps_per_interval,
                                          num_intervals, trace_state, len(d),
                                          d.ctypes.data_as(C.POINTER(C.c_uint32)), delta, _ptr(tr), _ptr(jac))
         if rc != 0:
-            raise ValueError("tangent_grl1_trace: bad arguments")
+            raise ValueError("tangent_trace: bad arguments")
         return tr, jac
 
 

@@ -1,10 +1,11 @@
 // Test infrastructure -- NOT part of the product path.
 //
-// FP64 forward-mode tangent-linear reference for GRL1 traces: the reference
-// user loop forward(t0 + j*interval, interval), j < J, with S internal GRL1
-// steps per interval (GRL1::forward, GRL1.cpp:61-82; the step
-// GRL1::_one_step, GRL1.h:72-84, with the threshold delta = 1e-8 of
-// GRL1.h:39), sampling one state after every interval, run in dual numbers.
+// FP64 forward-mode tangent-linear reference for GRL1 and RK4 traces: the
+// reference user loop forward(t0 + j*interval, interval), j < J, with S
+// internal steps per interval -- GRL1::forward (GRL1.cpp:61-82; the step
+// GRL1::_one_step, GRL1.h:72-84, threshold delta = 1e-8 of GRL1.h:39) or
+// RK4::forward (RK4.cpp:68-102 with RK4::axpy, RK4.h:70-74) -- sampling one
+// state after every interval, run in dual numbers.
 // Each node carries up to D tangent directions, each the unit perturbation
 // of one initial state or one field parameter, so the result is the exact
 // Jacobian d trace[j] / d input (up to FP64 rounding) along the same branch
@@ -15,7 +16,7 @@
 //
 // Compiled per model variant by oracle/pyoracle.py:
 //   g++ -O2 -fopenmp -I oracle/tangent -I <variant dir>
-//       -DGOSS_TANGENT_MODEL=M_<ident> -shared tangent_grl1.cpp
+//       -DGOSS_TANGENT_MODEL=M_<variant> -shared tangent_trace.cpp
 // (oracle/tangent/goss_device_math.cuh stands in for the CUDA header, so the
 // generated device.cuh compiles as host C++).
 #include <cstdint>
@@ -46,6 +47,7 @@ struct TraceArgs {
     uint32_t steps_per_interval, num_intervals, trace_state;
     uint32_t num_dirs;
     const uint32_t* dirs;        // direction k perturbs input dirs[k]: < n a state, else field dirs[k]-n
+    int solver;                  // 0 GRL1, 1 RK4
     double delta;
     double* trace;               // [J][N]
     double* jacobian;            // [J][N][num_dirs]
@@ -75,12 +77,28 @@ void node_trace(const TraceArgs& a, uint32_t node)
     for (uint32_t j = 0; j < a.num_intervals; ++j) {
         double lt = a.t0 + j * a.interval;
         for (uint32_t s = 0; s < S; ++s) {
-            for (int i = 0; i < kStates; ++i)
-                lin[i] = T(0.0);
-            Model::template linearized<T>(y, lt, P.data(), a.params, F, lin, rhs);
-            for (int i = 0; i < kStates; ++i)
-                y[i] = (gfabs(lin[i]) > a.delta) ? y[i] + rhs[i] / lin[i] * (gexp(lin[i] * ldt) - 1.0)
-                                                 : y[i] + rhs[i] * ldt;
+            if (a.solver == 0) {
+                for (int i = 0; i < kStates; ++i)
+                    lin[i] = T(0.0);
+                Model::template linearized<T>(y, lt, P.data(), a.params, F, lin, rhs);
+                for (int i = 0; i < kStates; ++i)
+                    y[i] = (gfabs(lin[i]) > a.delta) ? y[i] + rhs[i] / lin[i] * (gexp(lin[i] * ldt) - 1.0)
+                                                     : y[i] + rhs[i] * ldt;
+            } else {
+                T k1[kStates], k2[kStates], k3[kStates], k4[kStates], tmp[kStates];
+                Model::template rhs<T>(y, lt, P.data(), a.params, F, k1);
+                for (int i = 0; i < kStates; ++i)
+                    tmp[i] = y[i] + 0.5 * ldt * k1[i];
+                Model::template rhs<T>(tmp, lt + 0.5 * ldt, P.data(), a.params, F, k2);
+                for (int i = 0; i < kStates; ++i)
+                    tmp[i] = y[i] + 0.5 * ldt * k2[i];
+                Model::template rhs<T>(tmp, lt + 0.5 * ldt, P.data(), a.params, F, k3);
+                for (int i = 0; i < kStates; ++i)
+                    tmp[i] = y[i] + ldt * k3[i];
+                Model::template rhs<T>(tmp, lt + ldt, P.data(), a.params, F, k4);
+                for (int i = 0; i < kStates; ++i)
+                    y[i] = y[i] + ldt * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]) / 6.0;
+            }
             lt += ldt;
         }
         const T& v = y[a.trace_state];
@@ -108,22 +126,23 @@ __attribute__((visibility("default"))) int tangent_num_field_params() { return M
 __attribute__((visibility("default"))) int tangent_num_params() { return Model::num_params; }
 __attribute__((visibility("default"))) int tangent_num_derived() { return Model::num_derived; }
 
-// params: the model's num_params parameters followed by room for num_derived
-// derived constants, which this call fills in.  Returns 0, or -1 for bad
-// arguments (more than 32 directions, a direction out of range).
-__attribute__((visibility("default"))) int tangent_grl1_trace(
-    uint32_t num_nodes, const double* states0, const double* field_params, double* params, double t0,
+// solver: 0 GRL1, 1 RK4.  params: the model's num_params parameters followed
+// by room for num_derived derived constants, which this call fills in.
+// Returns 0, or -1 for bad arguments (more than 32 directions, a direction
+// out of range, an unknown solver).
+__attribute__((visibility("default"))) int tangent_trace(
+    int solver, uint32_t num_nodes, const double* states0, const double* field_params, double* params, double t0,
     double interval, uint32_t steps_per_interval, uint32_t num_intervals, uint32_t trace_state,
     uint32_t num_dirs, const uint32_t* dirs, double delta, double* trace, double* jacobian)
 {
-    if (num_dirs > 32 || steps_per_interval == 0 || trace_state >= (uint32_t)kStates)
+    if (num_dirs > 32 || steps_per_interval == 0 || trace_state >= (uint32_t)kStates || solver < 0 || solver > 1)
         return -1;
     for (uint32_t k = 0; k < num_dirs; ++k)
         if (dirs[k] >= (uint32_t)(kStates + Model::num_field_params))
             return -1;
     Model::derived(params, params + Model::num_params);
     const TraceArgs a{num_nodes, states0, field_params, params, t0, interval, steps_per_interval,
-                      num_intervals, trace_state, num_dirs, dirs, delta, trace, jacobian};
+                      num_intervals, trace_state, num_dirs, dirs, solver, delta, trace, jacobian};
     if (num_dirs <= 1) run<1>(a);
     else if (num_dirs <= 4) run<4>(a);
     else if (num_dirs <= 8) run<8>(a);
@@ -141,7 +160,7 @@ __attribute__((visibility("default"))) int tangent_grl1_trace(
 //                the generated reverse sweep `linearized_vjp` in FP64.
 // A dot-product test <abar, lin_dot> + <bbar, rhs_dot> = <ybar, ydot> +
 // <Fbar, Fdot> then checks the reverse sweep against forward mode.
-// params as for tangent_grl1_trace (derived constants filled in here).
+// params as for tangent_trace (derived constants filled in here).
 extern "C" {
 
 __attribute__((visibility("default"))) int tangent_jvp(const double* y, const double* F, double* params,

@@ -72,13 +72,14 @@ def parity(a, b, rtol=1e-10, atol=1e-12):
     return float(np.max(np.abs(a[m] - b[m]) / (atol + rtol * np.abs(b[m])))) if m.any() else 0.0
 
 
-def oracle_grl1_traces(name, field_parameters, fp, y0, interval, steps_per_interval, num_intervals, state_index,
-                       t0=0.0):
-    """Oracle (reference semantics) GRL1 traces [J, nodes] of one state: the
-    loop forward(t0 + j*interval, interval), sampled after every interval."""
+def oracle_state_traces(name, field_parameters, fp, y0, interval, steps_per_interval, num_intervals, state_index,
+                        t0=0.0, solver="GRL1"):
+    """Oracle (reference semantics) traces [J, nodes] of one state: the loop
+    forward(t0 + j*interval, interval) of an explicit solver, sampled after
+    every interval."""
     om = oracle_model(name, tuple(field_parameters))
     y0 = np.atleast_2d(np.asarray(y0, dtype=np.float64))
-    o = pyoracle.OracleSystem(om, "GRL1", y0.shape[0], ldt=interval / steps_per_interval)
+    o = pyoracle.OracleSystem(om, solver, y0.shape[0], ldt=interval / steps_per_interval)
     o.states[:] = y0
     if om.nfp:
         o.field_params[:] = fp

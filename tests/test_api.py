@@ -164,3 +164,11 @@ def test_c_params_layout():
     s.internal_time_step = 0.05
     p = s.c_params()
     assert p.theta == 0.75 and p.ldt == 0.05 and p.max_iterations == 30
+
+
+def test_solver_trace_rejects_solvers_without_adjoint():
+    from goss_b200.adjoint import SolverTrace
+
+    ode = goss.ParameterizedODE("fitzhughnagumo", field_parameters=["a", "b"])
+    with pytest.raises(ValueError):
+        SolverTrace(ode, 4, 1.0, 10, 2, 10, solver="ThetaSolver")

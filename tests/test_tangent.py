@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from helpers import column_rel_err, meta, oracle_grl1_traces, oracle_model, parity, variant_dir
+from helpers import column_rel_err, meta, oracle_model, oracle_state_traces, parity, variant_dir
 
 
 def _setup(name, fields, nodes, seed=3, spread=0.1):
@@ -27,7 +27,7 @@ def _setup(name, fields, nodes, seed=3, spread=0.1):
     idx = [md["parameter_names"].index(f) for f in fields]
     fp = params[idx][None, :] * np.exp(spread * rng.standard_normal((nodes, len(fields))))
     y0 = om.ic[None, :] * (1 + rng.uniform(-0.02, 0.02, (nodes, om.n)))
-    return pyoracle.TangentGRL1(vdir), om, md, params, fp, y0
+    return pyoracle.TangentTrace(vdir), om, md, params, fp, y0
 
 
 def _fd(name, fields, fp, y0, interval, S, J, iv, dirs, n, h=1e-6):
@@ -43,8 +43,8 @@ def _fd(name, fields, fp, y0, interval, S, J, iv, dirs, n, h=1e-6):
             step = h * np.abs(fp[:, d - n])
             fpp[:, d - n] += step
             fpm[:, d - n] -= step
-        tp = oracle_grl1_traces(name, fields, fpp, yp, interval, S, J, iv)
-        tm = oracle_grl1_traces(name, fields, fpm, ym, interval, S, J, iv)
+        tp = oracle_state_traces(name, fields, fpp, yp, interval, S, J, iv)
+        tm = oracle_state_traces(name, fields, fpm, ym, interval, S, J, iv)
         out[:, :, k] = (tp - tm) / (2 * step[None, :])
     return out
 
@@ -54,7 +54,7 @@ def test_primal_trace_matches_oracle():
     tl, om, md, params, fp, y0 = _setup(name, fields, 6)
     iv = md["state_names"].index("V")
     tr, jac = tl.trace(y0, fp, params, 0.0, 1.0, 100, 16, iv, [om.n + k for k in range(4)])
-    ref = oracle_grl1_traces(name, fields, fp, y0, 1.0, 100, 16, iv)
+    ref = oracle_state_traces(name, fields, fp, y0, 1.0, 100, 16, iv)
     assert jac.shape == (16, 6, 4)
     assert parity(tr, ref, rtol=1e-10, atol=1e-12) <= 1.0
 
@@ -122,3 +122,29 @@ def test_generated_vjp_dot_product(name, fields):
         scale = np.abs(abar * lin_dot).sum() + np.abs(bbar * rhs_dot).sum()
         worst = max(worst, abs(lhs - rhs_) / scale)
     assert worst < 1e-12, worst
+
+
+def test_rk4_primal_and_jacobian_smooth_model():
+    name, fields = "fitzhughnagumo", ["a", "b"]
+    tl, om, md, params, fp, y0 = _setup(name, fields, 5)
+    dirs = list(range(om.n + 2))
+    S, J = 20, 30
+    tr, jac = tl.trace(y0, fp, params, 0.0, 1.0, S, J, 0, dirs, solver="RK4")
+    ref = oracle_state_traces(name, fields, fp, y0, 1.0, S, J, 0, solver="RK4")
+    assert parity(tr, ref, rtol=1e-10, atol=1e-12) <= 1.0
+    out = np.zeros_like(jac)
+    h = 1e-4
+    for k, d in enumerate(dirs):
+        yp, ym, fpp, fpm = y0.copy(), y0.copy(), fp.copy(), fp.copy()
+        if d < om.n:
+            step = h * np.maximum(np.abs(y0[:, d]), 1.0)
+            yp[:, d] += step
+            ym[:, d] -= step
+        else:
+            step = h * np.abs(fp[:, d - om.n])
+            fpp[:, d - om.n] += step
+            fpm[:, d - om.n] -= step
+        tp = oracle_state_traces(name, fields, fpp, yp, 1.0, S, J, 0, solver="RK4")
+        tm = oracle_state_traces(name, fields, fpm, ym, 1.0, S, J, 0, solver="RK4")
+        out[:, :, k] = (tp - tm) / (2 * step[None, :])
+    assert column_rel_err(jac.reshape(-1, len(dirs)), out.reshape(-1, len(dirs))) < 1e-6
