@@ -145,6 +145,17 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings over all ranks (the slowest
+    rank sets the job's time); identity without a process group."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def run_gpu(args, rank, world, dist):
     import torch
 
@@ -259,11 +270,9 @@ def run_gpu(args, rank, world, dist):
 
     out["batched"] = run_batched(args, dev) if not args.skip_fp64 else None
     out["adjoint"] = run_adjoint(dev) if not args.skip_fp64 else None
+    out["implicit"] = run_implicit(dev) if not args.skip_fp64 else None
 
-    times = torch.tensor([ms32, fp64_ms or 0.0, e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms32, fp64_ms_max, e2e_s = [float(x) for x in times.tolist()]
+    ms32, fp64_ms_max, e2e_s = max_over_ranks([ms32, fp64_ms or 0.0, e2e_s], dist, "cuda")
     cell_steps = float(N) * steps_per_call * args.steps * world
     value = cell_steps / (ms32 / 1e3)
     out.update(dict(
@@ -411,14 +420,124 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
     }
 
 
+IMPLICIT_MODEL, IMPLICIT_FIELDS, IMPLICIT_NODES, IMPLICIT_DT = "tentusscher_2004_mcell", ["g_Kr", "g_CaL"], 262_144, 0.1
+IMPLICIT_SOLVERS = [("ThetaSolver", 0.1, 10), ("ESDIRK23a", -1.0, 2)]  # solver, internal step, timed intervals
+
+
+def implicit_inputs(nodes):
+    """TT04 M-cell states IC*(1+u), field parameters default*(1+u), u ~ U(+-5%) (seed 1234)."""
+    from goss_b200 import models
+
+    md = json.loads((models.find_variant(IMPLICIT_MODEL, IMPLICIT_FIELDS) / "model.json").read_text())
+    rng = np.random.default_rng(SEED)
+    ic = np.array(md["initial_conditions"])
+    y0 = ic[None, :] * (1.0 + rng.uniform(-0.05, 0.05, (nodes, ic.size)))
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * (1.0 + rng.uniform(-0.05, 0.05, (nodes, len(IMPLICIT_FIELDS))))
+    return md, y0, fp
+
+
+def run_implicit(dev):
+    """ThetaSolver (theta 0.5, one 0.1 ms step per interval) and ESDIRK23a
+    (adaptive) on TT04 M-cell, 262,144 nodes, FP64 Newton and LU, forward
+    (t, 0.1 ms) per step; one untimed interval first.  Unit: node-intervals/s.
+    With the reference's default tolerances ESDIRK23a rejects every TT04 step
+    down to min_dt (0.001 ms) and the states do not advance -- the reference's
+    own behaviour, reproduced -- so its cost is 100 rejected attempts per
+    interval."""
+    import torch
+
+    import goss_b200 as goss
+
+    md, y0, fp = implicit_inputs(IMPLICIT_NODES)
+    ode = goss.ParameterizedODE(IMPLICIT_MODEL, field_parameters=IMPLICIT_FIELDS)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for name, ldt, intervals in IMPLICIT_SOLVERS:
+        solver = goss.solvers.solver_mapper[name](ode)
+        solver.internal_time_step = ldt
+        system = goss.ODESystemSolver(IMPLICIT_NODES, solver, ode, device=dev)
+        system.set_stream(stream.cuda_stream)
+        system.set_states(y0)
+        system.field_parameters = fp
+        system.forward(0.0, IMPLICIT_DT)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t = IMPLICIT_DT
+        e0.record(stream)
+        for _ in range(intervals):
+            system.forward_async(t, IMPLICIT_DT)
+            t += IMPLICIT_DT
+        e1.record(stream)
+        system.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        jac, rej, acc = system.counters()
+        out[name] = {"value": IMPLICIT_NODES * intervals / (ms / 1e3), "unit": "node-intervals/s",
+                     "ms_per_interval": ms / intervals, "intervals": intervals, "internal_time_step": ldt,
+                     "jacobians_per_node_interval": float(np.mean(jac)) / (intervals + 1),
+                     "rejected_per_node_interval": float(np.mean(rej)) / (intervals + 1),
+                     "accepted_per_node_interval": float(np.mean(acc)) / (intervals + 1)}
+        del system
+    return {"workload": f"{IMPLICIT_MODEL} [g_Kr, g_CaL] U(+-5%), {IMPLICIT_NODES} nodes, forward(t, 0.1 ms), FP64",
+            **out}
+
+
+def implicit_reference_sample(target_s=6.0):
+    """The reference's ThetaSolver / ESDIRK23a (one solver per node, OpenMP)
+    on a node subset of the implicit workload: node-intervals/s."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from goss_b200 import models
+
+    vdir = models.find_variant(IMPLICIT_MODEL, IMPLICIT_FIELDS)
+    md = json.loads((vdir / "model.json").read_text())
+    threads = cpu_threads()
+    om = pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
+    plugin = pyoracle.REFDIR / vdir.name / "libplugin.so"
+    kind = "reference" if pyoracle.ref_available() and plugin.exists() else "port"
+    out = {}
+    for name, ldt, _ in IMPLICIT_SOLVERS:
+        nodes = threads * 4
+        for attempt in range(2):
+            _, y0, fp = implicit_inputs(nodes)
+            if kind == "reference":
+                r = pyoracle.RefSystem(plugin, md["class_name"], name, nodes, om.solver_params(name, ldt=ldt))
+                r.set_states(y0)
+                r.set_field_parameters(fp)
+                r.set_num_threads(threads)
+                fwd = lambda t: r.forward(t, IMPLICIT_DT)
+            else:
+                o = pyoracle.OracleSystem(om, name, nodes, ldt=ldt)
+                o.states[:] = y0
+                o.field_params[:] = fp
+                fwd = lambda t: o.forward(t, IMPLICIT_DT, threads=threads)
+            fwd(0.0)
+            t0 = time.perf_counter()
+            fwd(IMPLICIT_DT)
+            dt = time.perf_counter() - t0
+            if attempt == 0:
+                nodes = int(min(max(nodes * target_s / max(dt, 1e-6), nodes), IMPLICIT_NODES))
+                nodes = max(threads, nodes // threads * threads)
+        out[name] = {"value": nodes / dt, "unit": "node-intervals/s", "kind": kind, "cores": threads,
+                     "sample": f"{nodes} nodes x one 0.1 ms interval after one untimed interval, {dt:.1f} s"}
+    return out
+
+
 def roofline(md, value_fp32, ms_per_step, n_nodes):
-    """Operation census of one GRL1 step (generator) against the CUDA-core peaks."""
-    lin = md["op_census"]["linearized"]
+    """Operation census of one GRL1 step (generator) against the CUDA-core peaks.
+
+    The census is the generator's count of the linearised evaluation as the
+    kernel runs it (``op_census.linearized_split``: parameter-only terms folded,
+    every distinct exp/log/sqrt/reciprocal once).  MUFU (SFU) ops: exp, log,
+    sqrt, pow (2) and one reciprocal per division; the GRL update's phi1 is a
+    polynomial for |a h| < 1/4 (most states) and is not counted.  FP32-pipe
+    ops: adds, muls, the multiply of every division and exponential, and ~10
+    ops of the phi1 update per state."""
+    census = md["op_census"]
+    lin = census.get("linearized_split", census["linearized"])
     n = len(md["state_names"])
-    # MUFU (SFU) ops: exp, log, sqrt and the reciprocal of every division, plus the
-    # exponential of the GRL update; FP32 pipe ops: adds, muls, the multiply of
-    # every division/exp, and ~10 ops of the phi1 update per state
-    sfu = lin["exp"] + lin["log"] + lin["sqrt"] + lin["div"] + n
+    sfu = lin["exp"] + lin["log"] + lin["sqrt"] + 2 * lin["pow"] + lin["div"]
     fp = lin["add"] + lin["mul"] + lin["div"] + lin["exp"] + 10 * n
     sm_clock = 1.965e9
     sfu_peak = 148 * 16 * sm_clock          # 16 MUFU results / clk / SM
@@ -543,6 +662,11 @@ def main():
         except Exception as exc:  # the baseline is reported, never the target
             cpu = {"value": None, "unit": "cell-steps/s", "cores": cpu_threads(), "kind": "reference",
                    "sample": f"failed: {exc}"}
+        if not args.skip_fp64:
+            try:
+                cpu["implicit"] = implicit_reference_sample()
+            except Exception as exc:
+                cpu["implicit"] = {"failed": str(exc)}
     if rank == 0:
         rl = roofline(md, res["value"] / world, res["ms_per_step"], args.nodes)
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
@@ -556,7 +680,8 @@ def main():
                          if res["fp64_plain_value"] else None,
                          "v_max_rel_err_fp32_vs_fp64": res["v_max_rel_err_fp32_vs_fp64"]},
                 "state_max_rel_err_fp32_vs_fp64": res.get("state_max_rel_err_fp32_vs_fp64"),
-                "batched_heterogeneous": res.get("batched"), "adjoint": res.get("adjoint")}
+                "batched_heterogeneous": res.get("batched"), "adjoint": res.get("adjoint"),
+                "implicit": res.get("implicit")}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -112,8 +112,21 @@ class ModelSource:
             monitored_names=list(self.ir.monitored),
             linear_terms=self.linear_terms,
             intermediate_names=list(self.model.intermediates),
-            op_census=dict(rhs=count_ops(self.rhs), linearized=count_ops(self.ir.linearized_program(split=False))),
+            op_census=dict(rhs=count_ops(self.rhs), linearized=count_ops(self.ir.linearized_program(split=False)),
+                           linearized_split=self._split_census()),
         )
+
+    def _split_census(self) -> Dict[str, int]:
+        """Per-evaluation census of the linearised program as the kernels run
+        it: parameter-only sub-expressions folded into derived constants and
+        every distinct exp/log/sqrt/reciprocal counted once (the elementary
+        split of codegen/ad.py), time-only statements excluded."""
+        folded = self._fold(self.ir.linearized_program(split=False))
+        inter = {n: self.model.sym(n) for n in self.model.intermediates}
+        rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
+                            [self.model.sym(p) for p in self.fparams], inter)
+        body = [b for b in rp.forward if b.cls != TIME_CLS] + list(rp.outputs)
+        return count_ops(Program("linearized_split", body, None))
 
     # =======================================================================
     # C restatement (oracle)
