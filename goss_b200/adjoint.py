@@ -78,7 +78,7 @@ class SolverTrace:
         rows = 2 * self.n if self.precision == _capi.GOSS_FP32 else self.n
         dev = self.device
         self._checkpoints = torch.zeros((self.num_checkpoints, rows, self.ld), dtype=cp_dtype, device=dev)
-        self._scratch = torch.zeros((self.K, self.n, (self.N + 255) // 256 * 256), dtype=cp_dtype, device=dev)
+        self._scratch = torch.zeros((self.K, self.n, (self.N + 255) // 256 * 256 + 256), dtype=cp_dtype, device=dev)
         self._states = torch.zeros((self.n, self.ld), dtype=torch.float64, device=dev)
         self._fp = torch.zeros((max(self.nfp, 1), self.ld), dtype=torch.float64, device=dev)
         self._trace = torch.zeros((self.J, self.ld), dtype=torch.float64, device=dev)
@@ -86,7 +86,7 @@ class SolverTrace:
         self._fn = _AdjointFn(ode.module.desc.contents.adjoint)
         if not ode.module.desc.contents.adjoint:
             raise _capi.ExtensionMissingError("the model module has no adjoint kernels")
-        self.block = 0  # backward threads per block (0: the module's compiled default)
+        self.block = 0  # backward threads per block (0: chosen from the node count)
         self.final_states: Optional[object] = None
 
     def _launch(self, mode: int, trace_bar=None, fp_bar=None, states_bar=None) -> None:

@@ -123,7 +123,7 @@ struct AdjointArgs {
     void* checkpoints;         // [C][2n][ld] float (FP32: hi, lo) or [C][n][ld] double
     double* trace;             // [J][ld]
     const double* trace_bar;   // [J][ld]
-    T* scratch;                // [K][n][sld], sld = num_nodes rounded up to 256
+    T* scratch;                // [K][n][sld], sld = num_nodes rounded up to 256, plus 256
     double* fparams_bar;       // [nfp][ld]
     double* states_bar;        // [n][ld]
     uint32_t* flags;
@@ -377,6 +377,38 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
         a.states_bar[(uint64_t)i * a.ld + node] = lam[i].store();
 }
 
+// Threads per block for the backward kernel: every thread carries one node
+// through the whole trajectory, so the job runs in waves of (resident blocks
+// x SMs) blocks and its time is about waves x resident warps per SM.  Choose
+// the multiple of 32 (<= GOSS_ADJOINT_BLOCK) minimising that product (ties:
+// the larger block) -- e.g. 224 for 65,536 nodes on 148 SMs (two full waves
+// of 7 warps) instead of 256 (a second wave on 108 of 148 SMs).
+template <class M, typename T, Explicit S>
+inline unsigned adjoint_block(uint32_t num_nodes, size_t shm)
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        return GOSS_ADJOINT_BLOCK;
+    unsigned best = GOSS_ADJOINT_BLOCK;
+    uint64_t best_cost = ~0ull;
+    for (unsigned b = GOSS_ADJOINT_BLOCK; b >= 32; b -= 32) {
+        int active = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&active, adjoint_kernel<M, T, S>, (int)b, shm) !=
+                cudaSuccess || active <= 0)
+            continue;
+        const uint64_t grid = (num_nodes + b - 1) / b;
+        const uint64_t slots = (uint64_t)active * sms;
+        const uint64_t waves = (grid + slots - 1) / slots;
+        const uint64_t cost = waves * (uint64_t)active * b;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = b;
+        }
+    }
+    return best;
+}
+
 template <class M, typename T, Explicit S>
 inline int launch_adjoint_t(const goss_adjoint_launch* L)
 {
@@ -404,7 +436,8 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
     if (a.steps_per_interval == 0 || a.checkpoint_every == 0 || a.checkpoint_every % a.steps_per_interval ||
         a.trace_state >= (uint32_t)M::num_states)
         return GOSS_ERR_ARGUMENT;
-    a.sld = ((uint64_t)L->num_nodes + 255) / 256 * 256;
+    // room for grid * block <= round_up(num_nodes, block) for any block <= 256
+    a.sld = ((uint64_t)L->num_nodes + 255) / 256 * 256 + 256;
     if (L->num_nodes == 0)
         return 0;
     if (L->mode == 0) {
@@ -412,14 +445,13 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
         const unsigned grid = (L->num_nodes + block - 1) / block;
         record_kernel<M, T, S><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
     } else {
-        // power-of-two blocks up to the compiled bound keep grid * block <= sld
-        unsigned block = L->block ? L->block : GOSS_ADJOINT_BLOCK;
-        if (block > GOSS_ADJOINT_BLOCK || block < 32 || (block & (block - 1)))
-            return GOSS_ERR_ARGUMENT;
-        const unsigned grid = (L->num_nodes + block - 1) / block;
         const size_t shm = sizeof(double) * a.checkpoint_every;
         if (shm > 48 * 1024)
             return GOSS_ERR_ARGUMENT;
+        const unsigned block = L->block ? L->block : adjoint_block<M, T, S>(L->num_nodes, shm);
+        if (block == 0 || block > GOSS_ADJOINT_BLOCK || block % 32)
+            return GOSS_ERR_ARGUMENT;
+        const unsigned grid = (L->num_nodes + block - 1) / block;
         adjoint_kernel<M, T, S><<<grid, block, shm, (cudaStream_t)L->stream>>>(a);
     }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;

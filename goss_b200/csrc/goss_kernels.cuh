@@ -381,22 +381,33 @@ __device__ __forceinline__ void rhs64(const double* y, double t, const double* P
     M::template rhs<double>(y, t, P, P, F, out);
 }
 
-// ODE::compute_jacobian (ODE.cpp:47-67) into any matrix accessor
+// ODE::compute_jacobian (ODE.cpp:47-67) into any matrix accessor: column i is
+// (f(y + delta_i e_i) - f(y)) / delta_i with delta_i = sqrt(1e-15 max(1e-5, |y_i|)),
+// f1 = f(y, t) supplied by the caller (the reference evaluates it first with
+// the same arguments).  The perturbed state is built by selects over
+// compile-time indices, so y stays in registers (the reference perturbs y[i]
+// in place and restores it: the same values).
 template <class M, class Mat>
-__device__ void compute_jacobian(double* y, double t, const double* P, const double* F, const Mat& J, double* f1,
-                                 double* f2)
+__device__ void compute_jacobian(const double* y, double t, const double* P, const double* F, const Mat& J,
+                                 const double* f1)
 {
     constexpr int n = M::num_states;
-    rhs64<M>(y, t, P, F, f1);
+#pragma unroll 1
     for (int i = 0; i < n; ++i) {
-        const double ysafe = y[i];
+        double ysafe = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k)
+            ysafe = (k == i) ? y[k] : ysafe;
         const double max = 1e-5 > fabs(ysafe) ? 1e-5 : fabs(ysafe);
         const double delta = sqrt(1e-15 * max);
-        y[i] += delta;
-        rhs64<M>(y, t, P, F, f2);
+        double yp[n], f2[n];
+#pragma unroll
+        for (int k = 0; k < n; ++k)
+            yp[k] = (k == i) ? ysafe + delta : y[k];
+        rhs64<M>(yp, t, P, F, f2);
+#pragma unroll
         for (int j = 0; j < n; ++j)
             J(j, i) = (f2[j] - f1[j]) / delta;
-        y[i] = ysafe;
     }
 }
 
@@ -414,7 +425,7 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
     if (node >= a.N)
         return;
     const goss_solver_params& sp = a.sp;
-    double y[n], z1[n], prev[n], ft1[n], yz[n], f1[n], b[n], dz[n], g1[n], g2[n];
+    double y[n], z1[n], prev[n], ft1[n], yz[n], f1[n], b[n], dz[n];
     double Jm[n * n];
     const LocalMat<n> J{Jm};
 #pragma unroll
@@ -473,7 +484,7 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
                 break;
             if (recompute || always) {
                 // compute_factorized_jacobian (ImplicitODESolver.cpp:92-105)
-                compute_jacobian<M>(yz, tn, a.P, F, J, g1, g2);
+                compute_jacobian<M>(yz, tn, a.P, F, J, f1);  // f1 = f(yz, tn) from the residual
                 const double scale = -ldt * alpha;
                 for (int i = 0; i < n; ++i)
                     for (int j = 0; j < n; ++j)
@@ -622,12 +633,13 @@ struct EsdirkNode {
     int newton_iterations, first_step, new_jacobian;
     double jac_comp, rejects, accepted;
     double z1[n], z2[n], z3[n], z4[n], prev[n], yh[n];
-    double y_int[n], z_int[n], b[n], dz[n], prev_dz[n], g1[n], g2[n];
+    double y_int[n], z_int[n], b[n], dz[n], prev_dz[n], g1[n];
 
     // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
     __device__ void ode_jacobian(double* y, double t)
     {
-        compute_jacobian<M>(y, t, P, F, jac, g1, g2);
+        rhs64<M>(y, t, P, F, g1);
+        compute_jacobian<M>(y, t, P, F, jac, g1);
         jac_comp += 1;
         new_jacobian = 1;
     }

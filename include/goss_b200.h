@@ -132,15 +132,15 @@ typedef struct goss_eval_launch {
  *     FP64 [C][n][ld] doubles, C = ceil(J*S/K).
  *   mode 1 (backward): trace_bar [J][ld] = dLoss/dtrace -> field_params_bar
  *     [nfp][ld] = dLoss/dfield_params and states_bar [n][ld] = dLoss/dstates
- *     (initial); scratch holds [K][n][round_up(num_nodes, 256)] values of the
- *     arithmetic type (K = checkpoint_every). */
+ *     (initial); scratch holds [K][n][round_up(num_nodes, 256) + 256] values
+ *     of the arithmetic type (K = checkpoint_every). */
 typedef struct goss_adjoint_launch {
     int32_t mode;
     int32_t solver;           /* GOSS_GRL1 */
     int32_t precision;
     uint32_t num_nodes;
-    uint32_t block;           /* backward threads per block: 0 = compiled default,
-                                 else a power of two >= 32 not above it */
+    uint32_t block;           /* backward threads per block: 0 = chosen from the
+                                 node count, else a multiple of 32 <= 256 */
     uint64_t ld;
     double* states;
     const double* field_params;
