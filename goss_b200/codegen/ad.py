@@ -16,10 +16,11 @@ forward sweep that recomputes the program's values:
 With ``elementary=True`` (the default) the active statements are first split
 so that every transcendental operation is a statement of its own: each
 ``exp(u)``, ``log(u)``, ``sqrt(u)``, ``u**p`` (p not an integer) and each
-denominator of a product (one reciprocal ``1/(d_1 d_2 ...)`` per product)
-becomes a value ``__t<k>`` computed once in the forward sweep, shared by all
-statements with the same operand.  Their partial derivatives are written in
-terms of those values -- d exp(u) = exp(u) du, d(1/D) = -(1/D)^2 dD,
+distinct factor of a denominator becomes a value ``__t<k>`` computed once in
+the forward sweep, shared by all statements with the same operand (a
+denominator ``d_1^2 d_2`` costs the reciprocals of ``d_1`` and ``d_2``, reused
+by every other denominator containing them).  Their partial derivatives are
+written in terms of those values -- d exp(u) = exp(u) du, d(1/d) = -(1/d)^2 dd,
 d log(u) = (1/u) du, d sqrt(u) = du / (2 sqrt(u)) -- so the reverse sweep is
 multiplications and additions only; the transcendental work of a VJP is that
 of one forward evaluation.  Conditionals (``Piecewise``) are kept whole.
@@ -46,6 +47,8 @@ class _Splitter:
         self.active = active
         self.memo: Dict[sp.Expr, sp.Symbol] = {}
         self.nodes: List[Tuple[sp.Symbol, sp.Expr, Dict[sp.Symbol, sp.Expr]]] = []
+        self.inverse_of: Dict[sp.Symbol, sp.Expr] = {}  # reciprocal value -> its base
+        self.defs: Dict[sp.Symbol, sp.Expr] = {}        # split statement -> its expression
         self._count = 0
 
     def _is_active(self, e: sp.Expr) -> bool:
@@ -73,8 +76,47 @@ class _Splitter:
                 out[x] = outer * d
         return out
 
-    def recip(self, d: sp.Expr) -> sp.Symbol:
-        return self._node(sp.Pow(d, -1, evaluate=False), lambda r: self._chain(-r * r, d))
+    def _free_inverse(self, e: sp.Expr, depth: int = 0):
+        """1/e without a new reciprocal when e is a product of numbers,
+        reciprocal values and statements defined that way (a gate's
+        tau = alpha * beta with alpha = c/(1 + exp(u)) ...); else None."""
+        if e.is_Number and e != 0:
+            return 1 / e
+        if e in self.inverse_of:
+            return self.inverse_of[e]
+        if isinstance(e, sp.Mul):
+            parts = [self._free_inverse(f, depth) for f in e.args]
+            return None if any(p is None for p in parts) else sp.Mul(*parts)
+        if e.is_Pow and e.exp.is_Integer:
+            inv = self._free_inverse(e.base, depth)
+            return None if inv is None else inv ** e.exp
+        if e.is_Symbol and e in self.defs and depth < 8:
+            return self._free_inverse(self.defs[e], depth + 1)
+        return None
+
+    def recip_base(self, b: sp.Expr) -> sp.Expr:
+        """1/b for one factor b: a value of its own, shared by every product
+        and power of b (and 1/(1/x) = x)."""
+        free = self._free_inverse(b)
+        if free is not None:
+            return free
+        r = self._node(sp.Pow(b, -1, evaluate=False), lambda r: self._chain(-r * r, b))
+        self.inverse_of.setdefault(r, b)
+        return r
+
+    def recip(self, d: sp.Expr) -> sp.Expr:
+        """1/d for a product d of powers: the product of the reciprocals of its
+        distinct bases, so each base costs one reciprocal however many
+        denominators it appears in."""
+        out = []
+        for f in (d.args if isinstance(d, sp.Mul) else (d,)):
+            if not self._is_active(f):
+                out.append(sp.Pow(f, -1))
+            elif f.is_Pow and f.exp.is_Integer and f.exp > 0:
+                out.append(self.recip_base(f.base) ** f.exp)
+            else:
+                out.append(self.recip_base(f))
+        return sp.Mul(*out)
 
     def exp(self, u: sp.Expr) -> sp.Symbol:
         return self._node(sp.exp(u), lambda e: self._chain(e, u))
@@ -136,11 +178,12 @@ class ReverseProgram:
     values when ``elementary``); ``outputs``: the program's outputs in terms
     of them; ``seeds``: (symbol, array, index) of the output cotangents;
     ``reverse``: (adjoint symbol, value) in evaluation order; ``state_bar`` and
-    ``field_bar``: the VJP's results.
+    ``field_bar``: the VJP's results.  ``reverse=False`` builds the split
+    forward program only.
     """
 
     def __init__(self, prog: Program, state_syms: Sequence[sp.Symbol], field_syms: Sequence[sp.Symbol],
-                 inter_syms: Dict[str, sp.Symbol], elementary: bool = True):
+                 inter_syms: Dict[str, sp.Symbol], elementary: bool = True, reverse: bool = True):
         self.state_syms = list(state_syms)
         self.field_syms = list(field_syms)
         sym_of = dict(inter_syms)
@@ -170,6 +213,8 @@ class ReverseProgram:
                 self.forward.append(b)
                 continue
             nb = Assign(b.name, split(b.expr, b.cls), b.cls)
+            if splitter is not None:
+                splitter.defs[s] = nb.expr
             active.add(s)
             self.forward.append(nb)
             self.active_assigns.append((s, nb))
@@ -179,9 +224,13 @@ class ReverseProgram:
                 expr = split(o.expr, STATE) if (o.expr.free_symbols & active) else o.expr
                 self.outputs.append(Output(o.array, o.index, expr))
         self.active = active
+        self.seeds = []
+        self.reverse: List[Tuple[sp.Symbol, sp.Expr]] = []
+        if not reverse:  # the split forward program alone
+            self.state_bar, self.field_bar = [], []
+            return
         # contributions[u] = adjoint-weighted partials of the statements reading u
         contrib: Dict[sp.Symbol, List[sp.Expr]] = defaultdict(list)
-        self.seeds = []
         for o in self.outputs:
             seed = sp.Symbol(f"__seed_{o.array}_{o.index}", real=True)
             self.seeds.append((seed, o.array, o.index))
@@ -189,7 +238,6 @@ class ReverseProgram:
                 d = clean(sp.diff(o.expr, u))
                 if d != 0:
                     contrib[u].append(seed * d)
-        self.reverse: List[Tuple[sp.Symbol, sp.Expr]] = []
         for s, b in reversed(self.active_assigns):
             terms = contrib.pop(s, [])
             if not terms:

@@ -124,7 +124,7 @@ class ModelSource:
         folded = self._fold(self.ir.linearized_program(split=False))
         inter = {n: self.model.sym(n) for n in self.model.intermediates}
         rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
-                            [self.model.sym(p) for p in self.fparams], inter)
+                            [self.model.sym(p) for p in self.fparams], inter, reverse=False)
         body = [b for b in rp.forward if b.cls != TIME_CLS] + list(rp.outputs)
         return count_ops(Program("linearized_split", body, None))
 
@@ -450,6 +450,30 @@ class ModelSource:
             lines.append(f"Fbar[{k}] = {prT(e) if e != 0 else 'T(0.0)'};")
         return lines
 
+    def _dev_split_lines(self, prog: Program, arrays: Dict[str, str]) -> List[str]:
+        """Body of ``prog`` with every distinct exp/log/sqrt/pow/reciprocal of
+        state-dependent operands computed once (the elementary split of
+        codegen/ad.py); ``arrays`` names the output array of each of its
+        output arrays."""
+        folded = self._fold(prog)
+        inter = {n: self.model.sym(n) for n in self.model.intermediates}
+        rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
+                            [self.model.sym(p) for p in self.fparams], inter, reverse=False)
+        prT, prD = self._dev_printers()
+        lines = []
+        for b in rp.forward:
+            t = "double" if b.cls == TIME_CLS else "T"
+            pr = prD if b.cls == TIME_CLS else prT
+            lines.append(f"const {t} v_{b.name} = {pr(b.expr)};")
+        n = len(self.states)
+        for o in rp.outputs:
+            lines.append(f"{arrays[o.array]}[{o.index}] = {prT(o.expr)};")
+        for arr, name in arrays.items():
+            for i in range(n):
+                if not any(o.array == arr and o.index == i for o in rp.outputs):
+                    lines.append(f"{name}[{i}] = T(0.0);")
+        return lines
+
     def _derived_host_lines(self) -> List[str]:
         """Host code filling C[k] with the derived constants from P."""
         def sym(s):
@@ -525,6 +549,23 @@ class ModelSource:
         L.append(f"  __device__ static __forceinline__ void linearized({sig}, T* __restrict__ linear, T* __restrict__ rhs)")
         L.append("  {")
         L += ["    " + x for x in head + self._dev_body(lin_full)]
+        L.append("    (void)time; (void)P; (void)PD; (void)F;")
+        L.append("  }")
+        L.append("")
+        L.append("  // linearized with every distinct transcendental and reciprocal of a state-dependent")
+        L.append("  // operand evaluated once (the FP32 kernels' form; FP64 keeps the reference's operations)")
+        L.append("  template <typename T>")
+        L.append(f"  __device__ static __forceinline__ void linearized_split({sig}, T* __restrict__ linear, T* __restrict__ rhs)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_split_lines(lin_full, {"linear": "linear", "rhs": "rhs"})]
+        L.append("    (void)time; (void)P; (void)PD; (void)F;")
+        L.append("  }")
+        L.append("")
+        L.append("  // rhs in the same split form")
+        L.append("  template <typename T>")
+        L.append(f"  __device__ static __forceinline__ void rhs_split({sig}, T* __restrict__ values)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_split_lines(self.rhs, {"values": "values"})]
         L.append("    (void)time; (void)P; (void)PD; (void)F;")
         L.append("  }")
         L.append("")

@@ -255,7 +255,7 @@ __device__ __forceinline__ void reverse_step_rk4(const T* yt, double lt, double 
         for (int i = 0; i < n; ++i)
             u[i] = st == 0 ? yt[i] : yt[i] + hh * (st == 1 ? k1[i] : k2[i]);
         T k[n];
-        M::template rhs<T>(u, ts, P, PD, F, k);
+        model_rhs<M, T>(u, ts, P, PD, F, k);
         for (int i = 0; i < n; ++i) {
             k1[i] = st == 0 ? k[i] : k1[i];
             k2[i] = st == 1 ? k[i] : k2[i];

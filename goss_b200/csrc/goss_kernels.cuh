@@ -191,6 +191,31 @@ struct NodeIO {
     double delta;
 };
 
+// The model evaluations the explicit steps use.  FP32 kernels take the split
+// forms (every distinct transcendental and reciprocal evaluated once; they
+// are XU-pipe bound); FP64 kernels take the programs with the reference's
+// operation order (FP64 parity with the reference at 1e-10).
+#ifndef GOSS_FP32_SPLIT
+#define GOSS_FP32_SPLIT 1
+#endif
+template <class M, typename T>
+__device__ __forceinline__ void model_linearized(const T* y, double t, const T* P, const double* PD, const T* F,
+                                                 T* lin, T* rhs)
+{
+    if constexpr (GOSS_FP32_SPLIT && sizeof(T) == 4)
+        M::template linearized_split<T>(y, t, P, PD, F, lin, rhs);
+    else
+        M::template linearized<T>(y, t, P, PD, F, lin, rhs);
+}
+template <class M, typename T>
+__device__ __forceinline__ void model_rhs(const T* y, double t, const T* P, const double* PD, const T* F, T* f)
+{
+    if constexpr (GOSS_FP32_SPLIT && sizeof(T) == 4)
+        M::template rhs_split<T>(y, t, P, PD, F, f);
+    else
+        M::template rhs<T>(y, t, P, PD, F, f);
+}
+
 // One internal step of an explicit solver at time lt with step ldt, in place
 // on the accumulated states (shared by the solver kernels and the adjoint
 // kernels' record and recompute passes, so all take identical arithmetic).
@@ -208,7 +233,7 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
     if constexpr (S == Explicit::Euler) {
         // ExplicitEuler.cpp:80-81
         T f[n];
-        M::template rhs<T>(yt, lt, P, PD, F, f);
+        model_rhs<M, T>(yt, lt, P, PD, F, f);
 #pragma unroll
         for (int i = 0; i < n; ++i)
             y[i].add(h * f[i]);
@@ -216,25 +241,25 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
         // RK4.cpp:79-98 with RK4::axpy (RK4.h:70-74); the weighted sum is
         // accumulated in the order k1 + 2 k2 + 2 k3 + k4 of the reference.
         T k[n], sum[n], tmp[n];
-        M::template rhs<T>(yt, lt, P, PD, F, k);
+        model_rhs<M, T>(yt, lt, P, PD, F, k);
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             sum[i] = k[i];
             tmp[i] = y[i].plus(hh * k[i]);
         }
-        M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
+        model_rhs<M, T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             sum[i] = sum[i] + T(2.0) * k[i];
             tmp[i] = y[i].plus(hh * k[i]);
         }
-        M::template rhs<T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
+        model_rhs<M, T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             sum[i] = sum[i] + T(2.0) * k[i];
             tmp[i] = y[i].plus(h * k[i]);
         }
-        M::template rhs<T>(tmp, lt + ldt, P, PD, F, k);
+        model_rhs<M, T>(tmp, lt + ldt, P, PD, F, k);
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             sum[i] = sum[i] + k[i];
@@ -243,7 +268,7 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
     } else if constexpr (S == Explicit::GRL1) {
         // GRL1.h:72-84
         T lin[n], rhs[n];
-        M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
+        model_linearized<M, T>(yt, lt, P, PD, F, lin, rhs);
 #pragma unroll
         for (int i = 0; i < n; ++i)
             y[i].add(grl_increment(lin[i], rhs[i], h, delta));
@@ -252,11 +277,11 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
         // self-initialised local (GRL2.cpp:67) whose -O3 build behaves as 0:
         // the exponential form is used whenever the linear term is non-zero.
         T lin[n], rhs[n], y2[n];
-        M::template linearized<T>(yt, lt, P, PD, F, lin, rhs);
+        model_linearized<M, T>(yt, lt, P, PD, F, lin, rhs);
 #pragma unroll
         for (int i = 0; i < n; ++i)
             y2[i] = y[i].plus(grl_increment(lin[i], rhs[i], hh, T(0)));
-        M::template linearized<T>(y2, lt, P, PD, F, lin, rhs);
+        model_linearized<M, T>(y2, lt, P, PD, F, lin, rhs);
 #pragma unroll
         for (int i = 0; i < n; ++i)
             y[i].add(grl_increment(lin[i], rhs[i], h, T(0)));

@@ -63,6 +63,36 @@ struct M_fitzhughnagumo__8321f5ac {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
+  // linearized with every distinct transcendental and reciprocal of a state-dependent
+  // operand evaluated once (the FP32 kernels' form; FP64 keeps the reference's operations)
+  template <typename T>
+  __device__ static __forceinline__ void linearized_split(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ linear, T* __restrict__ rhs)
+  {
+    const T s_V = y[0];
+    const T s_s = y[1];
+    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+    const T v_dI_dV = ((P[12]*s_s) + (P[14]*(s_V + P[11])*(P[0] - ((s_V)))) + (P[14]*(s_V + P[13])*(P[0] - ((s_V)))) + (P[19]*(s_V + P[11])*(s_V + P[13])));
+    rhs[0] = (v_I + T(v_i_Stim));
+    rhs[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
+    linear[1] = P[18];
+    linear[0] = v_dI_dV;
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // rhs in the same split form
+  template <typename T>
+  __device__ static __forceinline__ void rhs_split(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  {
+    const T s_V = y[0];
+    const T s_s = y[1];
+    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+    values[0] = (v_I + T(v_i_Stim));
+    values[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+
   // vector-Jacobian product of linearized (reverse mode, generated): after the forward
   // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
   // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters

@@ -45,6 +45,31 @@ struct M_oscilator__5dc98ee0 {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
+  // linearized with every distinct transcendental and reciprocal of a state-dependent
+  // operand evaluated once (the FP32 kernels' form; FP64 keeps the reference's operations)
+  template <typename T>
+  __device__ static __forceinline__ void linearized_split(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ linear, T* __restrict__ rhs)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    rhs[0] = (-(F[0]*s_y));
+    rhs[1] = (F[1]*s_x);
+    linear[0] = T(0.0);
+    linear[1] = T(0.0);
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+
+  // rhs in the same split form
+  template <typename T>
+  __device__ static __forceinline__ void rhs_split(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    values[0] = (-(F[0]*s_y));
+    values[1] = (F[1]*s_x);
+    (void)time; (void)P; (void)PD; (void)F;
+  }
+
   // vector-Jacobian product of linearized (reverse mode, generated): after the forward
   // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
   // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters
