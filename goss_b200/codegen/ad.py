@@ -32,19 +32,65 @@ floor derivatives 0 and |x|' = sign(x) as a Piecewise.
 from __future__ import annotations
 
 from collections import defaultdict
-from typing import Dict, List, Sequence, Set, Tuple
+from typing import Dict, List, Optional, Sequence, Set, Tuple
 
 import sympy as sp
 
 from .ir import CONST, STATE, TIME_CLS, Assign, Output, Program, clean
 
 
+def _exp_shape(u: sp.Expr, active: Set[sp.Symbol]):
+    """u = c0 + slope * mono with c0 a number and mono normalised so that the
+    coefficient of its first term (in printed order) is 1: (shape key, slope,
+    c0, mono), or None for an argument without state-dependent terms."""
+    if not (u.free_symbols & active):
+        return None
+    c0, rest = u.as_coeff_Add()
+    terms = []
+    for t in sp.Add.make_args(rest):
+        c, m = t.as_coeff_Mul()
+        terms.append((str(m), float(c), m))
+    terms.sort(key=lambda x: x[0])
+    slope = terms[0][1]
+    if slope == 0:
+        return None
+    key = tuple((name, round(c / slope, 12)) for name, c, _ in terms)
+    mono = sp.Add(*[sp.Float(c / slope) * m if c != slope else m for _, c, m in terms])
+    return key, slope, c0, mono
+
+
+def _plan_exps(shapes: List[Tuple[tuple, float, sp.Expr]]) -> Dict:
+    """Exponentials that share their argument's shape share one value:
+    exp(c0 + s m) = e^c0 exp(s m), and exp(c0 + 2 s m) = e^c0 exp(s m)^2.
+    Only shapes met with more than one distinct argument are planned."""
+    args = defaultdict(set)
+    for key, slope, c0 in shapes:
+        args[key].add((slope, c0))
+    plan = {}
+    for key, members in args.items():
+        if len(members) < 2:
+            continue
+        bases: List[float] = []
+        for slope in sorted({sl for sl, _ in members}, key=abs):
+            for b in bases:
+                k = slope / b
+                if abs(k - 2.0) < 1e-12:
+                    plan[(key, slope)] = (b, 2)
+                    break
+            else:
+                bases.append(slope)
+                plan[(key, slope)] = (slope, 1)
+    return plan
+
+
 class _Splitter:
     """Rewrites active expressions so that transcendental operations are
     separate values (see the module docstring), recording their partials."""
 
-    def __init__(self, active: Set[sp.Symbol]):
+    def __init__(self, active: Set[sp.Symbol], exp_plan: Optional[Dict] = None):
         self.active = active
+        self.exp_plan = exp_plan                         # (argument shape, slope) -> (base slope, power)
+        self.exp_args: List[Tuple[tuple, float, sp.Expr]] = []  # every exp argument's shape, slope, constant
         self.memo: Dict[sp.Expr, sp.Symbol] = {}
         self.nodes: List[Tuple[sp.Symbol, sp.Expr, Dict[sp.Symbol, sp.Expr]]] = []
         self.inverse_of: Dict[sp.Symbol, sp.Expr] = {}  # reciprocal value -> its base
@@ -118,7 +164,17 @@ class _Splitter:
                 out.append(self.recip_base(f))
         return sp.Mul(*out)
 
-    def exp(self, u: sp.Expr) -> sp.Symbol:
+    def exp(self, u: sp.Expr) -> sp.Expr:
+        g = _exp_shape(u, self.active)
+        if g is not None:
+            key, slope, c0, mono = g
+            self.exp_args.append((key, slope, c0))
+            plan = (self.exp_plan or {}).get((key, slope))
+            if plan is not None:
+                base, power = plan
+                arg = sp.Float(base) * mono
+                e = self._node(sp.exp(arg), lambda e: self._chain(e, arg))
+                return sp.Float(sp.N(sp.exp(c0), 20)) * e ** power
         return self._node(sp.exp(u), lambda e: self._chain(e, u))
 
     def log(self, u: sp.Expr) -> sp.Symbol:
@@ -179,16 +235,33 @@ class ReverseProgram:
     of them; ``seeds``: (symbol, array, index) of the output cotangents;
     ``reverse``: (adjoint symbol, value) in evaluation order; ``state_bar`` and
     ``field_bar``: the VJP's results.  ``reverse=False`` builds the split
-    forward program only.
+    forward program only.  With ``elementary`` a first pass over the program
+    collects the exponentials' arguments, so that exponentials of the same
+    shape share one value (``_plan_exps``).
     """
 
     def __init__(self, prog: Program, state_syms: Sequence[sp.Symbol], field_syms: Sequence[sp.Symbol],
                  inter_syms: Dict[str, sp.Symbol], elementary: bool = True, reverse: bool = True):
         self.state_syms = list(state_syms)
         self.field_syms = list(field_syms)
+        plan = None
+        if elementary:
+            shapes = self._split_forward(prog, inter_syms, True, None)
+            plan = _plan_exps(shapes)
+        self._split_forward(prog, inter_syms, elementary, plan)
+        self.seeds = []
+        self.reverse: List[Tuple[sp.Symbol, sp.Expr]] = []
+        if not reverse:  # the split forward program alone
+            self.state_bar, self.field_bar = [], []
+            return
+        self._reverse_sweep()
+
+    def _split_forward(self, prog: Program, inter_syms: Dict[str, sp.Symbol], elementary: bool,
+                       plan: Optional[Dict]) -> List[Tuple[tuple, float, sp.Expr]]:
+        """Fill forward / active_assigns / outputs; return the exp shapes met."""
         sym_of = dict(inter_syms)
         active: Set[sp.Symbol] = set(self.state_syms) | set(self.field_syms)
-        splitter = _Splitter(active) if elementary else None
+        splitter = _Splitter(active, plan) if elementary else None
         node_partials: Dict[sp.Symbol, Dict[sp.Symbol, sp.Expr]] = {}
         self.forward: List[Assign] = []
         self.active_assigns: List[Tuple[sp.Symbol, Assign]] = []
@@ -224,11 +297,11 @@ class ReverseProgram:
                 expr = split(o.expr, STATE) if (o.expr.free_symbols & active) else o.expr
                 self.outputs.append(Output(o.array, o.index, expr))
         self.active = active
-        self.seeds = []
-        self.reverse: List[Tuple[sp.Symbol, sp.Expr]] = []
-        if not reverse:  # the split forward program alone
-            self.state_bar, self.field_bar = [], []
-            return
+        self._node_partials = node_partials
+        return splitter.exp_args if splitter is not None else []
+
+    def _reverse_sweep(self) -> None:
+        active, node_partials = self.active, self._node_partials
         # contributions[u] = adjoint-weighted partials of the statements reading u
         contrib: Dict[sp.Symbol, List[sp.Expr]] = defaultdict(list)
         for o in self.outputs:

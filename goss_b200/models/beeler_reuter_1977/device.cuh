@@ -154,57 +154,52 @@ struct M_beeler_reuter_1977 {
     const T v___t4 = gexp((-(T(0.082)*s_V)));
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.2)*s_V)));
-    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*v___t6)));
+    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
-    const T v___t8 = gexp((-(T(0.1)*s_V)));
-    const T v___t9 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t8)));
-    const T v_beta_j = (T(0.3)*v___t9);
-    const T v___t10 = glog((T(0.001)*s_Cai));
-    const T v___t11 = (T(1.0)/s_Cai);
-    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t10)));
+    const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
+    const T v_beta_j = (T(0.3)*v___t8);
+    const T v___t9 = glog((T(0.001)*s_Cai));
+    const T v___t10 = (T(1.0)/s_Cai);
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t12 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t13 = gexp((T(0.05) - ((T(0.01)*s_V))));
-    const T v___t14 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t12)));
-    const T v_alpha_d = (T(0.095)*v___t13*v___t14);
-    const T v___t15 = gexp((T(2.2) + (T(0.05)*s_V)));
-    const T v___t16 = gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))));
-    const T v___t17 = (T(1.0)/(T(1.0) + v___t15));
-    const T v_beta_d = (T(0.07)*v___t16*v___t17);
-    const T v___t18 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t19 = gexp(((-T(0.224)) - ((T(0.008)*s_V))));
-    const T v___t20 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t18)));
-    const T v_alpha_f = (T(0.012)*v___t19*v___t20);
-    const T v___t21 = gexp(((-T(6.0)) - ((T(0.2)*s_V))));
-    const T v___t22 = gexp(((-T(0.6)) - ((T(0.02)*s_V))));
-    const T v___t23 = (T(1.0)/(T(1.0) + v___t21));
-    const T v_beta_f = (T(0.0065)*v___t22*v___t23);
-    const T v___t24 = gexp((T(0.04)*s_V));
-    const T v___t25 = gexp((-(T(0.04)*s_V)));
-    const T v_i_x1 = (T(0.0019727757115328517)*v___t25*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)));
-    const T v___t26 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t27 = gexp((T(0.08264462809917356)*s_V));
-    const T v___t28 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t26)));
-    const T v_alpha_x1 = (T(0.031158410986342627)*v___t27*v___t28);
-    const T v___t29 = gexp(((-T(0.8)) - ((T(0.04)*s_V))));
-    const T v___t30 = gexp((-(T(0.05998800239952009)*s_V)));
-    const T v___t31 = (T(1.0)/(T(1.0) + v___t29));
-    const T v_beta_x1 = (T(0.0003916464405623223)*v___t30*v___t31);
+    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
+    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
+    const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
+    const T v___t14 = gexp((T(0.05)*s_V));
+    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
+    const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
+    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
+    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
+    const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
+    const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
+    const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
+    const T v___t21 = gexp((T(0.04)*s_V));
+    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
+    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
+    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
+    const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
+    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
+    const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t32 = gexp((-(T(0.04)*v_V_eff_1)));
-    const T v___t33 = (T(1.0)/(T(1.0) - ((v___t32))));
-    const T v___t34 = gexp((T(0.08)*s_V));
-    const T v___t35 = (T(1.0)/((T(8.331137487687693)*v___t24) + (T(69.4078518387552)*v___t34)));
-    const T v_i_K1 = ((T(0.0035)*v___t33*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t35*((-T(4.0)) + (T(119.85640018958804)*v___t24))));
+    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
+    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
+    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
-    const T v_dE_s_dCai = (-(T(13.0287)*v___t11));
+    const T v_dE_s_dCai = (-(T(13.0287)*v___t10));
     const T v_di_s_dCai = (P[15]*s_d*v_dE_s_dCai*s_f);
     const T v_dV_eff_1_dV = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0));
-    const T v_di_K1_dV = ((T(0.0007000000000000001)*v___t33) + (T(0.016779896026542326)*v___t24*v___t35) + (T(0.0035)*(v___t35*v___t35)*((-T(4.0)) + (T(119.85640018958804)*v___t24))*((-(T(0.3332454995075077)*v___t24)) - ((T(5.552628147100417)*v___t34)))) - ((T(0.00028000000000000003)*v___t32*v_dV_eff_1_dV*(v___t33*v___t33)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
+    const T v_di_K1_dV = ((T(0.0007000000000000001)*v___t29) + (T(0.016779896026542326)*v___t21*v___t30) + (T(0.0035)*(v___t30*v___t30)*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))) - ((T(0.00028000000000000003)*v___t28*v_dV_eff_1_dV*(v___t29*v___t29)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
     const T v_di_Na_dV = (P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)));
     const T v_di_s_dV = (s_d*s_f*P[3]);
-    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*v___t25*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)))));
+    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)))));
     rhs[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     rhs[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
     rhs[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
@@ -248,49 +243,44 @@ struct M_beeler_reuter_1977 {
     const T v___t4 = gexp((-(T(0.082)*s_V)));
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.2)*s_V)));
-    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*v___t6)));
+    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
-    const T v___t8 = gexp((-(T(0.1)*s_V)));
-    const T v___t9 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t8)));
-    const T v_beta_j = (T(0.3)*v___t9);
-    const T v___t10 = glog((T(0.001)*s_Cai));
-    const T v___t11 = (T(1.0)/s_Cai);
-    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t10)));
+    const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
+    const T v_beta_j = (T(0.3)*v___t8);
+    const T v___t9 = glog((T(0.001)*s_Cai));
+    const T v___t10 = (T(1.0)/s_Cai);
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t12 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t13 = gexp((T(0.05) - ((T(0.01)*s_V))));
-    const T v___t14 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t12)));
-    const T v_alpha_d = (T(0.095)*v___t13*v___t14);
-    const T v___t15 = gexp((T(2.2) + (T(0.05)*s_V)));
-    const T v___t16 = gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))));
-    const T v___t17 = (T(1.0)/(T(1.0) + v___t15));
-    const T v_beta_d = (T(0.07)*v___t16*v___t17);
-    const T v___t18 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t19 = gexp(((-T(0.224)) - ((T(0.008)*s_V))));
-    const T v___t20 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t18)));
-    const T v_alpha_f = (T(0.012)*v___t19*v___t20);
-    const T v___t21 = gexp(((-T(6.0)) - ((T(0.2)*s_V))));
-    const T v___t22 = gexp(((-T(0.6)) - ((T(0.02)*s_V))));
-    const T v___t23 = (T(1.0)/(T(1.0) + v___t21));
-    const T v_beta_f = (T(0.0065)*v___t22*v___t23);
-    const T v___t24 = gexp((T(0.04)*s_V));
-    const T v___t25 = gexp((-(T(0.04)*s_V)));
-    const T v_i_x1 = (T(0.0019727757115328517)*v___t25*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)));
-    const T v___t26 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t27 = gexp((T(0.08264462809917356)*s_V));
-    const T v___t28 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t26)));
-    const T v_alpha_x1 = (T(0.031158410986342627)*v___t27*v___t28);
-    const T v___t29 = gexp(((-T(0.8)) - ((T(0.04)*s_V))));
-    const T v___t30 = gexp((-(T(0.05998800239952009)*s_V)));
-    const T v___t31 = (T(1.0)/(T(1.0) + v___t29));
-    const T v_beta_x1 = (T(0.0003916464405623223)*v___t30*v___t31);
+    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
+    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
+    const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
+    const T v___t14 = gexp((T(0.05)*s_V));
+    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
+    const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
+    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
+    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
+    const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
+    const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
+    const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
+    const T v___t21 = gexp((T(0.04)*s_V));
+    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
+    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
+    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
+    const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
+    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
+    const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t32 = gexp((-(T(0.04)*v_V_eff_1)));
-    const T v___t33 = (T(1.0)/(T(1.0) - ((v___t32))));
-    const T v___t34 = gexp((T(0.08)*s_V));
-    const T v___t35 = (T(1.0)/((T(8.331137487687693)*v___t24) + (T(69.4078518387552)*v___t34)));
-    const T v_i_K1 = ((T(0.0035)*v___t33*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t35*((-T(4.0)) + (T(119.85640018958804)*v___t24))));
+    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
+    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
+    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     values[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     values[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
@@ -330,57 +320,52 @@ struct M_beeler_reuter_1977 {
     const T v___t4 = gexp((-(T(0.082)*s_V)));
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.2)*s_V)));
-    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*v___t6)));
+    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
-    const T v___t8 = gexp((-(T(0.1)*s_V)));
-    const T v___t9 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t8)));
-    const T v_beta_j = (T(0.3)*v___t9);
-    const T v___t10 = glog((T(0.001)*s_Cai));
-    const T v___t11 = (T(1.0)/s_Cai);
-    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t10)));
+    const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
+    const T v_beta_j = (T(0.3)*v___t8);
+    const T v___t9 = glog((T(0.001)*s_Cai));
+    const T v___t10 = (T(1.0)/s_Cai);
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t12 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t13 = gexp((T(0.05) - ((T(0.01)*s_V))));
-    const T v___t14 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t12)));
-    const T v_alpha_d = (T(0.095)*v___t13*v___t14);
-    const T v___t15 = gexp((T(2.2) + (T(0.05)*s_V)));
-    const T v___t16 = gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))));
-    const T v___t17 = (T(1.0)/(T(1.0) + v___t15));
-    const T v_beta_d = (T(0.07)*v___t16*v___t17);
-    const T v___t18 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t19 = gexp(((-T(0.224)) - ((T(0.008)*s_V))));
-    const T v___t20 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t18)));
-    const T v_alpha_f = (T(0.012)*v___t19*v___t20);
-    const T v___t21 = gexp(((-T(6.0)) - ((T(0.2)*s_V))));
-    const T v___t22 = gexp(((-T(0.6)) - ((T(0.02)*s_V))));
-    const T v___t23 = (T(1.0)/(T(1.0) + v___t21));
-    const T v_beta_f = (T(0.0065)*v___t22*v___t23);
-    const T v___t24 = gexp((T(0.04)*s_V));
-    const T v___t25 = gexp((-(T(0.04)*s_V)));
-    const T v_i_x1 = (T(0.0019727757115328517)*v___t25*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)));
-    const T v___t26 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t27 = gexp((T(0.08264462809917356)*s_V));
-    const T v___t28 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t26)));
-    const T v_alpha_x1 = (T(0.031158410986342627)*v___t27*v___t28);
-    const T v___t29 = gexp(((-T(0.8)) - ((T(0.04)*s_V))));
-    const T v___t30 = gexp((-(T(0.05998800239952009)*s_V)));
-    const T v___t31 = (T(1.0)/(T(1.0) + v___t29));
-    const T v_beta_x1 = (T(0.0003916464405623223)*v___t30*v___t31);
+    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
+    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
+    const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
+    const T v___t14 = gexp((T(0.05)*s_V));
+    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
+    const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
+    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
+    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
+    const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
+    const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
+    const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
+    const T v___t21 = gexp((T(0.04)*s_V));
+    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
+    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
+    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
+    const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
+    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
+    const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t32 = gexp((-(T(0.04)*v_V_eff_1)));
-    const T v___t33 = (T(1.0)/(T(1.0) - ((v___t32))));
-    const T v___t34 = gexp((T(0.08)*s_V));
-    const T v___t35 = (T(1.0)/((T(8.331137487687693)*v___t24) + (T(69.4078518387552)*v___t34)));
-    const T v_i_K1 = ((T(0.0035)*v___t33*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t35*((-T(4.0)) + (T(119.85640018958804)*v___t24))));
+    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
+    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
+    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
-    const T v_dE_s_dCai = (-(T(13.0287)*v___t11));
+    const T v_dE_s_dCai = (-(T(13.0287)*v___t10));
     const T v_di_s_dCai = (P[15]*s_d*v_dE_s_dCai*s_f);
     const T v_dV_eff_1_dV = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0));
-    const T v_di_K1_dV = ((T(0.0007000000000000001)*v___t33) + (T(0.016779896026542326)*v___t24*v___t35) + (T(0.0035)*(v___t35*v___t35)*((-T(4.0)) + (T(119.85640018958804)*v___t24))*((-(T(0.3332454995075077)*v___t24)) - ((T(5.552628147100417)*v___t34)))) - ((T(0.00028000000000000003)*v___t32*v_dV_eff_1_dV*(v___t33*v___t33)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
+    const T v_di_K1_dV = ((T(0.0007000000000000001)*v___t29) + (T(0.016779896026542326)*v___t21*v___t30) + (T(0.0035)*(v___t30*v___t30)*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))) - ((T(0.00028000000000000003)*v___t28*v_dV_eff_1_dV*(v___t29*v___t29)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
     const T v_di_Na_dV = (P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)));
     const T v_di_s_dV = (s_d*s_f*P[3]);
-    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*v___t25*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)))));
+    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)))));
     T lin_v[8], abar[8], rhs_v[8], bbar[8];
     rhs_v[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     rhs_v[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
@@ -403,52 +388,47 @@ struct M_beeler_reuter_1977 {
     const T a_di_s_dV = (P[16]*abar[7]);
     const T a_di_Na_dV = (P[16]*abar[7]);
     const T a_di_K1_dV = (P[16]*abar[7]);
-    const T a_dV_eff_1_dV = (-(T(0.00028000000000000003)*a_di_K1_dV*v___t32*(v___t33*v___t33)*(T(4.6000000000000005) + (T(0.2)*s_V))));
+    const T a_dV_eff_1_dV = (-(T(0.00028000000000000003)*a_di_K1_dV*v___t28*(v___t29*v___t29)*(T(4.6000000000000005) + (T(0.2)*s_V))));
     const T a_di_s_dCai = (-(T(0.01)*abar[3]));
     const T a_dE_s_dCai = (a_di_s_dCai*P[15]*s_d*s_f);
     const T a_i_K1 = (-(P[14]*bbar[7]));
-    const T a___t35 = ((a_di_K1_dV*((T(0.016779896026542326)*v___t24) + (T(0.007)*v___t35*((-T(4.0)) + (T(119.85640018958804)*v___t24))*((-(T(0.3332454995075077)*v___t24)) - ((T(5.552628147100417)*v___t34)))))) + (a_i_K1*((-T(0.014)) + (T(0.4194974006635582)*v___t24))));
-    const T a___t34 = ((-(T(69.4078518387552)*a___t35*(v___t35*v___t35))) - ((T(0.01943419851485146)*a_di_K1_dV*(v___t35*v___t35)*((-T(4.0)) + (T(119.85640018958804)*v___t24)))));
-    const T a___t33 = ((a_di_K1_dV*(T(0.0007000000000000001) - ((T(0.0005600000000000001)*v___t32*v___t33*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V)))))) + (a_i_K1*(T(0.016100000000000003) + (T(0.0007000000000000001)*s_V))));
-    const T a___t32 = ((a___t33*(v___t33*v___t33)) - ((T(0.00028000000000000003)*a_di_K1_dV*v_dV_eff_1_dV*(v___t33*v___t33)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
-    const T a_V_eff_1 = (-(T(0.04)*a___t32*v___t32));
+    const T a___t30 = ((a_di_K1_dV*((T(0.016779896026542326)*v___t21) + (T(0.007)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))))) + (a_i_K1*((-T(0.014)) + (T(0.4194974006635582)*v___t21))));
+    const T a___t29 = ((a_di_K1_dV*(T(0.0007000000000000001) - ((T(0.0005600000000000001)*v___t28*v___t29*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V)))))) + (a_i_K1*(T(0.016100000000000003) + (T(0.0007000000000000001)*s_V))));
+    const T a___t28 = ((a___t29*(v___t29*v___t29)) - ((T(0.00028000000000000003)*a_di_K1_dV*v_dV_eff_1_dV*(v___t29*v___t29)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
+    const T a_V_eff_1 = (-(T(0.04)*a___t28*v___t28));
     const T a_beta_x1 = ((-(abar[6])) - ((bbar[6]*s_x1)));
-    const T a___t31 = (T(0.0003916464405623223)*a_beta_x1*v___t30);
-    const T a___t30 = (T(0.0003916464405623223)*a_beta_x1*v___t31);
-    const T a___t29 = (-(a___t31*(v___t31*v___t31)));
+    const T a___t27 = (T(0.0003916464405623223)*a_beta_x1*v___t26);
+    const T a___t26 = (T(0.0003916464405623223)*a_beta_x1*v___t27);
     const T a_alpha_x1 = ((-(abar[6])) + (bbar[6]*(T(1.0) - ((s_x1)))));
-    const T a___t28 = (T(0.031158410986342627)*a_alpha_x1*v___t27);
-    const T a___t27 = (T(0.031158410986342627)*a_alpha_x1*v___t28);
-    const T a___t26 = (-(T(17.41170806332765)*a___t28*(v___t28*v___t28)));
+    const T a___t25 = (T(0.031158410986342627)*a_alpha_x1*v___t24);
+    const T a___t24 = (T(0.031158410986342627)*a_alpha_x1*v___t25);
+    const T a___t23 = (-(T(17.41170806332765)*a___t25*(v___t25*v___t25)));
     const T a_i_x1 = (-(P[14]*bbar[7]));
-    const T a___t25 = ((T(0.0019727757115328517)*a_i_x1*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24))) - ((T(7.891102846131407e-05)*a_di_x1_dV*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)))));
-    const T a___t24 = ((a_di_K1_dV*((T(0.016779896026542326)*v___t35) + (T(0.4194974006635582)*(v___t35*v___t35)*((-(T(0.3332454995075077)*v___t24)) - ((T(5.552628147100417)*v___t34)))) - ((T(0.001166359248276277)*(v___t35*v___t35)*((-T(4.0)) + (T(119.85640018958804)*v___t24)))))) + (T(0.4194974006635582)*a_i_K1*v___t35) - ((T(8.331137487687693)*a___t35*(v___t35*v___t35))) + (T(0.042924447768975804)*a_i_x1*v___t25*s_x1) - ((T(0.001716977910759032)*a_di_x1_dV*v___t25*s_x1)));
+    const T a___t22 = ((-(T(0.4493289641172216)*a___t27*(v___t27*v___t27))) + (T(0.0019727757115328517)*a_i_x1*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21))) - ((T(7.891102846131407e-05)*a_di_x1_dV*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)))));
+    const T a___t21 = ((a_di_K1_dV*((T(0.016779896026542326)*v___t30) + (T(0.4194974006635582)*(v___t30*v___t30)*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))) + (T(0.0035)*(v___t30*v___t30)*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-T(0.3332454995075077)) - ((T(11.105256294200833)*v___t21)))))) + (T(0.4194974006635582)*a_i_K1*v___t30) - ((a___t30*(v___t30*v___t30)*(T(8.331137487687693) + (T(138.8157036775104)*v___t21)))) + (T(0.042924447768975804)*a_i_x1*v___t22*s_x1) - ((T(0.001716977910759032)*a_di_x1_dV*v___t22*s_x1)));
     const T a_beta_f = ((-(abar[5])) - ((bbar[5]*s_f)));
-    const T a___t23 = (T(0.0065)*a_beta_f*v___t22);
-    const T a___t22 = (T(0.0065)*a_beta_f*v___t23);
-    const T a___t21 = (-(a___t23*(v___t23*v___t23)));
+    const T a___t20 = (T(0.0035672756346111717)*a_beta_f*(v___t12*v___t12));
     const T a_alpha_f = ((-(abar[5])) + (bbar[5]*(T(1.0) - ((s_f)))));
-    const T a___t20 = (T(0.012)*a_alpha_f*v___t19);
-    const T a___t19 = (T(0.012)*a_alpha_f*v___t20);
-    const T a___t18 = (-(T(66.5465065250986)*a___t20*(v___t20*v___t20)));
+    const T a___t19 = (T(0.009591781612432381)*a_alpha_f*v___t18);
+    const T a___t18 = (T(0.009591781612432381)*a_alpha_f*v___t19);
+    const T a___t17 = (-(T(66.5465065250986)*a___t19*(v___t19*v___t19)));
     const T a_beta_d = ((-(abar[4])) - ((bbar[4]*s_d)));
-    const T a___t17 = (T(0.07)*a_beta_d*v___t16);
-    const T a___t16 = (T(0.07)*a_beta_d*v___t17);
-    const T a___t15 = (-(a___t17*(v___t17*v___t17)));
+    const T a___t16 = (T(0.03320606467536786)*a_beta_d*v___t15);
+    const T a___t15 = (T(0.03320606467536786)*a_beta_d*v___t16);
+    const T a___t14 = (-(T(9.02501349943412)*a___t16*(v___t16*v___t16)));
     const T a_alpha_d = ((-(abar[4])) + (bbar[4]*(T(1.0) - ((s_d)))));
-    const T a___t14 = (T(0.095)*a_alpha_d*v___t13);
-    const T a___t13 = (T(0.095)*a_alpha_d*v___t14);
-    const T a___t12 = (-(T(1.4332881385696572)*a___t14*(v___t14*v___t14)));
+    const T a___t13 = (T(0.09987075415572229)*a_alpha_d*v___t12);
+    const T a___t12 = ((T(0.09987075415572229)*a_alpha_d*v___t13) + (T(0.0071345512692223435)*a_beta_f*v___t12*v___t20));
+    const T a___t11 = (-(T(1.4332881385696572)*a___t13*(v___t13*v___t13)));
     const T a_i_s = ((-(T(0.01)*bbar[3])) - ((P[14]*bbar[7])));
     const T a_E_s = (-(a_i_s*s_d*s_f*P[3]));
-    const T a___t11 = (-(T(13.0287)*a_dE_s_dCai));
-    const T a___t10 = (-(T(13.0287)*a_E_s));
+    const T a___t10 = (-(T(13.0287)*a_dE_s_dCai));
+    const T a___t9 = (-(T(13.0287)*a_E_s));
     const T a_beta_j = ((-(abar[2])) - ((bbar[2]*s_j)));
-    const T a___t9 = (T(0.3)*a_beta_j);
-    const T a___t8 = (-(T(0.040762203978366204)*a___t9*(v___t9*v___t9)));
+    const T a___t8 = (T(0.3)*a_beta_j);
     const T a_alpha_j = ((-(abar[2])) + (bbar[2]*(T(1.0) - ((s_j)))));
     const T a___t7 = (T(1.8690473007222892e-10)*a_alpha_j*v___t3);
-    const T a___t6 = (-(T(1.6788275299956603e-07)*a___t7*(v___t7*v___t7)));
+    const T a___t6 = ((-(T(0.040762203978366204)*a___t8*(v___t8*v___t8))) - ((T(3.3576550599913205e-07)*a___t7*v___t6*(v___t7*v___t7))) - ((T(0.004957504353332717)*a___t20*v___t6*(v___t20*v___t20))));
     const T a_beta_h = ((-(abar[1])) - ((bbar[1]*s_h)));
     const T a___t5 = (T(1.7)*a_beta_h);
     const T a___t4 = (-(T(0.1580253208896478)*a___t5*(v___t5*v___t5)));
@@ -464,11 +444,11 @@ struct M_beeler_reuter_1977 {
     ybar[0] = ((bbar[0]*((-(v_alpha_m)) - ((v_beta_m)))) + (T(3.0)*a_di_Na_dV*P[1]*s_h*s_j*(s_m*s_m)) + (T(3.0)*a_i_Na*P[1]*s_h*s_j*(s_m*s_m)*(s_V + P[10])));
     ybar[1] = ((bbar[1]*((-(v_alpha_h)) - ((v_beta_h)))) + (a_di_Na_dV*P[1]*s_j*(s_m*s_m*s_m)) + (a_i_Na*P[1]*s_j*(s_m*s_m*s_m)*(s_V + P[10])));
     ybar[2] = ((bbar[2]*((-(v_alpha_j)) - ((v_beta_j)))) + (a_di_Na_dV*P[1]*s_h*(s_m*s_m*s_m)) + (a_i_Na*P[1]*s_h*(s_m*s_m*s_m)*(s_V + P[10])));
-    ybar[3] = ((-(T(0.07)*bbar[3])) - ((a___t11*(v___t11*v___t11))) + (T(1.0)*a___t10*v___t11));
+    ybar[3] = ((-(T(0.07)*bbar[3])) - ((a___t10*(v___t10*v___t10))) + (T(1.0)*a___t9*v___t10));
     ybar[4] = ((bbar[4]*((-(v_alpha_d)) - ((v_beta_d)))) + (a_di_s_dV*s_f*P[3]) + (a_di_s_dCai*P[15]*v_dE_s_dCai*s_f) + (a_i_s*s_f*P[3]*(s_V - ((v_E_s)))));
     ybar[5] = ((bbar[5]*((-(v_alpha_f)) - ((v_beta_f)))) + (a_di_s_dV*s_d*P[3]) + (a_di_s_dCai*P[15]*s_d*v_dE_s_dCai) + (a_i_s*s_d*P[3]*(s_V - ((v_E_s)))));
-    ybar[6] = ((a_di_x1_dV*(T(0.0017169779107590322) - ((T(7.891102846131407e-05)*v___t25*((-T(1.0)) + (T(21.75840239619708)*v___t24)))))) + (bbar[6]*((-(v_alpha_x1)) - ((v_beta_x1)))) + (T(0.0019727757115328517)*a_i_x1*v___t25*((-T(1.0)) + (T(21.75840239619708)*v___t24))));
-    ybar[7] = ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) - ((T(0.2)*a___t21*v___t21)) - ((T(0.04)*a___t29*v___t29)) - ((T(0.02)*a___t22*v___t22)) - ((T(0.01694915254237288)*a___t16*v___t16)) - ((T(0.01)*a___t13*v___t13)) - ((T(0.008)*a___t19*v___t19)) + (T(0.05)*a___t15*v___t15) + (T(0.0007000000000000001)*a_i_K1*v___t33) + (T(0.08264462809917356)*a___t27*v___t27) + (T(0.14992503748125938)*a___t18*v___t18) + (T(0.04)*a___t24*v___t24) + (T(0.08)*a___t34*v___t34) + (T(0.05714285714285714)*a___t26*v___t26) - ((T(0.25)*a___t3*v___t3)) - ((T(0.07199424046076314)*a___t12*v___t12)) - ((T(0.1)*a___t8*v___t8)) - ((T(0.2)*a___t6*v___t6)) - ((T(0.04)*a___t25*v___t25)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t30*v___t30)) + (a_i_s*s_d*s_f*P[3]) - ((T(5.6000000000000006e-05)*a_di_K1_dV*v___t32*v_dV_eff_1_dV*(v___t33*v___t33))));
+    ybar[6] = ((a_di_x1_dV*(T(0.0017169779107590322) - ((T(7.891102846131407e-05)*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21)))))) + (bbar[6]*((-(v_alpha_x1)) - ((v_beta_x1)))) + (T(0.0019727757115328517)*a_i_x1*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21))));
+    ybar[7] = ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) + (T(0.0007000000000000001)*a_i_K1*v___t29) + (T(0.08264462809917356)*a___t24*v___t24) + (T(0.05)*a___t14*v___t14) + (T(0.14992503748125938)*a___t17*v___t17) + (T(0.04)*a___t21*v___t21) + (T(0.05714285714285714)*a___t23*v___t23) - ((T(0.25)*a___t3*v___t3)) - ((T(0.008)*a___t18*v___t18)) - ((T(0.07199424046076314)*a___t11*v___t11)) - ((T(0.1)*a___t6*v___t6)) - ((T(0.01694915254237288)*a___t15*v___t15)) - ((T(0.01)*a___t12*v___t12)) - ((T(0.04)*a___t22*v___t22)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t26*v___t26)) + (a_i_s*s_d*s_f*P[3]) - ((T(5.6000000000000006e-05)*a_di_K1_dV*v___t28*v_dV_eff_1_dV*(v___t29*v___t29))));
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
   }
 
@@ -499,49 +479,44 @@ struct M_beeler_reuter_1977 {
     const T v___t4 = gexp((-(T(0.082)*s_V)));
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.2)*s_V)));
-    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*v___t6)));
+    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
-    const T v___t8 = gexp((-(T(0.1)*s_V)));
-    const T v___t9 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t8)));
-    const T v_beta_j = (T(0.3)*v___t9);
-    const T v___t10 = glog((T(0.001)*s_Cai));
-    const T v___t11 = (T(1.0)/s_Cai);
-    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t10)));
+    const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
+    const T v_beta_j = (T(0.3)*v___t8);
+    const T v___t9 = glog((T(0.001)*s_Cai));
+    const T v___t10 = (T(1.0)/s_Cai);
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t12 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t13 = gexp((T(0.05) - ((T(0.01)*s_V))));
-    const T v___t14 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t12)));
-    const T v_alpha_d = (T(0.095)*v___t13*v___t14);
-    const T v___t15 = gexp((T(2.2) + (T(0.05)*s_V)));
-    const T v___t16 = gexp(((-T(0.7457627118644068)) - ((T(0.01694915254237288)*s_V))));
-    const T v___t17 = (T(1.0)/(T(1.0) + v___t15));
-    const T v_beta_d = (T(0.07)*v___t16*v___t17);
-    const T v___t18 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t19 = gexp(((-T(0.224)) - ((T(0.008)*s_V))));
-    const T v___t20 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t18)));
-    const T v_alpha_f = (T(0.012)*v___t19*v___t20);
-    const T v___t21 = gexp(((-T(6.0)) - ((T(0.2)*s_V))));
-    const T v___t22 = gexp(((-T(0.6)) - ((T(0.02)*s_V))));
-    const T v___t23 = (T(1.0)/(T(1.0) + v___t21));
-    const T v_beta_f = (T(0.0065)*v___t22*v___t23);
-    const T v___t24 = gexp((T(0.04)*s_V));
-    const T v___t25 = gexp((-(T(0.04)*s_V)));
-    const T v_i_x1 = (T(0.0019727757115328517)*v___t25*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)));
-    const T v___t26 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t27 = gexp((T(0.08264462809917356)*s_V));
-    const T v___t28 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t26)));
-    const T v_alpha_x1 = (T(0.031158410986342627)*v___t27*v___t28);
-    const T v___t29 = gexp(((-T(0.8)) - ((T(0.04)*s_V))));
-    const T v___t30 = gexp((-(T(0.05998800239952009)*s_V)));
-    const T v___t31 = (T(1.0)/(T(1.0) + v___t29));
-    const T v_beta_x1 = (T(0.0003916464405623223)*v___t30*v___t31);
+    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
+    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
+    const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
+    const T v___t14 = gexp((T(0.05)*s_V));
+    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
+    const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
+    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
+    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
+    const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
+    const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
+    const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
+    const T v___t21 = gexp((T(0.04)*s_V));
+    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
+    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
+    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
+    const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
+    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
+    const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t32 = gexp((-(T(0.04)*v_V_eff_1)));
-    const T v___t33 = (T(1.0)/(T(1.0) - ((v___t32))));
-    const T v___t34 = gexp((T(0.08)*s_V));
-    const T v___t35 = (T(1.0)/((T(8.331137487687693)*v___t24) + (T(69.4078518387552)*v___t34)));
-    const T v_i_K1 = ((T(0.0035)*v___t33*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t35*((-T(4.0)) + (T(119.85640018958804)*v___t24))));
+    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
+    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
+    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     T f_v[8], bbar[8];
     f_v[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
@@ -554,47 +529,42 @@ struct M_beeler_reuter_1977 {
     f_v[7] = (P[14]*(T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1))));
     seed(f_v, bbar);
     const T a_i_K1 = (-(P[14]*bbar[7]));
-    const T a___t35 = (a_i_K1*((-T(0.014)) + (T(0.4194974006635582)*v___t24)));
-    const T a___t34 = (-(T(69.4078518387552)*a___t35*(v___t35*v___t35)));
-    const T a___t33 = (a_i_K1*(T(0.016100000000000003) + (T(0.0007000000000000001)*s_V)));
-    const T a___t32 = (a___t33*(v___t33*v___t33));
-    const T a_V_eff_1 = (-(T(0.04)*a___t32*v___t32));
+    const T a___t30 = (a_i_K1*((-T(0.014)) + (T(0.4194974006635582)*v___t21)));
+    const T a___t29 = (a_i_K1*(T(0.016100000000000003) + (T(0.0007000000000000001)*s_V)));
+    const T a___t28 = (a___t29*(v___t29*v___t29));
+    const T a_V_eff_1 = (-(T(0.04)*a___t28*v___t28));
     const T a_beta_x1 = (-(bbar[6]*s_x1));
-    const T a___t31 = (T(0.0003916464405623223)*a_beta_x1*v___t30);
-    const T a___t30 = (T(0.0003916464405623223)*a_beta_x1*v___t31);
-    const T a___t29 = (-(a___t31*(v___t31*v___t31)));
+    const T a___t27 = (T(0.0003916464405623223)*a_beta_x1*v___t26);
+    const T a___t26 = (T(0.0003916464405623223)*a_beta_x1*v___t27);
     const T a_alpha_x1 = (bbar[6]*(T(1.0) - ((s_x1))));
-    const T a___t28 = (T(0.031158410986342627)*a_alpha_x1*v___t27);
-    const T a___t27 = (T(0.031158410986342627)*a_alpha_x1*v___t28);
-    const T a___t26 = (-(T(17.41170806332765)*a___t28*(v___t28*v___t28)));
+    const T a___t25 = (T(0.031158410986342627)*a_alpha_x1*v___t24);
+    const T a___t24 = (T(0.031158410986342627)*a_alpha_x1*v___t25);
+    const T a___t23 = (-(T(17.41170806332765)*a___t25*(v___t25*v___t25)));
     const T a_i_x1 = (-(P[14]*bbar[7]));
-    const T a___t25 = (T(0.0019727757115328517)*a_i_x1*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t24)));
-    const T a___t24 = ((T(0.4194974006635582)*a_i_K1*v___t35) - ((T(8.331137487687693)*a___t35*(v___t35*v___t35))) + (T(0.042924447768975804)*a_i_x1*v___t25*s_x1));
+    const T a___t22 = ((-(T(0.4493289641172216)*a___t27*(v___t27*v___t27))) + (T(0.0019727757115328517)*a_i_x1*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21))));
+    const T a___t21 = ((T(0.4194974006635582)*a_i_K1*v___t30) - ((a___t30*(v___t30*v___t30)*(T(8.331137487687693) + (T(138.8157036775104)*v___t21)))) + (T(0.042924447768975804)*a_i_x1*v___t22*s_x1));
     const T a_beta_f = (-(bbar[5]*s_f));
-    const T a___t23 = (T(0.0065)*a_beta_f*v___t22);
-    const T a___t22 = (T(0.0065)*a_beta_f*v___t23);
-    const T a___t21 = (-(a___t23*(v___t23*v___t23)));
+    const T a___t20 = (T(0.0035672756346111717)*a_beta_f*(v___t12*v___t12));
     const T a_alpha_f = (bbar[5]*(T(1.0) - ((s_f))));
-    const T a___t20 = (T(0.012)*a_alpha_f*v___t19);
-    const T a___t19 = (T(0.012)*a_alpha_f*v___t20);
-    const T a___t18 = (-(T(66.5465065250986)*a___t20*(v___t20*v___t20)));
+    const T a___t19 = (T(0.009591781612432381)*a_alpha_f*v___t18);
+    const T a___t18 = (T(0.009591781612432381)*a_alpha_f*v___t19);
+    const T a___t17 = (-(T(66.5465065250986)*a___t19*(v___t19*v___t19)));
     const T a_beta_d = (-(bbar[4]*s_d));
-    const T a___t17 = (T(0.07)*a_beta_d*v___t16);
-    const T a___t16 = (T(0.07)*a_beta_d*v___t17);
-    const T a___t15 = (-(a___t17*(v___t17*v___t17)));
+    const T a___t16 = (T(0.03320606467536786)*a_beta_d*v___t15);
+    const T a___t15 = (T(0.03320606467536786)*a_beta_d*v___t16);
+    const T a___t14 = (-(T(9.02501349943412)*a___t16*(v___t16*v___t16)));
     const T a_alpha_d = (bbar[4]*(T(1.0) - ((s_d))));
-    const T a___t14 = (T(0.095)*a_alpha_d*v___t13);
-    const T a___t13 = (T(0.095)*a_alpha_d*v___t14);
-    const T a___t12 = (-(T(1.4332881385696572)*a___t14*(v___t14*v___t14)));
+    const T a___t13 = (T(0.09987075415572229)*a_alpha_d*v___t12);
+    const T a___t12 = ((T(0.09987075415572229)*a_alpha_d*v___t13) + (T(0.0071345512692223435)*a_beta_f*v___t12*v___t20));
+    const T a___t11 = (-(T(1.4332881385696572)*a___t13*(v___t13*v___t13)));
     const T a_i_s = ((-(T(0.01)*bbar[3])) - ((P[14]*bbar[7])));
     const T a_E_s = (-(a_i_s*s_d*s_f*P[3]));
-    const T a___t10 = (-(T(13.0287)*a_E_s));
+    const T a___t9 = (-(T(13.0287)*a_E_s));
     const T a_beta_j = (-(bbar[2]*s_j));
-    const T a___t9 = (T(0.3)*a_beta_j);
-    const T a___t8 = (-(T(0.040762203978366204)*a___t9*(v___t9*v___t9)));
+    const T a___t8 = (T(0.3)*a_beta_j);
     const T a_alpha_j = (bbar[2]*(T(1.0) - ((s_j))));
     const T a___t7 = (T(1.8690473007222892e-10)*a_alpha_j*v___t3);
-    const T a___t6 = (-(T(1.6788275299956603e-07)*a___t7*(v___t7*v___t7)));
+    const T a___t6 = ((-(T(0.040762203978366204)*a___t8*(v___t8*v___t8))) - ((T(3.3576550599913205e-07)*a___t7*v___t6*(v___t7*v___t7))) - ((T(0.004957504353332717)*a___t20*v___t6*(v___t20*v___t20))));
     const T a_beta_h = (-(bbar[1]*s_h));
     const T a___t5 = (T(1.7)*a_beta_h);
     const T a___t4 = (-(T(0.1580253208896478)*a___t5*(v___t5*v___t5)));
@@ -610,11 +580,11 @@ struct M_beeler_reuter_1977 {
     ybar[0] = ((bbar[0]*((-(v_alpha_m)) - ((v_beta_m)))) + (T(3.0)*a_i_Na*P[1]*s_h*s_j*(s_m*s_m)*(s_V + P[10])));
     ybar[1] = ((bbar[1]*((-(v_alpha_h)) - ((v_beta_h)))) + (a_i_Na*P[1]*s_j*(s_m*s_m*s_m)*(s_V + P[10])));
     ybar[2] = ((bbar[2]*((-(v_alpha_j)) - ((v_beta_j)))) + (a_i_Na*P[1]*s_h*(s_m*s_m*s_m)*(s_V + P[10])));
-    ybar[3] = ((-(T(0.07)*bbar[3])) + (T(1.0)*a___t10*v___t11));
+    ybar[3] = ((-(T(0.07)*bbar[3])) + (T(1.0)*a___t9*v___t10));
     ybar[4] = ((bbar[4]*((-(v_alpha_d)) - ((v_beta_d)))) + (a_i_s*s_f*P[3]*(s_V - ((v_E_s)))));
     ybar[5] = ((bbar[5]*((-(v_alpha_f)) - ((v_beta_f)))) + (a_i_s*s_d*P[3]*(s_V - ((v_E_s)))));
-    ybar[6] = ((bbar[6]*((-(v_alpha_x1)) - ((v_beta_x1)))) + (T(0.0019727757115328517)*a_i_x1*v___t25*((-T(1.0)) + (T(21.75840239619708)*v___t24))));
-    ybar[7] = ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) - ((T(0.2)*a___t21*v___t21)) - ((T(0.04)*a___t29*v___t29)) - ((T(0.02)*a___t22*v___t22)) - ((T(0.01694915254237288)*a___t16*v___t16)) - ((T(0.01)*a___t13*v___t13)) - ((T(0.008)*a___t19*v___t19)) + (T(0.05)*a___t15*v___t15) + (T(0.0007000000000000001)*a_i_K1*v___t33) + (T(0.08264462809917356)*a___t27*v___t27) + (T(0.14992503748125938)*a___t18*v___t18) + (T(0.04)*a___t24*v___t24) + (T(0.08)*a___t34*v___t34) + (T(0.05714285714285714)*a___t26*v___t26) - ((T(0.25)*a___t3*v___t3)) - ((T(0.07199424046076314)*a___t12*v___t12)) - ((T(0.1)*a___t8*v___t8)) - ((T(0.2)*a___t6*v___t6)) - ((T(0.04)*a___t25*v___t25)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t30*v___t30)) + (a_i_s*s_d*s_f*P[3]));
+    ybar[6] = ((bbar[6]*((-(v_alpha_x1)) - ((v_beta_x1)))) + (T(0.0019727757115328517)*a_i_x1*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21))));
+    ybar[7] = ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) + (T(0.0007000000000000001)*a_i_K1*v___t29) + (T(0.08264462809917356)*a___t24*v___t24) + (T(0.05)*a___t14*v___t14) + (T(0.14992503748125938)*a___t17*v___t17) + (T(0.04)*a___t21*v___t21) + (T(0.05714285714285714)*a___t23*v___t23) - ((T(0.25)*a___t3*v___t3)) - ((T(0.008)*a___t18*v___t18)) - ((T(0.07199424046076314)*a___t11*v___t11)) - ((T(0.1)*a___t6*v___t6)) - ((T(0.01694915254237288)*a___t15*v___t15)) - ((T(0.01)*a___t12*v___t12)) - ((T(0.04)*a___t22*v___t22)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t26*v___t26)) + (a_i_s*s_d*s_f*P[3]));
     (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;
   }
 };
