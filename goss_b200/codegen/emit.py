@@ -26,6 +26,7 @@ import sympy as sp
 from .ir import CONST, FIELD, STATE, TIME_CLS, Assign, ModelIR, Output, Program, count_ops
 from .odeparse import TIME
 from .ad import ReverseProgram
+from .factor import factor_common
 from .hoist import ConstantFolder
 from .printer import CPrinter, c_double
 
@@ -428,33 +429,34 @@ class ModelSource:
         prT, prD = self._dev_printers()
         lines = []
         for b in rp.forward:
-            t = "double" if b.cls == TIME_CLS else "T"
-            pr = prD if b.cls == TIME_CLS else prT
-            lines.append(f"const {t} v_{b.name} = {pr(b.expr)};")
+            if b.cls == TIME_CLS:
+                lines.append(f"const double v_{b.name} = {prD(b.expr)};")
+            else:
+                lines.append(f"const T v_{b.name} = {prT(factor_common(b.expr))};")
         # the values themselves, then the caller's cotangents for them
         n = len(self.states)
         decl = ", ".join(f"{v}[{n}], {c}[{n}]" for v, c in arrays.values())
         lines.append(f"T {decl};")
         for o in rp.outputs:
-            lines.append(f"{arrays[o.array][0]}[{o.index}] = {prT(o.expr)};")
+            lines.append(f"{arrays[o.array][0]}[{o.index}] = {prT(factor_common(o.expr))};")
         for arr, (val, _) in arrays.items():
             for i in range(n):
                 if not any(o.array == arr and o.index == i for o in rp.outputs):
                     lines.append(f"{val}[{i}] = T(0.0);")
         lines.append(seed_call)
         for adj, e in rp.reverse:
-            lines.append(f"const T a_{adj.name[len('__adj_'):]} = {prT(e)};")
+            lines.append(f"const T a_{adj.name[len('__adj_'):]} = {prT(factor_common(e))};")
         for i, e in enumerate(rp.state_bar):
-            lines.append(f"ybar[{i}] = {prT(e) if e != 0 else 'T(0.0)'};")
+            lines.append(f"ybar[{i}] = {prT(factor_common(e)) if e != 0 else 'T(0.0)'};")
         for k, e in enumerate(rp.field_bar):
-            lines.append(f"Fbar[{k}] = {prT(e) if e != 0 else 'T(0.0)'};")
+            lines.append(f"Fbar[{k}] = {prT(factor_common(e)) if e != 0 else 'T(0.0)'};")
         return lines
 
     def _dev_split_lines(self, prog: Program, arrays: Dict[str, str]) -> List[str]:
         """Body of ``prog`` with every distinct exp/log/sqrt/pow/reciprocal of
         state-dependent operands computed once (the elementary split of
-        codegen/ad.py); ``arrays`` names the output array of each of its
-        output arrays."""
+        codegen/ad.py) and common factors pulled out of sums (codegen/factor.py);
+        ``arrays`` names the output array of each of its output arrays."""
         folded = self._fold(prog)
         inter = {n: self.model.sym(n) for n in self.model.intermediates}
         rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
@@ -462,12 +464,13 @@ class ModelSource:
         prT, prD = self._dev_printers()
         lines = []
         for b in rp.forward:
-            t = "double" if b.cls == TIME_CLS else "T"
-            pr = prD if b.cls == TIME_CLS else prT
-            lines.append(f"const {t} v_{b.name} = {pr(b.expr)};")
+            if b.cls == TIME_CLS:
+                lines.append(f"const double v_{b.name} = {prD(b.expr)};")
+            else:
+                lines.append(f"const T v_{b.name} = {prT(factor_common(b.expr))};")
         n = len(self.states)
         for o in rp.outputs:
-            lines.append(f"{arrays[o.array]}[{o.index}] = {prT(o.expr)};")
+            lines.append(f"{arrays[o.array]}[{o.index}] = {prT(factor_common(o.expr))};")
         for arr, name in arrays.items():
             for i in range(n):
                 if not any(o.array == arr and o.index == i for o in rp.outputs):

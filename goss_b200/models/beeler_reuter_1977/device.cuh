@@ -190,16 +190,16 @@ struct M_beeler_reuter_1977 {
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
     const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
-    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
-    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
+    const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
+    const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     const T v_dE_s_dCai = (-(T(13.0287)*v___t10));
     const T v_di_s_dCai = (P[15]*s_d*v_dE_s_dCai*s_f);
     const T v_dV_eff_1_dV = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0));
-    const T v_di_K1_dV = ((T(0.0007000000000000001)*v___t29) + (T(0.016779896026542326)*v___t21*v___t30) + (T(0.0035)*(v___t30*v___t30)*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))) - ((T(0.00028000000000000003)*v___t28*v_dV_eff_1_dV*(v___t29*v___t29)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
+    const T v_di_K1_dV = ((v___t30*(v___t21*(T(0.016779896026542326) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-T(0.3332454995075077)) - ((T(5.552628147100417)*v___t21))))))) + (v___t29*(T(0.0007000000000000001) - ((T(0.00028000000000000003)*v___t28*v___t29*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V)))))));
     const T v_di_Na_dV = (P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)));
     const T v_di_s_dV = (s_d*s_f*P[3]);
-    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)))));
+    const T v_di_x1_dV = (s_x1*(T(0.0017169779107590322) - ((T(7.891102846131407e-05)*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21))))));
     rhs[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     rhs[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
     rhs[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
@@ -215,7 +215,7 @@ struct M_beeler_reuter_1977 {
     linear[5] = ((-(v_alpha_f)) - ((v_beta_f)));
     linear[6] = ((-(v_alpha_x1)) - ((v_beta_x1)));
     linear[3] = ((-T(0.07)) - ((T(0.01)*v_di_s_dCai)));
-    linear[7] = ((P[16]*v_di_K1_dV) + (P[16]*v_di_Na_dV) + (P[16]*v_di_s_dV) + (P[16]*v_di_x1_dV));
+    linear[7] = (P[16]*(v_di_K1_dV + v_di_Na_dV + v_di_s_dV + v_di_x1_dV));
     (void)time; (void)P; (void)PD; (void)F;
   }
 
@@ -279,8 +279,8 @@ struct M_beeler_reuter_1977 {
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
     const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
-    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
-    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
+    const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
+    const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     values[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     values[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
@@ -356,16 +356,16 @@ struct M_beeler_reuter_1977 {
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
     const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
-    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
-    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
+    const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
+    const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     const T v_dE_s_dCai = (-(T(13.0287)*v___t10));
     const T v_di_s_dCai = (P[15]*s_d*v_dE_s_dCai*s_f);
     const T v_dV_eff_1_dV = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0));
-    const T v_di_K1_dV = ((T(0.0007000000000000001)*v___t29) + (T(0.016779896026542326)*v___t21*v___t30) + (T(0.0035)*(v___t30*v___t30)*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))) - ((T(0.00028000000000000003)*v___t28*v_dV_eff_1_dV*(v___t29*v___t29)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
+    const T v_di_K1_dV = ((v___t30*(v___t21*(T(0.016779896026542326) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-T(0.3332454995075077)) - ((T(5.552628147100417)*v___t21))))))) + (v___t29*(T(0.0007000000000000001) - ((T(0.00028000000000000003)*v___t28*v___t29*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V)))))));
     const T v_di_Na_dV = (P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)));
     const T v_di_s_dV = (s_d*s_f*P[3]);
-    const T v_di_x1_dV = ((T(0.0017169779107590322)*s_x1) - ((T(7.891102846131407e-05)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)))));
+    const T v_di_x1_dV = (s_x1*(T(0.0017169779107590322) - ((T(7.891102846131407e-05)*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21))))));
     T lin_v[8], abar[8], rhs_v[8], bbar[8];
     rhs_v[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
     rhs_v[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
@@ -382,7 +382,7 @@ struct M_beeler_reuter_1977 {
     lin_v[5] = ((-(v_alpha_f)) - ((v_beta_f)));
     lin_v[6] = ((-(v_alpha_x1)) - ((v_beta_x1)));
     lin_v[3] = ((-T(0.07)) - ((T(0.01)*v_di_s_dCai)));
-    lin_v[7] = ((P[16]*v_di_K1_dV) + (P[16]*v_di_Na_dV) + (P[16]*v_di_s_dV) + (P[16]*v_di_x1_dV));
+    lin_v[7] = (P[16]*(v_di_K1_dV + v_di_Na_dV + v_di_s_dV + v_di_x1_dV));
     seed(lin_v, rhs_v, abar, bbar);
     const T a_di_x1_dV = (P[16]*abar[7]);
     const T a_di_s_dV = (P[16]*abar[7]);
@@ -392,9 +392,9 @@ struct M_beeler_reuter_1977 {
     const T a_di_s_dCai = (-(T(0.01)*abar[3]));
     const T a_dE_s_dCai = (a_di_s_dCai*P[15]*s_d*s_f);
     const T a_i_K1 = (-(P[14]*bbar[7]));
-    const T a___t30 = ((a_di_K1_dV*((T(0.016779896026542326)*v___t21) + (T(0.007)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))))) + (a_i_K1*((-T(0.014)) + (T(0.4194974006635582)*v___t21))));
+    const T a___t30 = ((a_di_K1_dV*((T(0.016779896026542326)*v___t21) + (T(0.007)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))*(v___t21*((-T(0.3332454995075077)) - ((T(5.552628147100417)*v___t21))))))) + (a_i_K1*((-T(0.014)) + (T(0.4194974006635582)*v___t21))));
     const T a___t29 = ((a_di_K1_dV*(T(0.0007000000000000001) - ((T(0.0005600000000000001)*v___t28*v___t29*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V)))))) + (a_i_K1*(T(0.016100000000000003) + (T(0.0007000000000000001)*s_V))));
-    const T a___t28 = ((a___t29*(v___t29*v___t29)) - ((T(0.00028000000000000003)*a_di_K1_dV*v_dV_eff_1_dV*(v___t29*v___t29)*(T(4.6000000000000005) + (T(0.2)*s_V)))));
+    const T a___t28 = (v___t29*(v___t29*(a___t29 - ((T(0.00028000000000000003)*a_di_K1_dV*v_dV_eff_1_dV*(T(4.6000000000000005) + (T(0.2)*s_V)))))));
     const T a_V_eff_1 = (-(T(0.04)*a___t28*v___t28));
     const T a_beta_x1 = ((-(abar[6])) - ((bbar[6]*s_x1)));
     const T a___t27 = (T(0.0003916464405623223)*a_beta_x1*v___t26);
@@ -404,8 +404,8 @@ struct M_beeler_reuter_1977 {
     const T a___t24 = (T(0.031158410986342627)*a_alpha_x1*v___t25);
     const T a___t23 = (-(T(17.41170806332765)*a___t25*(v___t25*v___t25)));
     const T a_i_x1 = (-(P[14]*bbar[7]));
-    const T a___t22 = ((-(T(0.4493289641172216)*a___t27*(v___t27*v___t27))) + (T(0.0019727757115328517)*a_i_x1*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21))) - ((T(7.891102846131407e-05)*a_di_x1_dV*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)))));
-    const T a___t21 = ((a_di_K1_dV*((T(0.016779896026542326)*v___t30) + (T(0.4194974006635582)*(v___t30*v___t30)*((-(T(0.3332454995075077)*v___t21)) - ((T(5.552628147100417)*(v___t21*v___t21))))) + (T(0.0035)*(v___t30*v___t30)*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-T(0.3332454995075077)) - ((T(11.105256294200833)*v___t21)))))) + (T(0.4194974006635582)*a_i_K1*v___t30) - ((a___t30*(v___t30*v___t30)*(T(8.331137487687693) + (T(138.8157036775104)*v___t21)))) + (T(0.042924447768975804)*a_i_x1*v___t22*s_x1) - ((T(0.001716977910759032)*a_di_x1_dV*v___t22*s_x1)));
+    const T a___t22 = ((s_x1*(((-T(1.0)) + (T(21.75840239619708)*v___t21))*((T(0.0019727757115328517)*a_i_x1) - ((T(7.891102846131407e-05)*a_di_x1_dV))))) - ((T(0.4493289641172216)*a___t27*(v___t27*v___t27))));
+    const T a___t21 = ((s_x1*(v___t22*((T(0.042924447768975804)*a_i_x1) - ((T(0.001716977910759032)*a_di_x1_dV))))) + ((v___t30*((T(0.4194974006635582)*a_i_K1) - ((a___t30*v___t30*(T(8.331137487687693) + (T(138.8157036775104)*v___t21)))))) + (a_di_K1_dV*(v___t30*((v___t30*((T(0.0035)*((-T(4.0)) + (T(119.85640018958804)*v___t21))*((-T(0.3332454995075077)) - ((T(11.105256294200833)*v___t21)))) + (T(0.4194974006635582)*v___t21*((-T(0.3332454995075077)) - ((T(5.552628147100417)*v___t21)))))) + T(0.016779896026542326))))));
     const T a_beta_f = ((-(abar[5])) - ((bbar[5]*s_f)));
     const T a___t20 = (T(0.0035672756346111717)*a_beta_f*(v___t12*v___t12));
     const T a_alpha_f = ((-(abar[5])) + (bbar[5]*(T(1.0) - ((s_f)))));
@@ -428,7 +428,7 @@ struct M_beeler_reuter_1977 {
     const T a___t8 = (T(0.3)*a_beta_j);
     const T a_alpha_j = ((-(abar[2])) + (bbar[2]*(T(1.0) - ((s_j)))));
     const T a___t7 = (T(1.8690473007222892e-10)*a_alpha_j*v___t3);
-    const T a___t6 = ((-(T(0.040762203978366204)*a___t8*(v___t8*v___t8))) - ((T(3.3576550599913205e-07)*a___t7*v___t6*(v___t7*v___t7))) - ((T(0.004957504353332717)*a___t20*v___t6*(v___t20*v___t20))));
+    const T a___t6 = ((v___t6*((-(T(3.3576550599913205e-07)*a___t7*(v___t7*v___t7))) - ((T(0.004957504353332717)*a___t20*(v___t20*v___t20))))) - ((T(0.040762203978366204)*a___t8*(v___t8*v___t8))));
     const T a_beta_h = ((-(abar[1])) - ((bbar[1]*s_h)));
     const T a___t5 = (T(1.7)*a_beta_h);
     const T a___t4 = (-(T(0.1580253208896478)*a___t5*(v___t5*v___t5)));
@@ -441,14 +441,14 @@ struct M_beeler_reuter_1977 {
     const T a___t0 = (-(a___t1*(v___t1*v___t1)));
     const T a_V_eff_0 = (-(T(0.1)*a___t0*v___t0));
     const T a_i_Na = (-(P[14]*bbar[7]));
-    ybar[0] = ((bbar[0]*((-(v_alpha_m)) - ((v_beta_m)))) + (T(3.0)*a_di_Na_dV*P[1]*s_h*s_j*(s_m*s_m)) + (T(3.0)*a_i_Na*P[1]*s_h*s_j*(s_m*s_m)*(s_V + P[10])));
-    ybar[1] = ((bbar[1]*((-(v_alpha_h)) - ((v_beta_h)))) + (a_di_Na_dV*P[1]*s_j*(s_m*s_m*s_m)) + (a_i_Na*P[1]*s_j*(s_m*s_m*s_m)*(s_V + P[10])));
-    ybar[2] = ((bbar[2]*((-(v_alpha_j)) - ((v_beta_j)))) + (a_di_Na_dV*P[1]*s_h*(s_m*s_m*s_m)) + (a_i_Na*P[1]*s_h*(s_m*s_m*s_m)*(s_V + P[10])));
-    ybar[3] = ((-(T(0.07)*bbar[3])) - ((a___t10*(v___t10*v___t10))) + (T(1.0)*a___t9*v___t10));
-    ybar[4] = ((bbar[4]*((-(v_alpha_d)) - ((v_beta_d)))) + (a_di_s_dV*s_f*P[3]) + (a_di_s_dCai*P[15]*v_dE_s_dCai*s_f) + (a_i_s*s_f*P[3]*(s_V - ((v_E_s)))));
-    ybar[5] = ((bbar[5]*((-(v_alpha_f)) - ((v_beta_f)))) + (a_di_s_dV*s_d*P[3]) + (a_di_s_dCai*P[15]*s_d*v_dE_s_dCai) + (a_i_s*s_d*P[3]*(s_V - ((v_E_s)))));
+    ybar[0] = ((s_m*(s_m*(s_j*(s_h*(P[1]*(T(3.0)*(a_di_Na_dV + (a_i_Na*(s_V + P[10]))))))))) + (bbar[0]*((-(v_alpha_m)) - ((v_beta_m)))));
+    ybar[1] = ((s_m*(s_m*(s_m*(s_j*(P[1]*(a_di_Na_dV + (a_i_Na*(s_V + P[10])))))))) + (bbar[1]*((-(v_alpha_h)) - ((v_beta_h)))));
+    ybar[2] = ((s_m*(s_m*(s_m*(s_h*(P[1]*(a_di_Na_dV + (a_i_Na*(s_V + P[10])))))))) + (bbar[2]*((-(v_alpha_j)) - ((v_beta_j)))));
+    ybar[3] = ((v___t10*((T(1.0)*a___t9) - ((a___t10*v___t10)))) - ((T(0.07)*bbar[3])));
+    ybar[4] = ((s_f*((P[3]*(a_di_s_dV + (a_i_s*(s_V - ((v_E_s)))))) + (a_di_s_dCai*P[15]*v_dE_s_dCai))) + (bbar[4]*((-(v_alpha_d)) - ((v_beta_d)))));
+    ybar[5] = ((s_d*((P[3]*(a_di_s_dV + (a_i_s*(s_V - ((v_E_s)))))) + (a_di_s_dCai*P[15]*v_dE_s_dCai))) + (bbar[5]*((-(v_alpha_f)) - ((v_beta_f)))));
     ybar[6] = ((a_di_x1_dV*(T(0.0017169779107590322) - ((T(7.891102846131407e-05)*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21)))))) + (bbar[6]*((-(v_alpha_x1)) - ((v_beta_x1)))) + (T(0.0019727757115328517)*a_i_x1*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21))));
-    ybar[7] = ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) + (T(0.0007000000000000001)*a_i_K1*v___t29) + (T(0.08264462809917356)*a___t24*v___t24) + (T(0.05)*a___t14*v___t14) + (T(0.14992503748125938)*a___t17*v___t17) + (T(0.04)*a___t21*v___t21) + (T(0.05714285714285714)*a___t23*v___t23) - ((T(0.25)*a___t3*v___t3)) - ((T(0.008)*a___t18*v___t18)) - ((T(0.07199424046076314)*a___t11*v___t11)) - ((T(0.1)*a___t6*v___t6)) - ((T(0.01694915254237288)*a___t15*v___t15)) - ((T(0.01)*a___t12*v___t12)) - ((T(0.04)*a___t22*v___t22)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t26*v___t26)) + (a_i_s*s_d*s_f*P[3]) - ((T(5.6000000000000006e-05)*a_di_K1_dV*v___t28*v_dV_eff_1_dV*(v___t29*v___t29))));
+    ybar[7] = ((v___t29*((T(0.0007000000000000001)*a_i_K1) - ((T(5.6000000000000006e-05)*a_di_K1_dV*v___t28*v___t29*v_dV_eff_1_dV)))) + ((T(0.04)*((a___t21*v___t21) - ((a___t22*v___t22)))) + ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) + (T(0.08264462809917356)*a___t24*v___t24) + (T(0.05)*a___t14*v___t14) + (T(0.14992503748125938)*a___t17*v___t17) + (T(0.05714285714285714)*a___t23*v___t23) - ((T(0.25)*a___t3*v___t3)) - ((T(0.008)*a___t18*v___t18)) - ((T(0.07199424046076314)*a___t11*v___t11)) - ((T(0.1)*a___t6*v___t6)) - ((T(0.01694915254237288)*a___t15*v___t15)) - ((T(0.01)*a___t12*v___t12)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t26*v___t26)) + (a_i_s*s_d*s_f*P[3]))));
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
   }
 
@@ -515,8 +515,8 @@ struct M_beeler_reuter_1977 {
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
     const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
-    const T v___t30 = (T(1.0)/((T(8.331137487687693)*v___t21) + (T(69.4078518387552)*(v___t21*v___t21))));
-    const T v_i_K1 = ((T(0.0035)*v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (T(0.0035)*v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21))));
+    const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
+    const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
     const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
     T f_v[8], bbar[8];
     f_v[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
@@ -542,7 +542,7 @@ struct M_beeler_reuter_1977 {
     const T a___t23 = (-(T(17.41170806332765)*a___t25*(v___t25*v___t25)));
     const T a_i_x1 = (-(P[14]*bbar[7]));
     const T a___t22 = ((-(T(0.4493289641172216)*a___t27*(v___t27*v___t27))) + (T(0.0019727757115328517)*a_i_x1*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21))));
-    const T a___t21 = ((T(0.4194974006635582)*a_i_K1*v___t30) - ((a___t30*(v___t30*v___t30)*(T(8.331137487687693) + (T(138.8157036775104)*v___t21)))) + (T(0.042924447768975804)*a_i_x1*v___t22*s_x1));
+    const T a___t21 = ((v___t30*((T(0.4194974006635582)*a_i_K1) - ((a___t30*v___t30*(T(8.331137487687693) + (T(138.8157036775104)*v___t21)))))) + (T(0.042924447768975804)*a_i_x1*v___t22*s_x1));
     const T a_beta_f = (-(bbar[5]*s_f));
     const T a___t20 = (T(0.0035672756346111717)*a_beta_f*(v___t12*v___t12));
     const T a_alpha_f = (bbar[5]*(T(1.0) - ((s_f))));
@@ -564,7 +564,7 @@ struct M_beeler_reuter_1977 {
     const T a___t8 = (T(0.3)*a_beta_j);
     const T a_alpha_j = (bbar[2]*(T(1.0) - ((s_j))));
     const T a___t7 = (T(1.8690473007222892e-10)*a_alpha_j*v___t3);
-    const T a___t6 = ((-(T(0.040762203978366204)*a___t8*(v___t8*v___t8))) - ((T(3.3576550599913205e-07)*a___t7*v___t6*(v___t7*v___t7))) - ((T(0.004957504353332717)*a___t20*v___t6*(v___t20*v___t20))));
+    const T a___t6 = ((v___t6*((-(T(3.3576550599913205e-07)*a___t7*(v___t7*v___t7))) - ((T(0.004957504353332717)*a___t20*(v___t20*v___t20))))) - ((T(0.040762203978366204)*a___t8*(v___t8*v___t8))));
     const T a_beta_h = (-(bbar[1]*s_h));
     const T a___t5 = (T(1.7)*a_beta_h);
     const T a___t4 = (-(T(0.1580253208896478)*a___t5*(v___t5*v___t5)));
@@ -584,7 +584,7 @@ struct M_beeler_reuter_1977 {
     ybar[4] = ((bbar[4]*((-(v_alpha_d)) - ((v_beta_d)))) + (a_i_s*s_f*P[3]*(s_V - ((v_E_s)))));
     ybar[5] = ((bbar[5]*((-(v_alpha_f)) - ((v_beta_f)))) + (a_i_s*s_d*P[3]*(s_V - ((v_E_s)))));
     ybar[6] = ((bbar[6]*((-(v_alpha_x1)) - ((v_beta_x1)))) + (T(0.0019727757115328517)*a_i_x1*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21))));
-    ybar[7] = ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) + (T(0.0007000000000000001)*a_i_K1*v___t29) + (T(0.08264462809917356)*a___t24*v___t24) + (T(0.05)*a___t14*v___t14) + (T(0.14992503748125938)*a___t17*v___t17) + (T(0.04)*a___t21*v___t21) + (T(0.05714285714285714)*a___t23*v___t23) - ((T(0.25)*a___t3*v___t3)) - ((T(0.008)*a___t18*v___t18)) - ((T(0.07199424046076314)*a___t11*v___t11)) - ((T(0.1)*a___t6*v___t6)) - ((T(0.01694915254237288)*a___t15*v___t15)) - ((T(0.01)*a___t12*v___t12)) - ((T(0.04)*a___t22*v___t22)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t26*v___t26)) + (a_i_s*s_d*s_f*P[3]));
+    ybar[7] = ((T(0.04)*((a___t21*v___t21) - ((a___t22*v___t22)))) + ((a_V_eff_0*((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_V_eff_1*((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.0) : T(1.0))) + (a_i_Na*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m)))) - ((a_alpha_m*v___t1)) + (T(0.0007000000000000001)*a_i_K1*v___t29) + (T(0.08264462809917356)*a___t24*v___t24) + (T(0.05)*a___t14*v___t14) + (T(0.14992503748125938)*a___t17*v___t17) + (T(0.05714285714285714)*a___t23*v___t23) - ((T(0.25)*a___t3*v___t3)) - ((T(0.008)*a___t18*v___t18)) - ((T(0.07199424046076314)*a___t11*v___t11)) - ((T(0.1)*a___t6*v___t6)) - ((T(0.01694915254237288)*a___t15*v___t15)) - ((T(0.01)*a___t12*v___t12)) - ((T(0.082)*a___t4*v___t4)) - ((T(0.056)*a___t2*v___t2)) - ((T(0.05998800239952009)*a___t26*v___t26)) + (a_i_s*s_d*s_f*P[3])));
     (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;
   }
 };

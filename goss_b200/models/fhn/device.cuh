@@ -68,9 +68,9 @@ struct M_fhn {
   {
     const T s_v = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(P[11] + s_v)) + (P[14]*(P[11] + s_v)*(P[13] + s_v)*(P[9] - ((s_v)))));
+    const T v_I = ((P[11] + s_v)*((P[12]*s_s) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v))))));
     const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-    const T v_dI_dv = ((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) + (P[19]*(P[11] + s_v)*(P[13] + s_v)));
+    const T v_dI_dv = ((P[14]*((P[9] - ((s_v)))*(P[11] + P[13] + (T(2.0)*s_v)))) + ((P[12]*s_s) + (P[19]*(P[11] + s_v)*(P[13] + s_v))));
     rhs[0] = (v_I + T(v_i_Stim));
     rhs[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
     linear[1] = P[18];
@@ -84,7 +84,7 @@ struct M_fhn {
   {
     const T s_v = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(P[11] + s_v)) + (P[14]*(P[11] + s_v)*(P[13] + s_v)*(P[9] - ((s_v)))));
+    const T v_I = ((P[11] + s_v)*((P[12]*s_s) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v))))));
     const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     values[0] = (v_I + T(v_i_Stim));
     values[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
@@ -100,9 +100,9 @@ struct M_fhn {
   {
     const T s_v = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(P[11] + s_v)) + (P[14]*(P[11] + s_v)*(P[13] + s_v)*(P[9] - ((s_v)))));
+    const T v_I = ((P[11] + s_v)*((P[12]*s_s) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v))))));
     const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-    const T v_dI_dv = ((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) + (P[19]*(P[11] + s_v)*(P[13] + s_v)));
+    const T v_dI_dv = ((P[14]*((P[9] - ((s_v)))*(P[11] + P[13] + (T(2.0)*s_v)))) + ((P[12]*s_s) + (P[19]*(P[11] + s_v)*(P[13] + s_v))));
     T lin_v[2], abar[2], rhs_v[2], bbar[2];
     rhs_v[0] = (v_I + T(v_i_Stim));
     rhs_v[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
@@ -111,8 +111,8 @@ struct M_fhn {
     seed(lin_v, rhs_v, abar, bbar);
     const T a_dI_dv = abar[0];
     const T a_I = bbar[0];
-    ybar[0] = ((a_I*((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) - ((P[14]*(P[11] + s_v)*(P[13] + s_v))))) + (a_dI_dv*((P[19]*(P[11] + s_v)) + (P[19]*(P[13] + s_v)) - ((P[14]*(P[11] + s_v))) - ((P[14]*(P[13] + s_v))) + (T(2.0)*P[14]*(P[9] - ((s_v)))))) + (bbar[1]*P[1]));
-    ybar[1] = ((a_dI_dv*P[12]) + (a_I*P[12]*(P[11] + s_v)) + (P[17]*bbar[1]*P[1]));
+    ybar[0] = ((a_I*((P[14]*(((P[13] + s_v)*(P[9] - ((P[11])) - ((T(2.0)*s_v)))) + ((P[11] + s_v)*(P[9] - ((s_v)))))) + (P[12]*s_s))) + (a_dI_dv*((P[14]*((-(P[11])) - ((P[13])) - ((T(2.0)*s_v)) + (T(2.0)*(P[9] - ((s_v)))))) + (P[19]*(P[11] + P[13] + (T(2.0)*s_v))))) + (bbar[1]*P[1]));
+    ybar[1] = ((P[12]*(a_dI_dv + (a_I*(P[11] + s_v)))) + (P[17]*bbar[1]*P[1]));
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
   }
 
@@ -125,14 +125,14 @@ struct M_fhn {
   {
     const T s_v = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(P[11] + s_v)) + (P[14]*(P[11] + s_v)*(P[13] + s_v)*(P[9] - ((s_v)))));
+    const T v_I = ((P[11] + s_v)*((P[12]*s_s) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v))))));
     const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     T f_v[2], bbar[2];
     f_v[0] = (v_I + T(v_i_Stim));
     f_v[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
     seed(f_v, bbar);
     const T a_I = bbar[0];
-    ybar[0] = ((a_I*((P[12]*s_s) + (P[14]*(P[11] + s_v)*(P[9] - ((s_v)))) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v)))) - ((P[14]*(P[11] + s_v)*(P[13] + s_v))))) + (bbar[1]*P[1]));
+    ybar[0] = ((a_I*((P[14]*(((P[13] + s_v)*(P[9] - ((P[11])) - ((T(2.0)*s_v)))) + ((P[11] + s_v)*(P[9] - ((s_v)))))) + (P[12]*s_s))) + (bbar[1]*P[1]));
     ybar[1] = ((a_I*P[12]*(P[11] + s_v)) + (P[17]*bbar[1]*P[1]));
     (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;
   }

@@ -69,9 +69,9 @@ struct M_fitzhughnagumo__5dc98ee0 {
     const T s_V = y[0];
     const T s_s = y[1];
     const T v_V_th = (P[1] + (P[11]*F[0]));
-    const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[12])*((P[13]*s_s) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-    const T v_dI_dV = ((P[13]*s_s) + (P[14]*(s_V + P[12])*(P[0] - ((s_V)))) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))) + (P[18]*(s_V + P[12])*(s_V - ((v_V_th)))));
+    const T v_dI_dV = ((P[14]*((P[0] - ((s_V)))*(P[12] - ((v_V_th)) + (T(2.0)*s_V)))) + ((P[13]*s_s) + (P[18]*(s_V + P[12])*(s_V - ((v_V_th))))));
     rhs[0] = (v_I + T(v_i_Stim));
     rhs[1] = (F[1]*(s_V + P[12] + (P[17]*s_s)));
     linear[1] = (P[17]*F[1]);
@@ -86,7 +86,7 @@ struct M_fitzhughnagumo__5dc98ee0 {
     const T s_V = y[0];
     const T s_s = y[1];
     const T v_V_th = (P[1] + (P[11]*F[0]));
-    const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[12])*((P[13]*s_s) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     values[0] = (v_I + T(v_i_Stim));
     values[1] = (F[1]*(s_V + P[12] + (P[17]*s_s)));
@@ -103,9 +103,9 @@ struct M_fitzhughnagumo__5dc98ee0 {
     const T s_V = y[0];
     const T s_s = y[1];
     const T v_V_th = (P[1] + (P[11]*F[0]));
-    const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[12])*((P[13]*s_s) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-    const T v_dI_dV = ((P[13]*s_s) + (P[14]*(s_V + P[12])*(P[0] - ((s_V)))) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))) + (P[18]*(s_V + P[12])*(s_V - ((v_V_th)))));
+    const T v_dI_dV = ((P[14]*((P[0] - ((s_V)))*(P[12] - ((v_V_th)) + (T(2.0)*s_V)))) + ((P[13]*s_s) + (P[18]*(s_V + P[12])*(s_V - ((v_V_th))))));
     T lin_v[2], abar[2], rhs_v[2], bbar[2];
     rhs_v[0] = (v_I + T(v_i_Stim));
     rhs_v[1] = (F[1]*(s_V + P[12] + (P[17]*s_s)));
@@ -115,8 +115,8 @@ struct M_fitzhughnagumo__5dc98ee0 {
     const T a_dI_dV = abar[0];
     const T a_I = bbar[0];
     const T a_V_th = ((a_dI_dV*((-(P[14]*(P[0] - ((s_V))))) - ((P[18]*(s_V + P[12]))))) - ((a_I*P[14]*(s_V + P[12])*(P[0] - ((s_V))))));
-    ybar[0] = ((a_I*((P[13]*s_s) + (P[14]*(s_V + P[12])*(P[0] - ((s_V)))) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))) - ((P[14]*(s_V + P[12])*(s_V - ((v_V_th))))))) + (a_dI_dV*((P[18]*(s_V + P[12])) + (P[18]*(s_V - ((v_V_th)))) - ((P[14]*(s_V + P[12]))) - ((P[14]*(s_V - ((v_V_th))))) + (T(2.0)*P[14]*(P[0] - ((s_V)))))) + (bbar[1]*F[1]));
-    ybar[1] = ((a_dI_dV*P[13]) + (a_I*P[13]*(s_V + P[12])) + (P[17]*bbar[1]*F[1]));
+    ybar[0] = ((a_I*((P[14]*(((s_V - ((v_V_th)))*(P[0] - ((P[12])) - ((T(2.0)*s_V)))) + ((s_V + P[12])*(P[0] - ((s_V)))))) + (P[13]*s_s))) + (a_dI_dV*((P[14]*(v_V_th - ((P[12])) - ((T(2.0)*s_V)) + (T(2.0)*(P[0] - ((s_V)))))) + (P[18]*(P[12] - ((v_V_th)) + (T(2.0)*s_V))))) + (bbar[1]*F[1]));
+    ybar[1] = ((P[13]*(a_dI_dV + (a_I*(s_V + P[12])))) + (P[17]*bbar[1]*F[1]));
     Fbar[0] = (a_V_th*P[11]);
     Fbar[1] = ((P[17]*abar[1]) + (bbar[1]*(s_V + P[12] + (P[17]*s_s))));
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
@@ -132,7 +132,7 @@ struct M_fitzhughnagumo__5dc98ee0 {
     const T s_V = y[0];
     const T s_s = y[1];
     const T v_V_th = (P[1] + (P[11]*F[0]));
-    const T v_I = ((P[13]*s_s*(s_V + P[12])) + (P[14]*(s_V + P[12])*(s_V - ((v_V_th)))*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[12])*((P[13]*s_s) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     T f_v[2], bbar[2];
     f_v[0] = (v_I + T(v_i_Stim));
@@ -140,7 +140,7 @@ struct M_fitzhughnagumo__5dc98ee0 {
     seed(f_v, bbar);
     const T a_I = bbar[0];
     const T a_V_th = (-(a_I*P[14]*(s_V + P[12])*(P[0] - ((s_V)))));
-    ybar[0] = ((a_I*((P[13]*s_s) + (P[14]*(s_V + P[12])*(P[0] - ((s_V)))) + (P[14]*(s_V - ((v_V_th)))*(P[0] - ((s_V)))) - ((P[14]*(s_V + P[12])*(s_V - ((v_V_th))))))) + (bbar[1]*F[1]));
+    ybar[0] = ((a_I*((P[14]*(((s_V - ((v_V_th)))*(P[0] - ((P[12])) - ((T(2.0)*s_V)))) + ((s_V + P[12])*(P[0] - ((s_V)))))) + (P[13]*s_s))) + (bbar[1]*F[1]));
     ybar[1] = ((a_I*P[13]*(s_V + P[12])) + (P[17]*bbar[1]*F[1]));
     Fbar[0] = (a_V_th*P[11]);
     Fbar[1] = (bbar[1]*(s_V + P[12] + (P[17]*s_s)));

@@ -70,9 +70,9 @@ struct M_fitzhughnagumo__8321f5ac {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-    const T v_dI_dV = ((P[12]*s_s) + (P[14]*(s_V + P[11])*(P[0] - ((s_V)))) + (P[14]*(s_V + P[13])*(P[0] - ((s_V)))) + (P[19]*(s_V + P[11])*(s_V + P[13])));
+    const T v_dI_dV = ((P[14]*((P[0] - ((s_V)))*(P[11] + P[13] + (T(2.0)*s_V)))) + ((P[12]*s_s) + (P[19]*(s_V + P[11])*(s_V + P[13]))));
     rhs[0] = (v_I + T(v_i_Stim));
     rhs[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
     linear[1] = P[18];
@@ -86,7 +86,7 @@ struct M_fitzhughnagumo__8321f5ac {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     values[0] = (v_I + T(v_i_Stim));
     values[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
@@ -102,9 +102,9 @@ struct M_fitzhughnagumo__8321f5ac {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-    const T v_dI_dV = ((P[12]*s_s) + (P[14]*(s_V + P[11])*(P[0] - ((s_V)))) + (P[14]*(s_V + P[13])*(P[0] - ((s_V)))) + (P[19]*(s_V + P[11])*(s_V + P[13])));
+    const T v_dI_dV = ((P[14]*((P[0] - ((s_V)))*(P[11] + P[13] + (T(2.0)*s_V)))) + ((P[12]*s_s) + (P[19]*(s_V + P[11])*(s_V + P[13]))));
     T lin_v[2], abar[2], rhs_v[2], bbar[2];
     rhs_v[0] = (v_I + T(v_i_Stim));
     rhs_v[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
@@ -113,8 +113,8 @@ struct M_fitzhughnagumo__8321f5ac {
     seed(lin_v, rhs_v, abar, bbar);
     const T a_dI_dV = abar[0];
     const T a_I = bbar[0];
-    ybar[0] = ((a_I*((P[12]*s_s) + (P[14]*(s_V + P[11])*(P[0] - ((s_V)))) + (P[14]*(s_V + P[13])*(P[0] - ((s_V)))) - ((P[14]*(s_V + P[11])*(s_V + P[13]))))) + (a_dI_dV*((P[19]*(s_V + P[11])) + (P[19]*(s_V + P[13])) - ((P[14]*(s_V + P[11]))) - ((P[14]*(s_V + P[13]))) + (T(2.0)*P[14]*(P[0] - ((s_V)))))) + (bbar[1]*P[3]));
-    ybar[1] = ((a_dI_dV*P[12]) + (a_I*P[12]*(s_V + P[11])) + (P[17]*bbar[1]*P[3]));
+    ybar[0] = ((a_I*((P[14]*(((s_V + P[13])*(P[0] - ((P[11])) - ((T(2.0)*s_V)))) + ((s_V + P[11])*(P[0] - ((s_V)))))) + (P[12]*s_s))) + (a_dI_dV*((P[14]*((-(P[11])) - ((P[13])) - ((T(2.0)*s_V)) + (T(2.0)*(P[0] - ((s_V)))))) + (P[19]*(P[11] + P[13] + (T(2.0)*s_V))))) + (bbar[1]*P[3]));
+    ybar[1] = ((P[12]*(a_dI_dV + (a_I*(s_V + P[11])))) + (P[17]*bbar[1]*P[3]));
     (void)time; (void)P; (void)PD; (void)F; (void)abar; (void)bbar; (void)Fbar;
   }
 
@@ -127,14 +127,14 @@ struct M_fitzhughnagumo__8321f5ac {
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    const T v_I = ((P[12]*s_s*(s_V + P[11])) + (P[14]*(s_V + P[11])*(s_V + P[13])*(P[0] - ((s_V)))));
+    const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
     const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
     T f_v[2], bbar[2];
     f_v[0] = (v_I + T(v_i_Stim));
     f_v[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
     seed(f_v, bbar);
     const T a_I = bbar[0];
-    ybar[0] = ((a_I*((P[12]*s_s) + (P[14]*(s_V + P[11])*(P[0] - ((s_V)))) + (P[14]*(s_V + P[13])*(P[0] - ((s_V)))) - ((P[14]*(s_V + P[11])*(s_V + P[13]))))) + (bbar[1]*P[3]));
+    ybar[0] = ((a_I*((P[14]*(((s_V + P[13])*(P[0] - ((P[11])) - ((T(2.0)*s_V)))) + ((s_V + P[11])*(P[0] - ((s_V)))))) + (P[12]*s_s))) + (bbar[1]*P[3]));
     ybar[1] = ((a_I*P[12]*(s_V + P[11])) + (P[17]*bbar[1]*P[3]));
     (void)time; (void)P; (void)PD; (void)F; (void)bbar; (void)Fbar;
   }
