@@ -134,12 +134,12 @@ __device__ __forceinline__ float grl_increment(float a, float b, float h, float 
 
 // State accumulators.  FP64 kernels hold each state as a double and update it
 // exactly as the reference does (y = y + increment).  FP32 kernels hold each
-// state as an unevaluated sum hi + lo of two floats ("double-float"): the
-// model reads hi, increments are added with an error-free two-sum and the
-// pair is renormalised, which keeps ~48 significant bits (concentrations such
-// as K_i ~ 138 mM change by less than one float ulp per step) without the
-// FP32<->FP64 conversions that would otherwise compete with the model's
-// exponentials and reciprocals for the MUFU/XU pipe on every step.
+// state as an unevaluated sum hi + lo of two floats with compensated (Kahan)
+// updates: the model reads hi, lo carries what hi could not absorb, so
+// increments far below one float ulp of the state (K_i ~ 138 mM changes by
+// less than one ulp per step) still accumulate.  Four FP32 adds per update,
+// no FP32<->FP64 conversions (those would compete with the model's
+// exponentials and reciprocals for the XU pipe on every step).
 template <typename T>
 struct Acc;
 
@@ -166,14 +166,12 @@ struct Acc<float> {
     __device__ __forceinline__ float plus(float d) const { return hi + (lo + d); }
     __device__ __forceinline__ void add(float d)
     {
-        // two-sum: s + err == hi + d exactly
-        const float s = __fadd_rn(hi, d);
-        const float bb = __fadd_rn(s, -hi);
-        const float err = __fadd_rn(__fadd_rn(hi, -__fadd_rn(s, -bb)), __fadd_rn(d, -bb));
-        const float l = __fadd_rn(lo, err);
-        // renormalise (|s| >= |l|): hi + lo == s + l
-        hi = __fadd_rn(s, l);
-        lo = __fadd_rn(l, -__fadd_rn(hi, -s));
+        // hi + lo + d: the sum goes to hi, its rounding error (exact when
+        // |hi| >= |y|, Fast2Sum) back to lo
+        const float y = __fadd_rn(d, lo);
+        const float t = __fadd_rn(hi, y);
+        lo = __fsub_rn(y, __fsub_rn(t, hi));
+        hi = t;
     }
 };
 
