@@ -397,11 +397,21 @@ __device__ __forceinline__ double l2norm(const double* v)
     return sqrt(s);
 }
 
-// FP64 model right-hand side with the per-node parameter block
+// FP64 model right-hand side of the implicit solvers: the split form (every
+// distinct exp and reciprocal once, common factors pulled out), whose values
+// differ from the reference's operation order by rounding only; Newton
+// iterates to the same states (the implicit parity tests hold at 1e-10), and
+// the FD Jacobian, ~19 evaluations per Newton iteration, gets ~2x cheaper.
+#ifndef GOSS_IMPLICIT_SPLIT
+#define GOSS_IMPLICIT_SPLIT 1
+#endif
 template <class M>
 __device__ __forceinline__ void rhs64(const double* y, double t, const double* P, const double* F, double* out)
 {
-    M::template rhs<double>(y, t, P, P, F, out);
+    if constexpr (GOSS_IMPLICIT_SPLIT)
+        M::template rhs_split<double>(y, t, P, P, F, out);
+    else
+        M::template rhs<double>(y, t, P, P, F, out);
 }
 
 // ODE::compute_jacobian (ODE.cpp:47-67) into any matrix accessor: column i is
