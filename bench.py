@@ -50,14 +50,36 @@ def _args():
     ap.add_argument("--impl", default="goss_b200", choices=["goss_b200", "reference"])
     ap.add_argument("--nodes", type=int, default=N_NODES)
     ap.add_argument("--skip-fp64", action="store_true", help=argparse.SUPPRESS)
-    ap.add_argument("--profile", choices=["single", "double"], default=None,
-                    help="only run the timed forward loop in one precision (for ncu captures)")
+    ap.add_argument("--profile", choices=["single", "double", "adjoint-single", "adjoint-double"], default=None,
+                    help="only run the timed forward loop in one precision, or one adjoint gradient "
+                         "(65,536 nodes x 2,000 steps), for ncu captures")
     return ap.parse_args()
 
 
 def profile_run(args):
-    """Minimal run for profiler captures: W+K forward calls of one precision."""
+    """Minimal run for profiler captures: W+K forward calls of one precision,
+    or one record + backward pass of the adjoint workload shortened to 20 ms."""
     import goss_b200 as goss
+
+    if args.profile.startswith("adjoint"):
+        import torch
+        from goss_b200.adjoint import GRL1Trace
+
+        precision = args.profile.split("-")[1]
+        nodes = 65_536
+        ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS)
+        defaults = np.array([ode.get_parameter(p) for p in FIELDS])
+        rng = np.random.default_rng(SEED + 1)
+        fp = torch.tensor(defaults[None, :] * np.exp(0.2 * rng.standard_normal((nodes, 4))), device="cuda")
+        y0 = torch.tensor(ode.get_ic()[None, :] * (1 + rng.uniform(-0.02, 0.02, (nodes, ode.num_states))),
+                          device="cuda")
+        tr = GRL1Trace(ode, nodes, 1.0, 100, 20, 100, precision=precision)
+        v = tr.run_forward(fp, y0)
+        g, _ = tr.run_backward(2 * v)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "nodes": nodes, "steps": 2000,
+                          "finite": bool(torch.isfinite(g).all())}))
+        return
 
     md, y0, fp = inputs(args.nodes)
     ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS)
