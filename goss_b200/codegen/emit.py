@@ -323,8 +323,10 @@ class ModelSource:
     # =======================================================================
     # CUDA device code
     # =======================================================================
-    def _dev_printers(self):
-        """Printers for arithmetic type T and for double (time-only) context."""
+    def _dev_printers(self, split: bool = False):
+        """Printers for arithmetic type T and for double (time-only) context;
+        ``split``: the T printer of the split forms, whose exponentials with a
+        numeric coefficient go through exp2 (one multiply fewer)."""
         def make(ctx_double: bool):
             def sym(s):
                 n = s.name
@@ -360,11 +362,11 @@ class ModelSource:
                           pow="pow", fmax="fmax", fmin="fmin")
                 lit = c_double
             else:
-                fn = dict(exp="gexp", log="glog", sqrt="gsqrt", fabs="gfabs", floor="gfloor", ceil="gceil",
-                          pow="gpow", fmax="gfmax", fmin="gfmin", sin="gsin", cos="gcos", tan="gtan",
+                fn = dict(exp="gexp", exp2="gexp2", log="glog", sqrt="gsqrt", fabs="gfabs", floor="gfloor",
+                          ceil="gceil", pow="gpow", fmax="gfmax", fmin="gfmin", sin="gsin", cos="gcos", tan="gtan",
                           tanh="gtanh")
                 lit = lambda v: f"T({c_double(v)})"
-            return CPrinter(sym, fn=fn, lit=lit)
+            return CPrinter(sym, fn=fn, lit=lit, exp2_fold=split and not ctx_double)
         return make(False), make(True)
 
     def _cls_of(self, name: str) -> int:
@@ -426,7 +428,7 @@ class ModelSource:
         inter = {n: self.model.sym(n) for n in self.model.intermediates}
         rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
                             [self.model.sym(p) for p in self.fparams], inter)
-        prT, prD = self._dev_printers()
+        prT, prD = self._dev_printers(split=True)
         lines = []
         for b in rp.forward:
             if b.cls == TIME_CLS:
@@ -461,7 +463,7 @@ class ModelSource:
         inter = {n: self.model.sym(n) for n in self.model.intermediates}
         rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
                             [self.model.sym(p) for p in self.fparams], inter, reverse=False)
-        prT, prD = self._dev_printers()
+        prT, prD = self._dev_printers(split=True)
         lines = []
         for b in rp.forward:
             if b.cls == TIME_CLS:

@@ -21,6 +21,9 @@ from typing import Callable, Dict, Optional
 import sympy as sp
 
 
+_LOG2E = 1.4426950408889634  # log2(e)
+
+
 def c_double(v: float) -> str:
     r = repr(float(v))
     if r in ("inf", "-inf", "nan"):
@@ -40,9 +43,12 @@ class CPrinter:
     """
 
     def __init__(self, sym: Callable[[sp.Symbol], str], fn: Optional[Dict[str, str]] = None,
-                 lit: Callable[[float], str] = c_double):
+                 lit: Callable[[float], str] = c_double, exp2_fold: bool = False):
         self.sym = sym
-        self.fn = dict(exp="exp", log="log", sqrt="sqrt", fabs="fabs", floor="floor", ceil="ceil",
+        # exp(c*x) with a numeric c printed as exp2((c*log2(e))*x): the
+        # hardware exponential is base 2, so this saves the multiply by log2(e)
+        self.exp2_fold = exp2_fold
+        self.fn = dict(exp="exp", exp2="exp2", log="log", sqrt="sqrt", fabs="fabs", floor="floor", ceil="ceil",
                        pow="pow", fmax="fmax", fmin="fmin", sin="sin", cos="cos", tan="tan", tanh="tanh")
         if fn:
             self.fn.update(fn)
@@ -86,7 +92,7 @@ class CPrinter:
         if isinstance(e, sp.Pow):
             return self._pow(e)
         if isinstance(e, sp.exp):
-            return self._f("exp", self.p(e.args[0]))
+            return self._exp(e.args[0])
         if isinstance(e, sp.log):
             if len(e.args) != 1:
                 raise ValueError("log with base is not supported")
@@ -122,6 +128,14 @@ class CPrinter:
             return f"(!{self.p(e.args[0])})"
         raise ValueError(f"cannot print {type(e).__name__}: {e}")
 
+    def _exp(self, arg) -> str:
+        if self.exp2_fold:
+            c, rest = arg.as_coeff_Mul()
+            if c.is_Number and c != 1 and rest != 1:
+                return self._f("exp2", f"{self.lit(float(c) * _LOG2E)}*{self.p(rest)}"
+                               if float(c) > 0 else f"(-{self.lit(-float(c) * _LOG2E)})*{self.p(rest)}")
+        return self._f("exp", self.p(arg))
+
     def _piecewise(self, pieces) -> str:
         (val, cond), rest = pieces[0], pieces[1:]
         if cond is sp.true or cond == True:  # noqa: E712
@@ -135,7 +149,7 @@ class CPrinter:
     def _pow(self, e: sp.Pow) -> str:
         b, x = e.base, e.exp
         if b is sp.E:
-            return self._f("exp", self.p(x))
+            return self._exp(x)
         if x.is_Integer:
             n = int(x)
             if n == 0:

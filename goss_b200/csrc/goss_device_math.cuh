@@ -15,6 +15,15 @@ namespace goss_b200 { namespace models {
 
 __device__ __forceinline__ double gexp(double x) { return exp(x); }
 __device__ __forceinline__ float gexp(float x) { return __expf(x); }
+// 2^x: the hardware exponential (ex2.approx, flush-to-zero, as __expf uses) in
+// FP32; exp2 in FP64.  The generator prints exp(c*x) as gexp2((c*log2 e)*x).
+__device__ __forceinline__ double gexp2(double x) { return exp2(x); }
+__device__ __forceinline__ float gexp2(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ double glog(double x) { return log(x); }
 __device__ __forceinline__ float glog(float x) { return __logf(x); }
 __device__ __forceinline__ double gsqrt(double x) { return sqrt(x); }

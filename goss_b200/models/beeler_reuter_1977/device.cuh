@@ -144,17 +144,17 @@ struct M_beeler_reuter_1977 {
     const T s_V = y[7];
     const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
     const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
-    const T v___t0 = gexp((-(T(0.1)*v_V_eff_0)));
+    const T v___t0 = gexp2((-T(0.14426950408889636))*v_V_eff_0);
     const T v___t1 = (T(1.0)/((-T(1.0)) + v___t0));
     const T v_alpha_m = (v___t1*((-T(47.0)) - ((s_V))));
-    const T v___t2 = gexp((-(T(0.056)*s_V)));
+    const T v___t2 = gexp2((-T(0.08079092228978195))*s_V);
     const T v_beta_m = (T(0.7095526727489909)*v___t2);
-    const T v___t3 = gexp((-(T(0.25)*s_V)));
+    const T v___t3 = gexp2((-T(0.36067376022224085))*s_V);
     const T v_alpha_h = (T(5.497962438709065e-10)*v___t3);
-    const T v___t4 = gexp((-(T(0.082)*s_V)));
+    const T v___t4 = gexp2((-T(0.118300993352895))*s_V);
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t6 = gexp2((-T(0.14426950408889636))*s_V);
     const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
     const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
@@ -163,32 +163,32 @@ struct M_beeler_reuter_1977 {
     const T v___t10 = (T(1.0)/s_Cai);
     const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t11 = gexp2((-T(0.10386573368531053))*s_V);
+    const T v___t12 = gexp2((-T(0.014426950408889635))*s_V);
     const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
     const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
-    const T v___t14 = gexp((T(0.05)*s_V));
-    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t14 = gexp2(T(0.07213475204444818)*s_V);
+    const T v___t15 = gexp2((-T(0.024452458320151922))*s_V);
     const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
     const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
-    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t17 = gexp2(T(0.21629610807930486)*s_V);
+    const T v___t18 = gexp2((-T(0.011541560327111707))*s_V);
     const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
     const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
     const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
     const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
-    const T v___t21 = gexp((T(0.04)*s_V));
-    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v___t21 = gexp2(T(0.05770780163555854)*s_V);
+    const T v___t22 = gexp2((-T(0.05770780163555854))*s_V);
     const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
-    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t23 = gexp2(T(0.08243971662222647)*s_V);
+    const T v___t24 = gexp2(T(0.11923099511479036)*s_V);
     const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
     const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
-    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t26 = gexp2((-T(0.08654439357462287))*s_V);
     const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
     const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t28 = gexp2((-T(0.05770780163555854))*v_V_eff_1);
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
     const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
     const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
@@ -233,17 +233,17 @@ struct M_beeler_reuter_1977 {
     const T s_V = y[7];
     const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
     const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
-    const T v___t0 = gexp((-(T(0.1)*v_V_eff_0)));
+    const T v___t0 = gexp2((-T(0.14426950408889636))*v_V_eff_0);
     const T v___t1 = (T(1.0)/((-T(1.0)) + v___t0));
     const T v_alpha_m = (v___t1*((-T(47.0)) - ((s_V))));
-    const T v___t2 = gexp((-(T(0.056)*s_V)));
+    const T v___t2 = gexp2((-T(0.08079092228978195))*s_V);
     const T v_beta_m = (T(0.7095526727489909)*v___t2);
-    const T v___t3 = gexp((-(T(0.25)*s_V)));
+    const T v___t3 = gexp2((-T(0.36067376022224085))*s_V);
     const T v_alpha_h = (T(5.497962438709065e-10)*v___t3);
-    const T v___t4 = gexp((-(T(0.082)*s_V)));
+    const T v___t4 = gexp2((-T(0.118300993352895))*s_V);
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t6 = gexp2((-T(0.14426950408889636))*s_V);
     const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
     const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
@@ -252,32 +252,32 @@ struct M_beeler_reuter_1977 {
     const T v___t10 = (T(1.0)/s_Cai);
     const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t11 = gexp2((-T(0.10386573368531053))*s_V);
+    const T v___t12 = gexp2((-T(0.014426950408889635))*s_V);
     const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
     const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
-    const T v___t14 = gexp((T(0.05)*s_V));
-    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t14 = gexp2(T(0.07213475204444818)*s_V);
+    const T v___t15 = gexp2((-T(0.024452458320151922))*s_V);
     const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
     const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
-    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t17 = gexp2(T(0.21629610807930486)*s_V);
+    const T v___t18 = gexp2((-T(0.011541560327111707))*s_V);
     const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
     const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
     const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
     const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
-    const T v___t21 = gexp((T(0.04)*s_V));
-    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v___t21 = gexp2(T(0.05770780163555854)*s_V);
+    const T v___t22 = gexp2((-T(0.05770780163555854))*s_V);
     const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
-    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t23 = gexp2(T(0.08243971662222647)*s_V);
+    const T v___t24 = gexp2(T(0.11923099511479036)*s_V);
     const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
     const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
-    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t26 = gexp2((-T(0.08654439357462287))*s_V);
     const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
     const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t28 = gexp2((-T(0.05770780163555854))*v_V_eff_1);
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
     const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
     const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
@@ -310,17 +310,17 @@ struct M_beeler_reuter_1977 {
     const T s_V = y[7];
     const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
     const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
-    const T v___t0 = gexp((-(T(0.1)*v_V_eff_0)));
+    const T v___t0 = gexp2((-T(0.14426950408889636))*v_V_eff_0);
     const T v___t1 = (T(1.0)/((-T(1.0)) + v___t0));
     const T v_alpha_m = (v___t1*((-T(47.0)) - ((s_V))));
-    const T v___t2 = gexp((-(T(0.056)*s_V)));
+    const T v___t2 = gexp2((-T(0.08079092228978195))*s_V);
     const T v_beta_m = (T(0.7095526727489909)*v___t2);
-    const T v___t3 = gexp((-(T(0.25)*s_V)));
+    const T v___t3 = gexp2((-T(0.36067376022224085))*s_V);
     const T v_alpha_h = (T(5.497962438709065e-10)*v___t3);
-    const T v___t4 = gexp((-(T(0.082)*s_V)));
+    const T v___t4 = gexp2((-T(0.118300993352895))*s_V);
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t6 = gexp2((-T(0.14426950408889636))*s_V);
     const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
     const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
@@ -329,32 +329,32 @@ struct M_beeler_reuter_1977 {
     const T v___t10 = (T(1.0)/s_Cai);
     const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t11 = gexp2((-T(0.10386573368531053))*s_V);
+    const T v___t12 = gexp2((-T(0.014426950408889635))*s_V);
     const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
     const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
-    const T v___t14 = gexp((T(0.05)*s_V));
-    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t14 = gexp2(T(0.07213475204444818)*s_V);
+    const T v___t15 = gexp2((-T(0.024452458320151922))*s_V);
     const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
     const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
-    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t17 = gexp2(T(0.21629610807930486)*s_V);
+    const T v___t18 = gexp2((-T(0.011541560327111707))*s_V);
     const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
     const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
     const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
     const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
-    const T v___t21 = gexp((T(0.04)*s_V));
-    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v___t21 = gexp2(T(0.05770780163555854)*s_V);
+    const T v___t22 = gexp2((-T(0.05770780163555854))*s_V);
     const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
-    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t23 = gexp2(T(0.08243971662222647)*s_V);
+    const T v___t24 = gexp2(T(0.11923099511479036)*s_V);
     const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
     const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
-    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t26 = gexp2((-T(0.08654439357462287))*s_V);
     const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
     const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t28 = gexp2((-T(0.05770780163555854))*v_V_eff_1);
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
     const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
     const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
@@ -469,17 +469,17 @@ struct M_beeler_reuter_1977 {
     const T s_V = y[7];
     const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
     const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
-    const T v___t0 = gexp((-(T(0.1)*v_V_eff_0)));
+    const T v___t0 = gexp2((-T(0.14426950408889636))*v_V_eff_0);
     const T v___t1 = (T(1.0)/((-T(1.0)) + v___t0));
     const T v_alpha_m = (v___t1*((-T(47.0)) - ((s_V))));
-    const T v___t2 = gexp((-(T(0.056)*s_V)));
+    const T v___t2 = gexp2((-T(0.08079092228978195))*s_V);
     const T v_beta_m = (T(0.7095526727489909)*v___t2);
-    const T v___t3 = gexp((-(T(0.25)*s_V)));
+    const T v___t3 = gexp2((-T(0.36067376022224085))*s_V);
     const T v_alpha_h = (T(5.497962438709065e-10)*v___t3);
-    const T v___t4 = gexp((-(T(0.082)*s_V)));
+    const T v___t4 = gexp2((-T(0.118300993352895))*s_V);
     const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
     const T v_beta_h = (T(1.7)*v___t5);
-    const T v___t6 = gexp((-(T(0.1)*s_V)));
+    const T v___t6 = gexp2((-T(0.14426950408889636))*s_V);
     const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
     const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
     const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
@@ -488,32 +488,32 @@ struct M_beeler_reuter_1977 {
     const T v___t10 = (T(1.0)/s_Cai);
     const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
     const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
-    const T v___t11 = gexp((-(T(0.07199424046076314)*s_V)));
-    const T v___t12 = gexp((-(T(0.01)*s_V)));
+    const T v___t11 = gexp2((-T(0.10386573368531053))*s_V);
+    const T v___t12 = gexp2((-T(0.014426950408889635))*s_V);
     const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
     const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
-    const T v___t14 = gexp((T(0.05)*s_V));
-    const T v___t15 = gexp((-(T(0.01694915254237288)*s_V)));
+    const T v___t14 = gexp2(T(0.07213475204444818)*s_V);
+    const T v___t15 = gexp2((-T(0.024452458320151922))*s_V);
     const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
     const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
-    const T v___t17 = gexp((T(0.14992503748125938)*s_V));
-    const T v___t18 = gexp((-(T(0.008)*s_V)));
+    const T v___t17 = gexp2(T(0.21629610807930486)*s_V);
+    const T v___t18 = gexp2((-T(0.011541560327111707))*s_V);
     const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
     const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
     const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
     const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
-    const T v___t21 = gexp((T(0.04)*s_V));
-    const T v___t22 = gexp((-(T(0.04)*s_V)));
+    const T v___t21 = gexp2(T(0.05770780163555854)*s_V);
+    const T v___t22 = gexp2((-T(0.05770780163555854))*s_V);
     const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
-    const T v___t23 = gexp((T(0.05714285714285714)*s_V));
-    const T v___t24 = gexp((T(0.08264462809917356)*s_V));
+    const T v___t23 = gexp2(T(0.08243971662222647)*s_V);
+    const T v___t24 = gexp2(T(0.11923099511479036)*s_V);
     const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
     const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
-    const T v___t26 = gexp((-(T(0.05998800239952009)*s_V)));
+    const T v___t26 = gexp2((-T(0.08654439357462287))*s_V);
     const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
     const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
     const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
-    const T v___t28 = gexp((-(T(0.04)*v_V_eff_1)));
+    const T v___t28 = gexp2((-T(0.05770780163555854))*v_V_eff_1);
     const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
     const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
     const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));

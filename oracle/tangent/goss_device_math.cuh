@@ -106,6 +106,7 @@ GOSS_DUAL_CMP(!=)
 #undef GOSS_DUAL_CMP
 
 inline double gexp(double x) { return exp(x); }
+inline double gexp2(double x) { return std::exp2(x); }
 inline double glog(double x) { return log(x); }
 inline double gsqrt(double x) { return sqrt(x); }
 inline double gfabs(double x) { return fabs(x); }
@@ -120,6 +121,11 @@ inline double gtan(double x) { return std::tan(x); }
 inline double gtanh(double x) { return std::tanh(x); }
 
 template <int D> inline Dual<D> gexp(const Dual<D>& a) { const double e = exp(a.v); return Dual<D>::chain(e, e, a); }
+template <int D> inline Dual<D> gexp2(const Dual<D>& a)
+{
+    const double e = std::exp2(a.v);
+    return Dual<D>::chain(e, e * 0.6931471805599453, a);  // d 2^x = 2^x ln 2 dx
+}
 template <int D> inline Dual<D> glog(const Dual<D>& a) { return Dual<D>::chain(log(a.v), 1.0 / a.v, a); }
 template <int D> inline Dual<D> gsqrt(const Dual<D>& a)
 {
