@@ -32,22 +32,22 @@
 
 #include "goss_kernels.cuh"
 
-// Launch shape of the adjoint kernel: threads per block (at most 256, a
-// power of two) and the minimum resident blocks per SM it is compiled for
-// (its register cap is 65536 / (threads * blocks)).  With GOSS_ADJOINT_LOCKSTEP
-// the warps of a block synchronise after every step of the recompute and
-// reverse loops, so they walk the large straight-line step code together and
-// share instruction-cache lines.  Measured on B200 (ten Tusscher-Panfilov,
-// FP32, 65,536 nodes x 2,000 steps): 256 threads x 1 block in lockstep
-// 43.5 ms; 256 x 1 without lockstep 46.8 ms; 128 x 2 in lockstep 47.7 ms,
-// without 50.4 ms; register caps of 168 or 128 (3 or 4 blocks of 128) spill
-// more than the extra warps gain (65-67 ms).
-#ifndef GOSS_ADJOINT_BLOCK
-#define GOSS_ADJOINT_BLOCK 256
-#endif
-#ifndef GOSS_ADJOINT_MIN_BLOCKS
-#define GOSS_ADJOINT_MIN_BLOCKS 1
-#endif
+// Launch shape of the adjoint kernel per arithmetic type: the largest threads
+// per block (a multiple of 32, at most 256) and the minimum resident blocks
+// per SM it is compiled for (its register cap is 65536 / (threads * blocks)).
+// With GOSS_ADJOINT_LOCKSTEP the warps of a block synchronise after every step
+// of the recompute and reverse loops, so they walk the large straight-line
+// step code together and share instruction-cache lines.  Measured on B200
+// (ten Tusscher-Panfilov, 65,536 nodes x 2,000 steps, backward pass):
+//   FP32: blocks of up to 128 threads, 2 per SM (255 registers), lockstep
+//         28.0 ms; 256 x 1: 29.3 ms; register caps of 168 or 128 (3 or 4
+//         blocks of 128) spill more than the extra warps gain: 37.5 ms;
+//   FP64: 256 x 1: 207 ms; 128 x 2: 215 ms.
+template <typename T>
+struct AdjointShape {
+    static constexpr unsigned block = sizeof(T) == 4 ? 128 : 256;
+    static constexpr unsigned min_blocks = sizeof(T) == 4 ? 2 : 1;
+};
 #ifndef GOSS_ADJOINT_LOCKSTEP
 #define GOSS_ADJOINT_LOCKSTEP 1
 #endif
@@ -295,7 +295,7 @@ __device__ __forceinline__ void reverse_step_rk4(const T* yt, double lt, double 
 }
 
 template <class M, typename T, Explicit S>
-__global__ void __launch_bounds__(GOSS_ADJOINT_BLOCK, GOSS_ADJOINT_MIN_BLOCKS)
+__global__ void __launch_bounds__(AdjointShape<T>::block, AdjointShape<T>::min_blocks)
 adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
 {
     constexpr int n = M::num_states;
@@ -380,19 +380,20 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
 // Threads per block for the backward kernel: every thread carries one node
 // through the whole trajectory, so the job runs in waves of (resident blocks
 // x SMs) blocks and its time is about waves x resident warps per SM.  Choose
-// the multiple of 32 (<= GOSS_ADJOINT_BLOCK) minimising that product (ties:
-// the larger block) -- e.g. 224 for 65,536 nodes on 148 SMs (two full waves
-// of 7 warps) instead of 256 (a second wave on 108 of 148 SMs).
+// the multiple of 32 (<= AdjointShape<T>::block) minimising that product (ties:
+// the larger block) -- e.g. for 65,536 nodes on 148 SMs with two blocks per
+// SM: 112 threads (two nearly full waves) instead of 128 (a second wave on
+// 108 of 148 SMs).
 template <class M, typename T, Explicit S>
 inline unsigned adjoint_block(uint32_t num_nodes, size_t shm)
 {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
-        return GOSS_ADJOINT_BLOCK;
-    unsigned best = GOSS_ADJOINT_BLOCK;
+        return AdjointShape<T>::block;
+    unsigned best = AdjointShape<T>::block;
     uint64_t best_cost = ~0ull;
-    for (unsigned b = GOSS_ADJOINT_BLOCK; b >= 32; b -= 32) {
+    for (unsigned b = AdjointShape<T>::block; b >= 32; b -= 32) {
         int active = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&active, adjoint_kernel<M, T, S>, (int)b, shm) !=
                 cudaSuccess || active <= 0)
@@ -449,7 +450,7 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
         if (shm > 48 * 1024)
             return GOSS_ERR_ARGUMENT;
         const unsigned block = L->block ? L->block : adjoint_block<M, T, S>(L->num_nodes, shm);
-        if (block == 0 || block > GOSS_ADJOINT_BLOCK || block % 32)
+        if (block == 0 || block > AdjointShape<T>::block || block % 32)
             return GOSS_ERR_ARGUMENT;
         const unsigned grid = (L->num_nodes + block - 1) / block;
         adjoint_kernel<M, T, S><<<grid, block, shm, (cudaStream_t)L->stream>>>(a);

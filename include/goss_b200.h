@@ -140,7 +140,8 @@ typedef struct goss_adjoint_launch {
     int32_t precision;
     uint32_t num_nodes;
     uint32_t block;           /* backward threads per block: 0 = chosen from the
-                                 node count, else a multiple of 32 <= 256 */
+                                 node count, else a multiple of 32 <= 128 (FP32)
+                                 or <= 256 (FP64) */
     uint64_t ld;
     double* states;
     const double* field_params;
