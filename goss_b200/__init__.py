@@ -5,7 +5,8 @@ Drop-in for the ``goss`` Python entry points of that path
 
 * :class:`ParameterizedODE` / :class:`ODE` -- compiled cell models from
   gotran ``.ode`` files (own parser and code generator, CUDA device code)
-* :mod:`solvers` -- ExplicitEuler, RK4, GRL1, GRL2, ThetaSolver, ESDIRK23a
+* :mod:`solvers` -- ExplicitEuler, RK2, RK4, RL1, RL2, GRL1, GRL2,
+  ImplicitEuler, ThetaSolver, ESDIRK23a
 * :class:`ODESystemSolver` -- one model at every mesh node on the GPU
 
 The compute path is the CUDA runtime ``goss_b200/_lib/libgoss_b200.so`` and

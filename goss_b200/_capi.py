@@ -14,7 +14,8 @@ RUNTIME_SO = PKG / "_lib" / "libgoss_b200.so"
 
 ABI_VERSION = 1
 
-GOSS_EXPLICIT_EULER, GOSS_RK4, GOSS_GRL1, GOSS_GRL2, GOSS_THETA, GOSS_ESDIRK23A = range(6)
+(GOSS_EXPLICIT_EULER, GOSS_RK4, GOSS_GRL1, GOSS_GRL2, GOSS_THETA, GOSS_ESDIRK23A, GOSS_RL1, GOSS_RL2, GOSS_RK2,
+ GOSS_IMPLICIT_EULER) = range(10)
 GOSS_FP64, GOSS_FP32 = 0, 1
 GOSS_OK, GOSS_ERR_ARGUMENT, GOSS_ERR_CUDA, GOSS_ERR_NEWTON, GOSS_ERR_UNSUPPORTED, GOSS_ERR_TIMEOUT = range(6)
 GOSS_FLAG_NONFINITE, GOSS_FLAG_NEWTON_FAILED, GOSS_FLAG_ITERATION_CAP = 1, 2, 4
@@ -26,6 +27,10 @@ SOLVER_KINDS = {
     "GRL2": GOSS_GRL2,
     "ThetaSolver": GOSS_THETA,
     "ESDIRK23a": GOSS_ESDIRK23A,
+    "RL1": GOSS_RL1,
+    "RL2": GOSS_RL2,
+    "RK2": GOSS_RK2,
+    "ImplicitEuler": GOSS_IMPLICIT_EULER,
 }
 
 

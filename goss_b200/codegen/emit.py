@@ -541,6 +541,11 @@ class ModelSource:
         nder = len(self.folder.derived)
         L.insert(L.index(f"  static constexpr int num_monitored = {len(self.ir.monitored)};") + 1,
                  f"  static constexpr int num_derived = {nder};")
+        lin_idx = [i for i, f in enumerate(self.linear_terms) if f]
+        cond = " || ".join(f"i == {i}" for i in lin_idx) or "false"
+        L.insert(L.index(f"  static constexpr int num_derived = {nder};") + 1,
+                 "  // the reference generator's linear-term flags (RL1/RL2 use the exponential update for these)\n"
+                 f"  __host__ __device__ static constexpr bool linear_term(int i) {{ return {cond}; }}")
         L.append("  // derived constants: parameter-only sub-expressions, evaluated once per")
         L.append("  // launch on the host in FP64 and stored after the parameters")
         L.append("  static void derived(const double* P, double* C)")

@@ -107,7 +107,7 @@ struct EvalArgs {
 // ---------------------------------------------------------------------------
 // explicit solvers
 // ---------------------------------------------------------------------------
-enum class Explicit { Euler, RK4, GRL1, GRL2 };
+enum class Explicit { Euler, RK4, GRL1, GRL2, RL1, RL2, RK2 };
 
 template <class M, typename T>
 __device__ __forceinline__ void load_field(const double* __restrict__ fp, uint64_t ld, uint32_t node,
@@ -130,6 +130,18 @@ __device__ __forceinline__ double grl_increment(double a, double b, double h, do
 __device__ __forceinline__ float grl_increment(float a, float b, float h, float /*delta*/)
 {
     return b * h * phi1f(a * h);
+}
+
+// RL increment of one state (RL1.h:68-77): the exponential form for the model's
+// linear-term states whatever the coefficient (the reference divides by it),
+// the Euler increment otherwise
+__device__ __forceinline__ double rl_increment(bool linear, double a, double b, double h)
+{
+    return linear ? b / a * (exp(a * h) - 1.0) : b * h;
+}
+__device__ __forceinline__ float rl_increment(bool linear, float a, float b, float h)
+{
+    return linear ? b * h * phi1f(a * h) : b * h;
 }
 
 // State accumulators.  FP64 kernels hold each state as a double and update it
@@ -270,7 +282,7 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
 #pragma unroll
         for (int i = 0; i < n; ++i)
             y[i].add(grl_increment(lin[i], rhs[i], h, delta));
-    } else {
+    } else if constexpr (S == Explicit::GRL2) {
         // GRL2: GRL2.cpp:78-82.  The reference's branch threshold is a
         // self-initialised local (GRL2.cpp:67) whose -O3 build behaves as 0:
         // the exponential form is used whenever the linear term is non-zero.
@@ -283,6 +295,37 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
 #pragma unroll
         for (int i = 0; i < n; ++i)
             y[i].add(grl_increment(lin[i], rhs[i], h, T(0)));
+    } else if constexpr (S == Explicit::RL1) {
+        // RL1.h:68-77
+        T lin[n], rhs[n];
+        model_linearized<M, T>(yt, lt, P, PD, F, lin, rhs);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y[i].add(rl_increment(M::linear_term(i), lin[i], rhs[i], h));
+    } else if constexpr (S == Explicit::RL2) {
+        // RL2.cpp:78-83: a half step to y2 linearised at y, then the full step
+        // from y linearised at y2, both at time lt
+        T lin[n], rhs[n], y2[n];
+        model_linearized<M, T>(yt, lt, P, PD, F, lin, rhs);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y2[i] = y[i].plus(rl_increment(M::linear_term(i), lin[i], rhs[i], hh));
+        model_linearized<M, T>(y2, lt, P, PD, F, lin, rhs);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y[i].add(rl_increment(M::linear_term(i), lin[i], rhs[i], h));
+    } else {
+        // RK2: RK2.cpp:78-89 with RK2::axpy (RK2.h:70-74), the midpoint rule
+        static_assert(S == Explicit::RK2, "unhandled explicit solver");
+        T k[n], tmp[n];
+        model_rhs<M, T>(yt, lt, P, PD, F, k);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            tmp[i] = y[i].plus(hh * k[i]);
+        model_rhs<M, T>(tmp, lt + 0.5 * ldt, P, PD, F, k);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y[i].add(h * k[i]);
     }
 }
 
@@ -450,7 +493,12 @@ __device__ void compute_jacobian(const double* y, double t, const double* P, con
 // per-node solver state rows
 enum ThetaRows { TH_ETA = 0, TH_RECOMPUTE, TH_ALWAYS, TH_JUSTREFINED, TH_JACCOMP, TH_REJECTS, TH_ACCEPTED, TH_ROWS };
 
-template <class M>
+// ThetaSolver::forward (ThetaSolver.cpp:49-155); with IE, ImplicitEuler::forward
+// (ImplicitEuler.cpp:57-152): theta = 1 (no explicit part, stage time t + ldt),
+// the Jacobian always recomputed once MORE than num_refinements_without_
+// always_recomputing_jacobian refinements happened (Theta: up to that many),
+// and a failed step requests a new Jacobian.
+template <class M, bool IE>
 __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ ImplicitArgs<M> a)
 {
     constexpr int n = M::num_states;
@@ -473,6 +521,14 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
     int always = ss[TH_ALWAYS * ld] != 0.0;
     int justrefined = ss[TH_JUSTREFINED * ld] != 0.0;
     double jac_comp = ss[TH_JACCOMP * ld], rejects = ss[TH_REJECTS * ld], accepted = ss[TH_ACCEPTED * ld];
+    // ImplicitEuler keeps its factorised Jacobian from one forward to the next
+    // (the reference's solver member _jac; ThetaSolver recomputes it first thing
+    // in every forward): it lives in the solver-state rows after the scalars
+    double* const jrows = ss + (uint64_t)TH_ROWS * ld;
+    if constexpr (IE) {
+        for (int k = 0; k < n * n; ++k)
+            Jm[k] = jrows[(uint64_t)k * ld];
+    }
 
     double t = a.t;
     const double dt = a.interval;
@@ -492,16 +548,17 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
         }
         for (int i = 0; i < n; ++i)
             z1[i] = 0.0;
-        if (fabs(sp.theta - 1.0) > kGossEps) {
+        if (!IE && fabs(sp.theta - 1.0) > kGossEps) {
             rhs64<M>(y, t, a.P, F, ft1);
             for (int i = 0; i < n; ++i)
                 prev[i] = (1 - sp.theta) * ft1[i];
         }
-        if (num_refinements <= sp.num_refinements_without_always_recomputing_jacobian)
+        if (IE ? num_refinements > sp.num_refinements_without_always_recomputing_jacobian
+               : num_refinements <= sp.num_refinements_without_always_recomputing_jacobian)
             always = 1;
         // ImplicitODESolver::newton_solve (ImplicitODESolver.cpp:114-245)
-        const double tn = t + sp.theta * ldt;
-        const double alpha = sp.theta;
+        const double tn = IE ? t + ldt : t + sp.theta * ldt;
+        const double alpha = IE ? 1.0 : sp.theta;
         bool step_ok = true;
         int newton_iterations = 0;
         double relative_previous_residual = 1.0, relative_residual = 1.0, previous_residual = 1.0;
@@ -585,6 +642,8 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
                 status |= GOSS_FLAG_NEWTON_FAILED;
                 break;
             }
+            if (IE)
+                recompute = 1;
             justrefined = 1;
             num_refinements += 1;
         }
@@ -596,6 +655,10 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
     }
     if (!finite)
         status |= GOSS_FLAG_NONFINITE;
+    if constexpr (IE) {
+        for (int k = 0; k < n * n; ++k)
+            jrows[(uint64_t)k * ld] = Jm[k];
+    }
     ss[TH_ETA * ld] = eta;
     ss[TH_RECOMPUTE * ld] = recompute;
     ss[TH_ALWAYS * ld] = always;
@@ -923,6 +986,8 @@ inline uint32_t solver_state_rows(int32_t solver)
     constexpr uint32_t n = M::num_states;
     if (solver == GOSS_THETA)
         return TH_ROWS;
+    if (solver == GOSS_IMPLICIT_EULER)
+        return TH_ROWS + n * n;
     if (solver == GOSS_ESDIRK23A)
         return ES_SCALARS + 2 * n * n;
     return 0;
@@ -976,7 +1041,9 @@ inline int launch_implicit(const goss_launch* L)
     if (grid == 0)
         return 0;
     if (L->solver == GOSS_THETA)
-        theta_kernel<M><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+        theta_kernel<M, false><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    else if (L->solver == GOSS_IMPLICIT_EULER)
+        theta_kernel<M, true><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
     else
         esdirk_kernel<M><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
@@ -995,8 +1062,15 @@ inline int launch_solver(const goss_launch* L)
         return f32 ? launch_explicit<M, float, Explicit::GRL1>(L) : launch_explicit<M, double, Explicit::GRL1>(L);
     case GOSS_GRL2:
         return f32 ? launch_explicit<M, float, Explicit::GRL2>(L) : launch_explicit<M, double, Explicit::GRL2>(L);
+    case GOSS_RL1:
+        return f32 ? launch_explicit<M, float, Explicit::RL1>(L) : launch_explicit<M, double, Explicit::RL1>(L);
+    case GOSS_RL2:
+        return f32 ? launch_explicit<M, float, Explicit::RL2>(L) : launch_explicit<M, double, Explicit::RL2>(L);
+    case GOSS_RK2:
+        return f32 ? launch_explicit<M, float, Explicit::RK2>(L) : launch_explicit<M, double, Explicit::RK2>(L);
     case GOSS_THETA:
     case GOSS_ESDIRK23A:
+    case GOSS_IMPLICIT_EULER:
         if (f32)
             return GOSS_ERR_UNSUPPORTED;
         return launch_implicit<M>(L);

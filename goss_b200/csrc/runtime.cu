@@ -186,9 +186,10 @@ int init_solver_state(goss_system* s)
     if (!s->sstate_rows)
         return 0;
     std::vector<double> v(s->sstate_rows, 0.0);
-    if (s->solver == GOSS_THETA) {
+    if (s->solver == GOSS_THETA || s->solver == GOSS_IMPLICIT_EULER) {
         // TH_ETA, TH_RECOMPUTE, TH_ALWAYS, TH_JUSTREFINED, counters
-        // (ImplicitODESolver::reset, ImplicitODESolver.cpp:80-90; ThetaSolver.cpp:37-45)
+        // (ImplicitODESolver::reset, ImplicitODESolver.cpp:80-90; ThetaSolver.cpp:37-45;
+        // ImplicitEuler.cpp:14-21)
         v[0] = s->sp.eta_0;
         v[1] = 1.0;
         v[2] = s->sp.always_recompute_jacobian ? 1.0 : 0.0;
@@ -281,8 +282,8 @@ GOSS_API int goss_solver_default_params(int32_t solver, goss_solver_params* p)
     p->max_iterations = 30;                    // ImplicitODESolver.h:39
     p->max_relative_previous_residual = 0.01;  // ImplicitODESolver.h:40
     p->always_recompute_jacobian = 0;          // ImplicitODESolver.h:41
-    p->num_refinements_without_always_recomputing_jacobian = 2;  // ThetaSolver.h:35
-    p->min_dt = solver == GOSS_ESDIRK23A ? 0.001 : 0.0001;      // ESDIRK23a.h:38, ThetaSolver.h:36
+    p->num_refinements_without_always_recomputing_jacobian = 2;  // ThetaSolver.h:35, ImplicitEuler.h:35
+    p->min_dt = solver == GOSS_ESDIRK23A ? 0.001 : 0.0001;      // ESDIRK23a.h:38, ThetaSolver.h:36, ImplicitEuler.h:36
     p->theta = 0.5;                                              // ThetaSolver.h:37
     return 0;
 }
@@ -299,7 +300,7 @@ GOSS_API int goss_system_create(const goss_model_desc* m, int32_t solver, const 
         return fail(nullptr, GOSS_ERR_UNSUPPORTED, "solver kind %d is not available for model %s", solver, m->name);
     if (precision != GOSS_FP64 && precision != GOSS_FP32)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "invalid precision %d", precision);
-    if ((solver == GOSS_THETA || solver == GOSS_ESDIRK23A) && precision == GOSS_FP32)
+    if ((solver == GOSS_THETA || solver == GOSS_ESDIRK23A || solver == GOSS_IMPLICIT_EULER) && precision == GOSS_FP32)
         return fail(nullptr, GOSS_ERR_UNSUPPORTED,
                     "implicit solvers run their Newton iteration in FP64; use GOSS_FP64 precision");
     auto* s = new goss_system();
@@ -1001,7 +1002,7 @@ GOSS_API int goss_system_counters(const goss_system* cs, int64_t* jac_comp, int6
     if (!s)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL system");
     uint32_t rows[3];
-    if (s->solver == GOSS_THETA) {
+    if (s->solver == GOSS_THETA || s->solver == GOSS_IMPLICIT_EULER) {
         rows[0] = 4, rows[1] = 5, rows[2] = 6;  // TH_JACCOMP, TH_REJECTS, TH_ACCEPTED
     } else if (s->solver == GOSS_ESDIRK23A) {
         rows[0] = 6, rows[1] = 7, rows[2] = 8;  // ES_JACCOMP, ES_REJECTS, ES_ACCEPTED

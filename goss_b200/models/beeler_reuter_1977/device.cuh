@@ -13,6 +13,8 @@ struct M_beeler_reuter_1977 {
   static constexpr int num_field_params = 0;
   static constexpr int num_monitored = 0;
   static constexpr int num_derived = 7;
+  // the reference generator's linear-term flags (RL1/RL2 use the exponential update for these)
+  __host__ __device__ static constexpr bool linear_term(int i) { return i == 0 || i == 1 || i == 2 || i == 4 || i == 5 || i == 6; }
 
   // values = f(y, time)
   template <typename T>

@@ -13,6 +13,8 @@ struct M_oscilator__5dc98ee0 {
   static constexpr int num_field_params = 2;
   static constexpr int num_monitored = 0;
   static constexpr int num_derived = 0;
+  // the reference generator's linear-term flags (RL1/RL2 use the exponential update for these)
+  __host__ __device__ static constexpr bool linear_term(int i) { return false; }
 
   // values = f(y, time)
   template <typename T>

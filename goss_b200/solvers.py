@@ -6,8 +6,8 @@ carries its parameters and the ODE it is attached to; the arithmetic runs in
 the sm_100a kernels.  ``forward``/``solve`` on a single state vector run a
 one-node :class:`~goss_b200.systemsolver.ODESystemSolver`.
 
-Solvers of the reference outside this package's scope (RK2, RL1, RL2,
-ImplicitEuler, RKF32, BasicImplicitEuler, ESDIRK4O32) are not provided.
+Solvers of the reference outside this package's scope (RKF32,
+BasicImplicitEuler, ESDIRK4O32) are not provided.
 """
 from __future__ import annotations
 
@@ -162,6 +162,18 @@ class ExplicitEuler(ODESolver):
     _kind = _capi.GOSS_EXPLICIT_EULER
 
 
+class RL1(ODESolver):
+    _kind = _capi.GOSS_RL1
+
+
+class RL2(ODESolver):
+    _kind = _capi.GOSS_RL2
+
+
+class RK2(ODESolver):
+    _kind = _capi.GOSS_RK2
+
+
 class RK4(ODESolver):
     _kind = _capi.GOSS_RK4
 
@@ -208,6 +220,19 @@ class ImplicitODESolver(ODESolver, abc.ABC):
         self._ode.lu_factorize(jac)
         self._jac = jac
         self._counters["jac_comp"] += 1
+
+
+class ImplicitEuler(ImplicitODESolver):
+    _kind = _capi.GOSS_IMPLICIT_EULER
+
+    @staticmethod
+    def default_parameters() -> Dict[str, Any]:
+        names = ImplicitODESolver.default_parameters()
+        names.update({
+            "num_refinements_without_always_recomputing_jacobian": 2,
+            "min_dt": 0.0001,
+        })
+        return names
 
 
 class ThetaSolver(ImplicitODESolver):
@@ -302,30 +327,42 @@ class ESDIRK23a(ESDIRK):
 
 class GOSSSolvers(Enum):
     ExplicitEuler = "ExplicitEuler"
+    RK2 = "RK2"
     RK4 = "RK4"
+    RL1 = "RL1"
+    RL2 = "RL2"
     GRL1 = "GRL1"
     GRL2 = "GRL2"
+    ImplicitEuler = "ImplicitEuler"
     ThetaSolver = "ThetaSolver"
     ESDIRK23a = "ESDIRK23a"
 
 
 class GOSSImplicitSolvers(Enum):
+    ImplicitEuler = "ImplicitEuler"
     ThetaSolver = "ThetaSolver"
     ESDIRK23a = "ESDIRK23a"
 
 
 class GOSSExplicitSolvers(Enum):
     ExplicitEuler = "ExplicitEuler"
+    RK2 = "RK2"
     RK4 = "RK4"
+    RL1 = "RL1"
+    RL2 = "RL2"
     GRL1 = "GRL1"
     GRL2 = "GRL2"
 
 
 class GOSSNonAdaptiveSolvers(Enum):
     ExplicitEuler = "ExplicitEuler"
+    RK2 = "RK2"
     RK4 = "RK4"
+    RL1 = "RL1"
+    RL2 = "RL2"
     GRL1 = "GRL1"
     GRL2 = "GRL2"
+    ImplicitEuler = "ImplicitEuler"
     ThetaSolver = "ThetaSolver"
 
 
@@ -335,9 +372,13 @@ class GOSSAdaptiveSolvers(Enum):
 
 solver_mapper = {
     "ExplicitEuler": ExplicitEuler,
+    "RK2": RK2,
     "RK4": RK4,
+    "RL1": RL1,
+    "RL2": RL2,
     "GRL1": GRL1,
     "GRL2": GRL2,
+    "ImplicitEuler": ImplicitEuler,
     "ThetaSolver": ThetaSolver,
     "ESDIRK23a": ESDIRK23a,
 }

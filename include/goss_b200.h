@@ -3,8 +3,8 @@
  *
  * This is the drop-in boundary that replaces the execution of
  * goss::ODESystemSolver (reference cpp/goss/ODESystemSolver.h:43-124) and of
- * the per-node solvers it drives (ExplicitEuler, RK4, GRL1, GRL2,
- * ThetaSolver, ESDIRK23a).  Only plain C types cross it: pointers, sizes,
+ * the per-node solvers it drives (ExplicitEuler, RK2, RK4, RL1, RL2, GRL1,
+ * GRL2, ImplicitEuler, ThetaSolver, ESDIRK23a).  Only plain C types cross it: pointers, sizes,
  * doubles and integer status codes.  Host arrays are borrowed for the
  * duration of a call and the call is complete on return (the reference is
  * synchronous), except for the *_async entry points.
@@ -45,7 +45,11 @@ enum goss_solver_kind {
     GOSS_GRL2 = 3,           /* cpp/goss/GRL2.cpp:63-86 */
     GOSS_THETA = 4,          /* cpp/goss/ThetaSolver.cpp:49-155 */
     GOSS_ESDIRK23A = 5,      /* cpp/goss/ESDIRK23a.cpp:280-316 */
-    GOSS_NUM_SOLVERS = 6
+    GOSS_RL1 = 6,            /* cpp/goss/RL1.cpp:60-80, RL1.h:68-77 */
+    GOSS_RL2 = 7,            /* cpp/goss/RL2.cpp:64-87 */
+    GOSS_RK2 = 8,            /* cpp/goss/RK2.cpp:62-92 */
+    GOSS_IMPLICIT_EULER = 9, /* cpp/goss/ImplicitEuler.cpp:57-152 */
+    GOSS_NUM_SOLVERS = 10
 };
 
 /* Arithmetic of the right-hand side.  States are always stored and

@@ -62,8 +62,8 @@ void oracle_default_solver_params(int solver, oracle_solver_params* p)
     p->max_iterations = 30;              /* :39 */
     p->max_relative_previous_residual = 0.01; /* :40 */
     p->always_recompute_jacobian = 0;    /* :41 */
-    p->num_refinements_without_always_recomputing_jacobian = 2; /* ThetaSolver.h:35 */
-    p->min_dt = solver == ORACLE_ESDIRK23A ? 0.001 : 0.0001;   /* ESDIRK23a.h:38, ThetaSolver.h:36 */
+    p->num_refinements_without_always_recomputing_jacobian = 2; /* ThetaSolver.h:35, ImplicitEuler.h:35 */
+    p->min_dt = solver == ORACLE_ESDIRK23A ? 0.001 : 0.0001;   /* ESDIRK23a.h:38, ThetaSolver.h:36, ImplicitEuler.h:36 */
     p->theta = 0.5;                      /* ThetaSolver.h:37 */
 }
 
@@ -84,7 +84,7 @@ static void node_reset(oracle_system* s, node_state* st)
     st->first_step = 1;
     st->new_jacobian = 1;
     st->justrefined = 0;
-    if (s->solver == ORACLE_THETA || s->solver == ORACLE_ESDIRK23A) {
+    if (s->solver == ORACLE_THETA || s->solver == ORACLE_ESDIRK23A || s->solver == ORACLE_IMPLICIT_EULER) {
         st->jac = (double*)calloc((size_t)n * n, sizeof(double));
         st->jfac = (double*)calloc((size_t)n * n, sizeof(double));
     } else {
@@ -324,6 +324,65 @@ static void fwd_grl2(const oracle_model* m, const double* P, double* y, double t
     }
 }
 
+/* RL1::_one_step (RL1.h:68-77): linearized_eval with only_linear = true, then
+ * the exponential update for the model's linear-term states (no threshold:
+ * a zero linear coefficient gives the reference's 0/0) and Euler otherwise */
+static void rl_one_step(const oracle_model* m, const double* P, double* y2, const double* y, const double* y0,
+                        double t, double dt, scratch* w)
+{
+    int n = m->num_states;
+    double *lin = w->a, *rhs = w->b;
+    m->linearized(y, t, P, lin, rhs, 1);
+    for (int i = 0; i < n; ++i)
+        y2[i] = m->linear_terms[i] ? y0[i] + rhs[i] / lin[i] * (exp(lin[i] * dt) - 1.0) : y0[i] + rhs[i] * dt;
+}
+
+/* RL1::forward (RL1.cpp:60-80) */
+static void fwd_rl1(const oracle_model* m, const double* P, double* y, double t, double dt, double ldt_0,
+                    scratch* w)
+{
+    unsigned long nsteps = num_steps(ldt_0, dt);
+    double ldt = dt / nsteps, lt = t;
+    for (unsigned long s = 0; s < nsteps; ++s) {
+        rl_one_step(m, P, y, y, y, lt, ldt, w);
+        lt += ldt;
+    }
+}
+
+/* RL2::forward (RL2.cpp:64-87): half step to y2 linearised at y, then a full
+ * step from y linearised at y2, both at time lt */
+static void fwd_rl2(const oracle_model* m, const double* P, double* y, double t, double dt, double ldt_0,
+                    scratch* w)
+{
+    unsigned long nsteps = num_steps(ldt_0, dt);
+    double ldt = dt / nsteps, lt = t;
+    double* y2 = w->c;
+    for (unsigned long s = 0; s < nsteps; ++s) {
+        rl_one_step(m, P, y2, y, y, lt, ldt * 0.5, w);
+        rl_one_step(m, P, y, y2, y, lt, ldt, w);
+        lt += ldt;
+    }
+}
+
+/* RK2::forward (RK2.cpp:62-92) with RK2::axpy (RK2.h:70-74): the midpoint rule */
+static void fwd_rk2(const oracle_model* m, const double* P, double* y, double t, double dt, double ldt_0,
+                    scratch* w)
+{
+    int n = m->num_states;
+    double *k1 = w->a, *tmp = w->b;
+    unsigned long nsteps = num_steps(ldt_0, dt);
+    double ldt = dt / nsteps, lt = t;
+    for (unsigned long j = 0; j < nsteps; ++j) {
+        m->rhs(y, lt, P, k1);
+        for (int i = 0; i < n; ++i)
+            tmp[i] = y[i] + 0.5 * ldt * k1[i];
+        m->rhs(tmp, lt + 0.5 * ldt, P, k1);
+        for (int i = 0; i < n; ++i)
+            y[i] += ldt * k1[i];
+        lt += ldt;
+    }
+}
+
 /* ---------------------------------------------------------------------- */
 /* ThetaSolver                                                            */
 /* ---------------------------------------------------------------------- */
@@ -452,6 +511,60 @@ static int fwd_theta(const oracle_model* m, const double* P, const oracle_solver
             ldt /= 2.0;
             if (ldt < sp->min_dt)
                 return 1;
+            st->justrefined = 1;
+            num_refinements += 1;
+        }
+    }
+    return 0;
+}
+
+/* ImplicitEuler::forward (ImplicitEuler.cpp:57-152): the theta loop at
+ * theta = 1 (no explicit part, stage time t + ldt), except that the Jacobian
+ * is always recomputed once more than num_refinements_without_always_
+ * recomputing_jacobian refinements happened (ThetaSolver: up to that many),
+ * and a failed step also requests a new Jacobian.  Returns 0 on success and
+ * 1 when the step size fell below min_dt (the reference throws). */
+static int fwd_implicit_euler(const oracle_model* m, const double* P, const oracle_solver_params* sp,
+                              node_state* st, double* y, double t, double dt, scratch* w)
+{
+    int n = m->num_states;
+    double *z1 = w->a, *prev = w->c;
+    const double t_end = t + dt;
+    const double ldt_0 = sp->ldt;
+    double ldt = ldt_0 > 0 ? ldt_0 : dt;
+    int num_refinements = 0;
+    const double eps = GOSS_EPS * 1000;
+    for (int i = 0; i < n; ++i)
+        prev[i] = 0.0;
+    while (1) {
+        for (int i = 0; i < n; ++i)
+            z1[i] = 0.0;
+        if (num_refinements > sp->num_refinements_without_always_recomputing_jacobian)
+            st->always_recompute_jacobian = 1;
+        int step_ok = newton_solve(m, P, sp, st, z1, prev, y, t + ldt, ldt, 1.0, st->always_recompute_jacobian, w);
+        if (step_ok) {
+            for (int i = 0; i < n; ++i)
+                y[i] += z1[i];
+            t += ldt;
+            st->accepted++;
+            if (fabs(t - t_end) < eps)
+                break;
+            if (!st->justrefined) {
+                const double tmp = 2.0 * ldt;
+                if (ldt_0 > 0. && tmp >= ldt_0)
+                    ldt = ldt_0;
+                else
+                    ldt = tmp;
+            } else {
+                st->justrefined = 0;
+            }
+            if ((t + ldt + GOSS_EPS) > t_end)
+                ldt = t_end - t;
+        } else {
+            ldt /= 2.0;
+            if (ldt < sp->min_dt)
+                return 1;
+            st->recompute_jacobian = 1;
             st->justrefined = 1;
             num_refinements += 1;
         }
@@ -721,6 +834,18 @@ int oracle_system_forward(oracle_system* s, double t, double interval, int num_t
                 break;
             case ORACLE_ESDIRK23A:
                 fwd_esdirk(m, P, &s->sp, st, y, t, interval, &w);
+                break;
+            case ORACLE_RL1:
+                fwd_rl1(m, P, y, t, interval, s->sp.ldt, &w);
+                break;
+            case ORACLE_RL2:
+                fwd_rl2(m, P, y, t, interval, s->sp.ldt, &w);
+                break;
+            case ORACLE_RK2:
+                fwd_rk2(m, P, y, t, interval, s->sp.ldt, &w);
+                break;
+            case ORACLE_IMPLICIT_EULER:
+                failures += fwd_implicit_euler(m, P, &s->sp, st, y, t, interval, &w);
                 break;
             default:
                 break;

@@ -47,7 +47,11 @@ enum {
     ORACLE_GRL1 = 2,
     ORACLE_GRL2 = 3,
     ORACLE_THETA = 4,
-    ORACLE_ESDIRK23A = 5
+    ORACLE_ESDIRK23A = 5,
+    ORACLE_RL1 = 6,
+    ORACLE_RL2 = 7,
+    ORACLE_RK2 = 8,
+    ORACLE_IMPLICIT_EULER = 9
 };
 
 /* solver parameters (public members of the reference solver classes) */

@@ -22,7 +22,8 @@ HERE = Path(__file__).resolve().parent
 BUILD = HERE / "_build"
 REFDIR = HERE / "_ref"
 
-SOLVERS = {"ExplicitEuler": 0, "RK4": 1, "GRL1": 2, "GRL2": 3, "ThetaSolver": 4, "ESDIRK23a": 5}
+SOLVERS = {"ExplicitEuler": 0, "RK4": 1, "GRL1": 2, "GRL2": 3, "ThetaSolver": 4, "ESDIRK23a": 5,
+           "RL1": 6, "RL2": 7, "RK2": 8, "ImplicitEuler": 9}
 
 _dp = C.POINTER(C.c_double)
 

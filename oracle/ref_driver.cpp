@@ -26,9 +26,13 @@
 #include "goss/ExplicitEuler.h"
 #include "goss/GRL1.h"
 #include "goss/GRL2.h"
+#include "goss/ImplicitEuler.h"
 #include "goss/ODESystemSolver.h"
 #include "goss/ParameterizedODE.h"
+#include "goss/RK2.h"
 #include "goss/RK4.h"
+#include "goss/RL1.h"
+#include "goss/RL2.h"
 #include "goss/ThetaSolver.h"
 
 namespace {
@@ -90,6 +94,29 @@ std::shared_ptr<goss::ODESolver> make_solver(int kind, const RefParams& p)
         s = es;
         break;
     }
+    case 6:
+        s = std::make_shared<goss::RL1>();
+        break;
+    case 7:
+        s = std::make_shared<goss::RL2>();
+        break;
+    case 8:
+        s = std::make_shared<goss::RK2>();
+        break;
+    case 9: {
+        auto ie = std::make_shared<goss::ImplicitEuler>();
+        ie->eta_0 = p.eta_0;
+        ie->kappa = p.kappa;
+        ie->relative_tolerance = p.relative_tolerance;
+        ie->max_iterations = p.max_iterations;
+        ie->max_relative_previous_residual = p.max_relative_previous_residual;
+        ie->always_recompute_jacobian = p.always_recompute_jacobian != 0;
+        ie->num_refinements_without_always_recomputing_jacobian =
+            p.num_refinements_without_always_recomputing_jacobian;
+        ie->min_dt = p.min_dt;
+        s = ie;
+        break;
+    }
     default:
         return nullptr;
     }
@@ -111,7 +138,7 @@ struct RefSystem {
     uint32_t threads = 0;
 };
 
-bool implicit(int kind) { return kind == 4 || kind == 5; }
+bool implicit(int kind) { return kind == 4 || kind == 5 || kind == 9; }
 
 }  // namespace
 

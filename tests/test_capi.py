@@ -65,7 +65,7 @@ def test_model_descriptor_matches_metadata(vdir):
     assert [d.initial_conditions[i] for i in range(n)] == md["initial_conditions"]
     assert [d.default_parameters[i] for i in range(npar)] == md["default_parameters"]
     assert [d.linear_terms[i] for i in range(n)] == md["linear_terms"]
-    assert d.supported_solvers == (1 << 6) - 1
+    assert d.supported_solvers == (1 << 10) - 1
     assert d.solver_state_rows(_capi.GOSS_GRL1) == 0
     assert d.solver_state_rows(_capi.GOSS_ESDIRK23A) == 9 + 2 * n * n
 

@@ -155,3 +155,46 @@ def test_config1_tp06_grl1_1024_nodes_1000ms():
     gpu, cpu = system.states, o.states.copy()
     assert np.isfinite(gpu).all()
     assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+# ---------------------------------------------------------------------------
+# RL1, RL2, RK2 and ImplicitEuler (RL1.h:68-77, RL2.cpp:64-87, RK2.cpp:62-92,
+# ImplicitEuler.cpp:57-152)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("model,solver,steps,dt,ldt", [
+    ("tentusscher_panfilov_2006_M_cell", "RL1", 40, 0.5, 0.01),
+    ("tentusscher_panfilov_2006_M_cell", "RL2", 40, 0.5, 0.05),
+    ("tentusscher_panfilov_2006_M_cell", "RK2", 40, 0.5, 0.001),
+    ("beeler_reuter_1977", "RL1", 20, 1.0, 0.01),
+    ("beeler_reuter_1977", "RL2", 20, 1.0, 0.01),
+    ("fitzhughnagumo", "RK2", 20, 1.0, 0.01),
+    ("fhn", "RL2", 20, 1.0, 0.01),
+])
+def test_rush_larsen_and_rk2_fp64(model, solver, steps, dt, ldt):
+    gpu, cpu, _ = run_pair(model, solver, 37, steps, dt, ldt)
+    assert np.isfinite(cpu).all()
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+
+
+@pytest.mark.parametrize("steps,dt,ldt", [(40, 0.1, 0.1), (30, 0.1, -1.0)])
+def test_tt04_implicit_euler_fp64(steps, dt, ldt):
+    gpu, cpu, system = run_pair("tentusscher_2004_mcell", "ImplicitEuler", 16, steps, dt, ldt)
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+    jc, _, _ = system.counters()
+    assert jc.min() > 0
+
+
+@pytest.mark.parametrize("solver,ldt", [("RL1", 0.01), ("RL2", 0.01), ("RK2", 0.001)])
+def test_new_explicit_solvers_fp32_close_to_fp64(solver, ldt):
+    """FP32 arithmetic with compensated FP64-equivalent state accumulation:
+    V through the TP06 upstroke within 1e-3 of FP64."""
+    g32, _, s32 = run_pair("tentusscher_panfilov_2006_M_cell", solver, 40, 30, 1.0, ldt, precision="single")
+    g64, cpu, _ = run_pair("tentusscher_panfilov_2006_M_cell", solver, 40, 30, 1.0, ldt)
+    iv = s32.ode.state_names.index("V")
+    assert np.max(np.abs(g32[:, iv] - g64[:, iv]) / np.abs(g64[:, iv])) < 1e-3
+
+
+def test_implicit_euler_rejects_fp32():
+    ode = goss.ParameterizedODE("tentusscher_2004_mcell")
+    with pytest.raises(Exception):
+        goss.ODESystemSolver(4, goss.solvers.ImplicitEuler(ode), ode, precision="single")

@@ -25,6 +25,13 @@ CASES = [
     ("tentusscher_2004_mcell", "ESDIRK23a", 4, 60, 0.1, -1.0),
     ("beeler_reuter_1977", "GRL1", 8, 1500, 0.01, 0.01),
     ("fitzhughnagumo", "RK4", 8, 500, 0.1, 0.01),
+    ("tentusscher_panfilov_2006_M_cell", "RL1", 8, 1500, 0.01, 0.01),
+    ("tentusscher_panfilov_2006_M_cell", "RL2", 8, 150, 0.1, 0.1),
+    ("tentusscher_panfilov_2006_M_cell", "RK2", 8, 1500, 0.01, 0.005),
+    ("beeler_reuter_1977", "RL2", 8, 1500, 0.01, 0.01),
+    ("fitzhughnagumo", "RK2", 8, 500, 0.1, 0.01),
+    ("tentusscher_2004_mcell", "ImplicitEuler", 4, 150, 0.1, 0.1),
+    ("tentusscher_2004_mcell", "ImplicitEuler", 4, 60, 0.1, -1.0),
 ]
 
 
@@ -44,7 +51,7 @@ def test_restatement_bit_identical_to_reference(model, solver, N, steps, dt, ldt
         assert r.forward(k * dt, dt) == 0
     a, b = o.states.copy(), r.get_states()
     assert np.array_equal(a, b, equal_nan=True), float(np.nanmax(np.abs(a - b)))
-    if solver in ("ThetaSolver", "ESDIRK23a"):
+    if solver in ("ThetaSolver", "ESDIRK23a", "ImplicitEuler"):
         jc, _, _ = o.counters()
         assert np.array_equal(jc, r.num_jac_comp())
 
