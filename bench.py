@@ -293,6 +293,7 @@ def run_gpu(args, rank, world, dist):
     out["batched"] = run_batched(args, dev) if not args.skip_fp64 else None
     out["adjoint"] = run_adjoint(dev) if not args.skip_fp64 else None
     out["implicit"] = run_implicit(dev) if not args.skip_fp64 else None
+    out["coupled"] = run_coupled(dev) if not args.skip_fp64 else None
 
     ms32, fp64_ms_max, e2e_s = max_over_ranks([ms32, fp64_ms or 0.0, e2e_s], dist, "cuda")
     cell_steps = float(N) * steps_per_call * args.steps * world
@@ -440,6 +441,67 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
                                       "elementwise_median": float(np.median(elem)),
                                       "elementwise_p99": float(np.quantile(elem, 0.99))},
     }
+
+
+def run_coupled(dev, steps=200, pde_dt=0.1):
+    """Operator splitting on the headline population: 1,048,576 TP06 nodes,
+    FP32 GRL1 at 0.01 ms, V exchanged with a PDE vector every 0.1 ms (10
+    internal steps per exchange), 200 exchanges.  Device: FieldStateCoupling
+    (PDE vector a CUDA tensor, zero-copy exchange on the launch stream);
+    host: the reference's way, field states copied to and from a host vector
+    every exchange.  No PDE work in either, so the difference is the exchange."""
+    import torch
+
+    import goss_b200 as goss
+    from goss_b200.coupling import FieldStateCoupling
+
+    md, y0, fp = inputs(N_NODES)
+    ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS, field_states=["V"])
+    iv = md["state_names"].index("V")
+
+    def make():
+        solver = goss.solvers.GRL1(ode)
+        solver.internal_time_step = LDT
+        system = goss.ODESystemSolver(N_NODES, solver, ode, precision="single", device=dev)
+        system.set_states(y0)
+        system.field_parameters = fp
+        return system
+
+    out = {}
+    system = make()
+    cpl = FieldStateCoupling({"tissue": system}, {"tissue": np.arange(N_NODES)}, N_NODES)
+    v = torch.tensor(y0[:, iv], device=torch.device("cuda", dev))
+    for k in range(5):
+        cpl.step((k * pde_dt, (k + 1) * pde_dt), v)
+    cpl.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(cpl.stream)
+    for k in range(5, 5 + steps):
+        cpl.step((k * pde_dt, (k + 1) * pde_dt), v)
+    e1.record(cpl.stream)
+    cpl.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cell_steps = float(N_NODES) * steps * round(pde_dt / LDT)
+    out["device"] = {"value": cell_steps / (ms / 1e3), "ms_per_exchange": ms / steps}
+    del cpl, system
+    system = make()
+    vh = np.ascontiguousarray(y0[:, iv:iv + 1])
+    for k in range(5):
+        system.field_states = vh
+        system.forward(k * pde_dt, pde_dt)
+        vh = system.field_states
+    w0 = time.perf_counter()
+    for k in range(5, 5 + steps):
+        system.field_states = vh
+        system.forward(k * pde_dt, pde_dt)
+        vh = system.field_states
+    s = time.perf_counter() - w0
+    out["host_copies"] = {"value": cell_steps / s, "ms_per_exchange": 1e3 * s / steps}
+    out["workload"] = (f"{MODEL} FP32 GRL1 dt=0.01ms, {N_NODES} nodes, V exchanged every {pde_dt} ms, "
+                       f"{steps} exchanges")
+    out["unit"] = "cell-steps/s"
+    return out
 
 
 IMPLICIT_MODEL, IMPLICIT_FIELDS, IMPLICIT_NODES, IMPLICIT_DT = "tentusscher_2004_mcell", ["g_Kr", "g_CaL"], 262_144, 0.1
@@ -703,7 +765,7 @@ def main():
                          "v_max_rel_err_fp32_vs_fp64": res["v_max_rel_err_fp32_vs_fp64"]},
                 "state_max_rel_err_fp32_vs_fp64": res.get("state_max_rel_err_fp32_vs_fp64"),
                 "batched_heterogeneous": res.get("batched"), "adjoint": res.get("adjoint"),
-                "implicit": res.get("implicit")}
+                "implicit": res.get("implicit"), "coupled": res.get("coupled")}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -8,6 +8,8 @@ Drop-in for the ``goss`` Python entry points of that path
 * :mod:`solvers` -- ExplicitEuler, RK2, RK4, RL1, RL2, GRL1, GRL2,
   ImplicitEuler, ThetaSolver, ESDIRK23a
 * :class:`ODESystemSolver` -- one model at every mesh node on the GPU
+* :class:`FieldStateCoupling` -- operator-splitting exchange with a PDE
+  vector kept on the GPU (the role of ``DOLFINODESystemSolver``)
 
 The compute path is the CUDA runtime ``goss_b200/_lib/libgoss_b200.so`` and
 one ``libgoss_model.so`` per model variant; there is no CPU fallback.
@@ -48,5 +50,6 @@ __all__ = [
 ]
 
 from .batch import BatchSolver  # noqa: E402
+from .coupling import FieldStateCoupling  # noqa: E402
 
-__all__.append("BatchSolver")
+__all__ += ["BatchSolver", "FieldStateCoupling"]
