@@ -54,8 +54,20 @@ struct BatchArgs : BatchParamsT<T> {
     }
 };
 
+// Resident 128-thread blocks per SM the batch kernel is compiled for: a launch
+// streams every population's states through HBM for a step or a few, so
+// warps in flight matter -- FP32 fits 4 blocks (128 registers), FP64 stays at
+// the compiler's choice (its models spill heavily below ~240 registers).
+#ifndef GOSS_BATCH_MIN_BLOCKS_F32
+#define GOSS_BATCH_MIN_BLOCKS_F32 4
+#endif
+template <typename T>
+struct BatchShape {
+    static constexpr int min_blocks = sizeof(T) == 4 ? GOSS_BATCH_MIN_BLOCKS_F32 : 1;
+};
+
 template <class Dispatch, typename T>
-__global__ void __launch_bounds__(128) batch_kernel(const __grid_constant__ BatchArgs<T> a)
+__global__ void __launch_bounds__(128, BatchShape<T>::min_blocks) batch_kernel(const __grid_constant__ BatchArgs<T> a)
 {
     __shared__ uint32_t s_tile;
     uint32_t tile = blockIdx.x;
