@@ -87,6 +87,8 @@ def tune_batch(batch: BatchSolver, interval: float, t0: float = 0.0, steps: int 
                         if schedule == 1 and grid == 0:
                             continue  # a work counter only helps a persistent grid
                         candidates.append(dict(block=block, grid=grid, schedule=schedule, order=order))
+            for order in (None, [int(i) for i in by_cost]):   # persistent, prefetching
+                candidates.append(dict(block=block, grid=0, schedule=2, order=order))
     best = None
     try:
         for c in candidates:

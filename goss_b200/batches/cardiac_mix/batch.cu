@@ -20,6 +20,22 @@ struct Dispatch {
         default: break;
         }
     }
+    // the same with the node's state rows, then its field-parameter rows, at
+    // rows[r * stride] (a tile staged in shared memory)
+    static constexpr int max_rows = 23;
+    template <typename T>
+    __device__ static __forceinline__ void run_from(int kind, const goss_b200::NodeIO& io, uint32_t node,
+                                                    const T* __restrict__ P, const double* __restrict__ PD,
+                                                    const double* rows, uint32_t stride)
+    {
+        switch (kind) {
+        case 0: goss_b200::explicit_node_from<goss_b200::models::M_fitzhughnagumo__5dc98ee0, T, goss_b200::Explicit::RK4>(io, node, P, PD, rows, stride); break;
+        case 1: goss_b200::explicit_node_from<goss_b200::models::M_oscilator__5dc98ee0, T, goss_b200::Explicit::RK4>(io, node, P, PD, rows, stride); break;
+        case 2: goss_b200::explicit_node_from<goss_b200::models::M_tentusscher_2004_mcell__dc47354d, T, goss_b200::Explicit::GRL1>(io, node, P, PD, rows, stride); break;
+        case 3: goss_b200::explicit_node_from<goss_b200::models::M_tentusscher_panfilov_2006_M_cell__dc47354d, T, goss_b200::Explicit::GRL1>(io, node, P, PD, rows, stride); break;
+        default: break;
+        }
+    }
     static int param_block_size(int kind)
     {
         switch (kind) {
@@ -28,6 +44,16 @@ struct Dispatch {
         case 2: return goss_b200::Dims<goss_b200::models::M_tentusscher_2004_mcell__dc47354d>::np;
         case 3: return goss_b200::Dims<goss_b200::models::M_tentusscher_panfilov_2006_M_cell__dc47354d>::np;
         default: return -1;
+        }
+    }
+    static void row_counts(int kind, uint32_t* ns, uint32_t* nf)
+    {
+        switch (kind) {
+        case 0: *ns = 2; *nf = 2; return;
+        case 1: *ns = 2; *nf = 2; return;
+        case 2: *ns = 17; *nf = 4; return;
+        case 3: *ns = 19; *nf = 4; return;
+        default: *ns = *nf = 0; return;
         }
     }
     static void param_block(int kind, const double* params, double* out)

@@ -26,7 +26,8 @@ def batch_name(kinds: Sequence[Tuple[str, str]]) -> str:
 
 def emit_batch(name: str, kinds: Sequence[Tuple[Path, str]], pkg_dir: Path) -> str:
     """kinds: (variant directory, solver name) per kind."""
-    inc, cases, sizes, blocks, variants, solvers, nstates = [], [], [], [], [], [], []
+    inc, cases, cases_from, sizes, blocks, variants, solvers, nstates, rows = [], [], [], [], [], [], [], [], []
+    max_rows = 1
     for k, (vdir, solver) in enumerate(kinds):
         vdir = Path(vdir).resolve()
         md = json.loads((vdir / "model.json").read_text())
@@ -37,6 +38,10 @@ def emit_batch(name: str, kinds: Sequence[Tuple[Path, str]], pkg_dir: Path) -> s
         inc.append(f'#include "{rel.as_posix()}/device.cuh"')
         S = f"goss_b200::Explicit::{EXPLICIT[solver][0]}"
         cases.append(f"        case {k}: goss_b200::explicit_node<{M}, T, {S}>(io, node, P, PD); break;")
+        cases_from.append(f"        case {k}: goss_b200::explicit_node_from<{M}, T, {S}>(io, node, P, PD, rows, stride); "
+                          "break;")
+        max_rows = max(max_rows, len(md["state_names"]) + len(md["field_parameter_names"]))
+        rows.append(f"        case {k}: *ns = {len(md['state_names'])}; *nf = {len(md['field_parameter_names'])}; return;")
         sizes.append(f"        case {k}: return goss_b200::Dims<{M}>::np;")
         blocks.append(f"        case {k}: {{ double tmp[goss_b200::Dims<{M}>::np]; "
                       f"goss_b200::parameter_block<{M}>(params, tmp); "
@@ -61,11 +66,31 @@ def emit_batch(name: str, kinds: Sequence[Tuple[Path, str]], pkg_dir: Path) -> s
         "        default: break;",
         "        }",
         "    }",
+        "    // the same with the node's state rows, then its field-parameter rows, at",
+        "    // rows[r * stride] (a tile staged in shared memory)",
+        f"    static constexpr int max_rows = {max_rows};",
+        "    template <typename T>",
+        "    __device__ static __forceinline__ void run_from(int kind, const goss_b200::NodeIO& io, uint32_t node,",
+        "                                                    const T* __restrict__ P, const double* __restrict__ PD,",
+        "                                                    const double* rows, uint32_t stride)",
+        "    {",
+        "        switch (kind) {",
+        *cases_from,
+        "        default: break;",
+        "        }",
+        "    }",
         "    static int param_block_size(int kind)",
         "    {",
         "        switch (kind) {",
         *sizes,
         "        default: return -1;",
+        "        }",
+        "    }",
+        "    static void row_counts(int kind, uint32_t* ns, uint32_t* nf)",
+        "    {",
+        "        switch (kind) {",
+        *rows,
+        "        default: *ns = *nf = 0; return;",
         "        }",
         "    }",
         "    static void param_block(int kind, const double* params, double* out)",

@@ -329,19 +329,13 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
     }
 }
 
-// Advance one node over nsteps internal steps of one explicit solver.
+// Advance one node over nsteps internal steps of one explicit solver, from
+// its accumulated states and field parameters, and store the result.
 template <class M, typename T, Explicit S>
-__device__ __forceinline__ void explicit_node(const NodeIO& a, uint32_t node, const T* __restrict__ P,
-                                              const double* __restrict__ PD)
+__device__ __forceinline__ void explicit_node_core(const NodeIO& a, uint32_t node, const T* __restrict__ P,
+                                                   const double* __restrict__ PD, Acc<T>* y, const T* F)
 {
     constexpr int n = M::num_states;
-    Acc<T> y[n];
-#pragma unroll
-    for (int i = 0; i < n; ++i)
-        y[i].load(a.states[i * a.ld + node]);
-    T F[Dims<M>::nfp];
-    load_field<M, T>(a.fparams, a.ld, node, F);
-
     const double ldt = a.ldt;
     const T delta = T(a.delta);
     double lt = a.t;
@@ -360,6 +354,40 @@ __device__ __forceinline__ void explicit_node(const NodeIO& a, uint32_t node, co
         a.node_status[node] |= GOSS_FLAG_NONFINITE;
         atomicOr(a.flags, GOSS_FLAG_NONFINITE);
     }
+}
+
+// ... reading the node's states and field parameters from global memory
+template <class M, typename T, Explicit S>
+__device__ __forceinline__ void explicit_node(const NodeIO& a, uint32_t node, const T* __restrict__ P,
+                                              const double* __restrict__ PD)
+{
+    constexpr int n = M::num_states;
+    Acc<T> y[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+        y[i].load(a.states[i * a.ld + node]);
+    T F[Dims<M>::nfp];
+    load_field<M, T>(a.fparams, a.ld, node, F);
+    explicit_node_core<M, T, S>(a, node, P, PD, y, F);
+}
+
+// ... reading them from rows[r * stride]: the n state rows, then the field
+// parameter rows (a tile staged in shared memory by the batch kernel)
+template <class M, typename T, Explicit S>
+__device__ __forceinline__ void explicit_node_from(const NodeIO& a, uint32_t node, const T* __restrict__ P,
+                                                   const double* __restrict__ PD, const double* rows,
+                                                   uint32_t stride)
+{
+    constexpr int n = M::num_states;
+    Acc<T> y[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+        y[i].load(rows[i * stride]);
+    T F[Dims<M>::nfp];
+#pragma unroll
+    for (int k = 0; k < Dims<M>::nfp; ++k)
+        F[k] = (k < M::num_field_params) ? T(rows[(n + k) * stride]) : T(0);
+    explicit_node_core<M, T, S>(a, node, P, PD, y, F);
 }
 
 template <class M, typename T, Explicit S>

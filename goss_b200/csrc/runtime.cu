@@ -571,8 +571,9 @@ GOSS_API int goss_batch_set_config(goss_batch* b, uint32_t block, uint32_t grid,
         return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL batch");
     if (block && (block % 32 || block > 128))
         return batch_fail(b, GOSS_ERR_ARGUMENT, "block must be a multiple of 32 and at most 128");
-    if (schedule > 1)
-        return batch_fail(b, GOSS_ERR_ARGUMENT, "schedule must be 0 (round-robin) or 1 (dynamic)");
+    if (schedule > 2)
+        return batch_fail(b, GOSS_ERR_ARGUMENT,
+                          "schedule must be 0 (round-robin), 1 (dynamic) or 2 (persistent with prefetch)");
     if (order) {
         std::vector<uint32_t> o(order, order + b->systems.size());
         std::vector<uint32_t> s(o);

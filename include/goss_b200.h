@@ -217,7 +217,9 @@ typedef struct goss_batch_launch {
     const uint32_t* order;   /* tile order of the populations (NULL: as given) */
     uint32_t block;          /* nodes per tile = threads per block */
     uint32_t grid;           /* persistent grid size (0: one block per tile) */
-    uint32_t schedule;       /* 0: round-robin tiles, 1: tiles claimed from an atomic counter */
+    uint32_t schedule;       /* 0: round-robin tiles, 1: tiles claimed from an atomic counter,
+                                2: persistent CTAs staging the next tile's rows in shared memory
+                                   with bulk asynchronous copies (grid 0: all resident CTAs) */
     uint32_t* counters;      /* device [2], zero before the first launch */
     double t;
     double interval;

@@ -67,11 +67,17 @@ def test_batch_matches_separate_systems(precision):
         assert parity(p.states, r.states, rtol=tol, atol=1e-12) <= 1.0
 
 
-def test_schedules_and_orders_give_identical_results():
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_schedules_and_orders_give_identical_results(precision):
+    """Round-robin, atomic-counter and prefetching (rows staged in shared memory
+    by bulk copies; populations of 3 and other odd-tile counts) schedules run
+    the same arithmetic on the same values: bit-identical states."""
     results = []
     for cfg in (dict(block=128, grid=0, schedule=0), dict(block=64, grid=296, schedule=1, order=[5, 4, 3, 2, 1, 0]),
-                dict(block=128, grid=148, schedule=0, order=[3, 1, 0, 2, 5, 4])):
-        pops = make_pops()
+                dict(block=128, grid=148, schedule=0, order=[3, 1, 0, 2, 5, 4]),
+                dict(block=64, grid=0, schedule=2), dict(block=128, grid=0, schedule=2, order=[3, 1, 0, 2, 5, 4]),
+                dict(block=96, grid=7, schedule=2)):
+        pops = make_pops(precision)
         batch = goss.BatchSolver(pops)
         batch.set_config(**cfg)
         for k in range(5):
