@@ -505,7 +505,11 @@ def run_coupled(dev, steps=200, pde_dt=0.1):
 
 
 IMPLICIT_MODEL, IMPLICIT_FIELDS, IMPLICIT_NODES, IMPLICIT_DT = "tentusscher_2004_mcell", ["g_Kr", "g_CaL"], 262_144, 0.1
-IMPLICIT_SOLVERS = [("ThetaSolver", 0.1, 10), ("ESDIRK23a", -1.0, 2)]  # solver, internal step, timed intervals
+# label, solver, internal step, timed intervals, analytic Jacobian (code_params generate_jacobian)
+IMPLICIT_SOLVERS = [("ThetaSolver", "ThetaSolver", 0.1, 10, False), ("ESDIRK23a", "ESDIRK23a", -1.0, 2, False),
+                    ("ThetaSolver+jacobian", "ThetaSolver", 0.1, 20, True),
+                    ("ImplicitEuler+jacobian", "ImplicitEuler", 0.1, 20, True),
+                    ("ESDIRK23a+jacobian", "ESDIRK23a", -1.0, 4, True)]
 
 
 def implicit_inputs(nodes):
@@ -534,10 +538,12 @@ def run_implicit(dev):
     import goss_b200 as goss
 
     md, y0, fp = implicit_inputs(IMPLICIT_NODES)
-    ode = goss.ParameterizedODE(IMPLICIT_MODEL, field_parameters=IMPLICIT_FIELDS)
+    odes = {jac: goss.ParameterizedODE(IMPLICIT_MODEL, field_parameters=IMPLICIT_FIELDS,
+                                       code_params={"generate_jacobian": jac}) for jac in (False, True)}
     stream = torch.cuda.current_stream(dev)
     out = {}
-    for name, ldt, intervals in IMPLICIT_SOLVERS:
+    for label, name, ldt, intervals, jac in IMPLICIT_SOLVERS:
+        ode = odes[jac]
         solver = goss.solvers.solver_mapper[name](ode)
         solver.internal_time_step = ldt
         system = goss.ODESystemSolver(IMPLICIT_NODES, solver, ode, device=dev)
@@ -557,7 +563,7 @@ def run_implicit(dev):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         jac, rej, acc = system.counters()
-        out[name] = {"value": IMPLICIT_NODES * intervals / (ms / 1e3), "unit": "node-intervals/s",
+        out[label] = {"value": IMPLICIT_NODES * intervals / (ms / 1e3), "unit": "node-intervals/s",
                      "ms_per_interval": ms / intervals, "intervals": intervals, "internal_time_step": ldt,
                      "jacobians_per_node_interval": float(np.mean(jac)) / (intervals + 1),
                      "rejected_per_node_interval": float(np.mean(rej)) / (intervals + 1),
@@ -574,14 +580,14 @@ def implicit_reference_sample(target_s=6.0):
     import pyoracle
     from goss_b200 import models
 
-    vdir = models.find_variant(IMPLICIT_MODEL, IMPLICIT_FIELDS)
-    md = json.loads((vdir / "model.json").read_text())
     threads = cpu_threads()
-    om = pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
-    plugin = pyoracle.REFDIR / vdir.name / "libplugin.so"
-    kind = "reference" if pyoracle.ref_available() and plugin.exists() else "port"
     out = {}
-    for name, ldt, _ in IMPLICIT_SOLVERS:
+    for label, name, ldt, _, jac in IMPLICIT_SOLVERS:
+        vdir = models.find_variant(IMPLICIT_MODEL, IMPLICIT_FIELDS, jacobian=jac)
+        md = json.loads((vdir / "model.json").read_text())
+        om = pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
+        plugin = pyoracle.REFDIR / vdir.name / "libplugin.so"
+        kind = "reference" if pyoracle.ref_available() and plugin.exists() else "port"
         nodes = threads * 4
         for attempt in range(2):
             _, y0, fp = implicit_inputs(nodes)
@@ -603,7 +609,7 @@ def implicit_reference_sample(target_s=6.0):
             if attempt == 0:
                 nodes = int(min(max(nodes * target_s / max(dt, 1e-6), nodes), IMPLICIT_NODES))
                 nodes = max(threads, nodes // threads * threads)
-        out[name] = {"value": nodes / dt, "unit": "node-intervals/s", "kind": kind, "cores": threads,
+        out[label] = {"value": nodes / dt, "unit": "node-intervals/s", "kind": kind, "cores": threads,
                      "sample": f"{nodes} nodes x one 0.1 ms interval after one untimed interval, {dt:.1f} s"}
     return out
 

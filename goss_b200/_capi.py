@@ -12,7 +12,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 RUNTIME_SO = PKG / "_lib" / "libgoss_b200.so"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 (GOSS_EXPLICIT_EULER, GOSS_RK4, GOSS_GRL1, GOSS_GRL2, GOSS_THETA, GOSS_ESDIRK23A, GOSS_RL1, GOSS_RL2, GOSS_RK2,
  GOSS_IMPLICIT_EULER) = range(10)
@@ -84,6 +84,8 @@ class ModelDesc(C.Structure):
         ("op_census_linearized", C.POINTER(C.c_uint32)),
         ("op_census_rhs", C.POINTER(C.c_uint32)),
         ("adjoint", C.c_void_p),
+        ("has_jacobian", C.c_uint32),
+        ("lu_nnz", C.c_uint32),
     ]
 
 

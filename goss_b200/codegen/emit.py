@@ -29,6 +29,7 @@ from .ad import ReverseProgram
 from .factor import factor_common
 from .hoist import ConstantFolder
 from .printer import CPrinter, c_double
+from .sparse import LUStructure
 
 _RESERVED = {
     "auto", "break", "case", "char", "const", "continue", "default", "do", "double", "else", "enum",
@@ -79,7 +80,7 @@ def _body_lines(prog: Program, pr_for, decl_for, out_for, split_code: List[str] 
 class ModelSource:
     """Bundle of everything generated for one model + field-parameter set."""
 
-    def __init__(self, ir: ModelIR, name: str = None):
+    def __init__(self, ir: ModelIR, name: str = None, jacobian: bool = False):
         self.ir = ir
         self.model = ir.model
         self.name = name or self.model.name
@@ -88,6 +89,9 @@ class ModelSource:
         self.lin = ir.linearized_program(split=True)
         self.linear_terms = ir.linear_terms()
         self.mon = ir.monitored_program() if ir.monitored else None
+        # analytic Jacobian (the reference's code_params["generate_jacobian"])
+        self.jac = ir.jacobian_program() if jacobian else None
+        self.lus = LUStructure(ir.jacobian_structure())
         self.params = list(self.model.parameters)
         self.states = list(self.model.states)
         self.pindex = {p: i for i, p in enumerate(self.params)}
@@ -114,7 +118,11 @@ class ModelSource:
             linear_terms=self.linear_terms,
             intermediate_names=list(self.model.intermediates),
             op_census=dict(rhs=count_ops(self.rhs), linearized=count_ops(self.ir.linearized_program(split=False)),
-                           linearized_split=self._split_census()),
+                           linearized_split=self._split_census(),
+                           **({"jacobian": count_ops(self.jac)} if self.jac is not None else {})),
+            jacobian=self.jac is not None,
+            jacobian_structure=[[int(v) for v in row] for row in self.lus.jac],
+            lu_nnz=self.lus.nnz,
         )
 
     def _split_census(self) -> Dict[str, int]:
@@ -179,6 +187,13 @@ class ModelSource:
                                              split_code=["if (only_linear) return;"])]
         L.append("}")
         L.append("")
+        if self.jac is not None:
+            L.append(f"static void {m}_jacobian(const double* states, double time, const double* params, double* jac)")
+            L.append("{")
+            L += ["  " + x for x in self._c_head()]
+            L += ["  " + x for x in _body_lines(self.jac, lambda c: pr, decl, out)]
+            L.append("}")
+            L.append("")
         if self.mon is not None:
             L.append(f"static void {m}_monitored(const double* states, double time, const double* params, double* monitored)")
             L.append("{")
@@ -208,6 +223,7 @@ class ModelSource:
         L.append(f"  model.ic = {m}_ic;")
         L.append(f"  model.default_params = {m}_defaults;")
         L.append(f"  model.linear_terms = {m}_linear_terms;")
+        L.append(f"  model.jacobian = {m + '_jacobian' if self.jac is not None else '0'};")
         L.append("  return &model;")
         L.append("}")
         return "\n".join(L) + "\n"
@@ -281,6 +297,13 @@ class ModelSource:
                                                   split_code=["if (only_linear) return;"])]
         L.append("    }")
         L.append("")
+        if self.jac is not None:
+            L.append("    // Compute analytic jacobian")
+            L.append("    void compute_jacobian(double* states, double time, double* jac)")
+            L.append("    {")
+            L += [I(8) + x for x in head + _body_lines(self.jac, lambda c: pr, decl, out)]
+            L.append("    }")
+            L.append("")
         L.append("    void get_ic(goss::DoubleVector* values) const")
         L.append("    {")
         L.append("        values->n = _num_states;")
@@ -369,6 +392,9 @@ class ModelSource:
             return CPrinter(sym, fn=fn, lit=lit, exp2_fold=split and not ctx_double)
         return make(False), make(True)
 
+    def _programs(self) -> Tuple[Program, ...]:
+        return (self.rhs, self.lin) + ((self.mon,) if self.mon else ()) + ((self.jac,) if self.jac else ())
+
     def _cls_of(self, name: str) -> int:
         return self._cls_map.get(name, STATE)
 
@@ -376,7 +402,7 @@ class ModelSource:
     def _cls_map(self) -> Dict[str, int]:
         if not hasattr(self, "_cls_cache"):
             d = {}
-            for prog in (self.rhs, self.lin) + ((self.mon,) if self.mon else ()):
+            for prog in self._programs():
                 for b in prog.assigns():
                     d[b.name] = b.cls
             self._cls_cache = d
@@ -399,7 +425,7 @@ class ModelSource:
         if not hasattr(self, "_folder"):
             uniform = {self.model.sym(p) for p in self.params if p not in self.findex}
             const_inter = {}
-            for prog in (self.rhs, self.lin) + ((self.mon,) if self.mon else ()):
+            for prog in self._programs():
                 for b in prog.assigns():
                     if b.cls == CONST:
                         const_inter[self.model.sym(b.name)] = b.expr
@@ -454,11 +480,28 @@ class ModelSource:
             lines.append(f"Fbar[{k}] = {prT(factor_common(e)) if e != 0 else 'T(0.0)'};")
         return lines
 
-    def _dev_split_lines(self, prog: Program, arrays: Dict[str, str]) -> List[str]:
+    def _packed_jacobian(self) -> Program:
+        """The analytic Jacobian program with its outputs at the packed
+        positions of the LU structure (entries outside it are exactly 0)."""
+        n = len(self.states)
+        body = []
+        for b in self.jac.body:
+            if isinstance(b, Output):
+                r, c = divmod(b.index, n)
+                if self.lus.nz(r, c):
+                    body.append(Output("jac", self.lus.pos[(r, c)], b.expr))
+                elif b.expr != 0:
+                    raise AssertionError(f"jac[{r}][{c}] outside the dependency structure")
+            else:
+                body.append(b)
+        return Program("jacobian_packed", body, None)
+
+    def _dev_split_lines(self, prog: Program, arrays: Dict[str, str], size: int = None) -> List[str]:
         """Body of ``prog`` with every distinct exp/log/sqrt/pow/reciprocal of
         state-dependent operands computed once (the elementary split of
         codegen/ad.py) and common factors pulled out of sums (codegen/factor.py);
-        ``arrays`` names the output array of each of its output arrays."""
+        ``arrays`` names the output array of each of its output arrays, each of
+        ``size`` entries (default: the number of states)."""
         folded = self._fold(prog)
         inter = {n: self.model.sym(n) for n in self.model.intermediates}
         rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
@@ -470,7 +513,7 @@ class ModelSource:
                 lines.append(f"const double v_{b.name} = {prD(b.expr)};")
             else:
                 lines.append(f"const T v_{b.name} = {prT(factor_common(b.expr))};")
-        n = len(self.states)
+        n = len(self.states) if size is None else size
         for o in rp.outputs:
             lines.append(f"{arrays[o.array]}[{o.index}] = {prT(factor_common(o.expr))};")
         for arr, name in arrays.items():
@@ -488,8 +531,7 @@ class ModelSource:
             return f"v_{n}"
         pr = CPrinter(sym)
         lines = []
-        order = [b for prog in (self.rhs, self.lin) + ((self.mon,) if self.mon else ())
-                 for b in prog.assigns() if b.cls == CONST]
+        order = [b for prog in self._programs() for b in prog.assigns() if b.cls == CONST]
         seen = set()
         for b in order:
             if b.name in seen:
@@ -538,6 +580,8 @@ class ModelSource:
         rhs_lines = self._dev_body(self.rhs)
         lin_lines = self._dev_body(lin_full)
         mon_lines = self._dev_body(self.mon) if self.mon is not None else []
+        jac_lines = (self._dev_split_lines(self._packed_jacobian(), {"jac": "J"}, self.lus.nnz)
+                     if self.jac is not None else [])
         nder = len(self.folder.derived)
         L.insert(L.index(f"  static constexpr int num_monitored = {len(self.ir.monitored)};") + 1,
                  f"  static constexpr int num_derived = {nder};")
@@ -546,6 +590,7 @@ class ModelSource:
         L.insert(L.index(f"  static constexpr int num_derived = {nder};") + 1,
                  "  // the reference generator's linear-term flags (RL1/RL2 use the exponential update for these)\n"
                  f"  __host__ __device__ static constexpr bool linear_term(int i) {{ return {cond}; }}")
+        L += self._dev_lu_lines(head, sig, jac_lines)
         L.append("  // derived constants: parameter-only sub-expressions, evaluated once per")
         L.append("  // launch on the host in FP64 and stored after the parameters")
         L.append("  static void derived(const double* P, double* C)")
@@ -615,6 +660,76 @@ class ModelSource:
         L.append("}}  // namespace goss_b200::models")
         L.append("#endif")
         return "\n".join(L) + "\n"
+
+    def _dev_lu_lines(self, head: List[str], sig: str, jac_lines: List[str]) -> List[str]:
+        """Packed Newton matrix of the implicit solvers: the LU structure of
+        I - h*alpha*J, the structure-aware factorisation and solve
+        (codegen/sparse.py), the forward-difference column store and, with the
+        analytic Jacobian, its evaluation into the packed layout."""
+        lus, n = self.lus, len(self.states)
+        I4 = lambda lines: ["    " + x for x in lines]
+        L = []
+        L.append(f"  // Newton matrix: {lus.nnz} packed entries (the Jacobian's {sum(map(sum, lus.jac))} structural")
+        L.append("  // non-zeros, the diagonal and the LU fill-in; row-major over the structure)")
+        L.append(f"  static constexpr int lu_nnz = {lus.nnz};")
+        L.append(f"  static constexpr bool has_jacobian = {'true' if self.jac is not None else 'false'};")
+        L.append("  // J := scale*J + I")
+        L.append("  template <class A>")
+        L.append("  __device__ static __forceinline__ void lu_shift(A J, const double scale)")
+        L.append("  {")
+        L += I4(lus.shift_lines("J", "scale"))
+        L.append("  }")
+        L.append("  // D := scale*S + I")
+        L.append("  template <class A, class B>")
+        L.append("  __device__ static __forceinline__ void lu_copy_shift(A S, B D, const double scale)")
+        L.append("  {")
+        L += I4(lus.copy_shift_lines("S", "D", "scale"))
+        L.append("  }")
+        L.append("  // in-place Doolittle LU without pivoting over the structure")
+        L.append("  template <class A>")
+        L.append("  __device__ static __forceinline__ void lu_factorize(A J)")
+        L.append("  {")
+        L += I4(lus.lu_factorize_lines("J"))
+        L.append("  }")
+        L.append("  // x = (LU)^-1 b, forward then backward substitution; b and x may alias")
+        L.append("  template <class A>")
+        L.append("  __device__ static __forceinline__ void lu_solve(A J, const double* b, double* x)")
+        L.append("  {")
+        L += I4(lus.solve_lines("J", "b", "x"))
+        L.append("  }")
+        L.append("  // forward differences: zero the entries outside the Jacobian's structure, then")
+        L.append("  // column i = (f2 - f1) / delta at its structural rows")
+        L.append("  template <class A>")
+        L.append("  __device__ static __forceinline__ void fd_clear(A J)")
+        L.append("  {")
+        L += I4(lus.clear_extra_lines("J"))
+        L.append("    (void)J;")
+        L.append("  }")
+        L.append("  template <class A>")
+        L.append("  __device__ static __forceinline__ void fd_column(const int i, const double* f1, const double* f2,")
+        L.append("                                                   const double delta, A J)")
+        L.append("  {")
+        L += I4(lus.fd_column_lines("J"))
+        L.append("  }")
+        L.append("  // dense row-major copy: out(r*n + c, value) for every entry")
+        L.append("  template <typename T, class Out>")
+        L.append("  __device__ static __forceinline__ void lu_unpack(const T* J, Out&& out)")
+        L.append("  {")
+        for r in range(n):
+            for c in range(n):
+                L.append(f"    out({r * n + c}, {f'J[{lus.pos[(r, c)]}]' if lus.nz(r, c) else 'T(0.0)'});")
+        L.append("  }")
+        if self.jac is not None:
+            L.append("  // analytic Jacobian d f_i / d y_j (every path through the intermediates once)")
+            L.append("  // into the packed layout, in the split form")
+            L.append("  template <typename T, class A>")
+            L.append(f"  __device__ static __forceinline__ void jacobian({sig}, A J)")
+            L.append("  {")
+            L += I4(head + jac_lines)
+            L.append("    (void)time; (void)P; (void)PD; (void)F;")
+            L.append("  }")
+        L.append("")
+        return L
 
     def metadata_json(self) -> str:
         return json.dumps(self.metadata(), indent=1)

@@ -353,6 +353,44 @@ class ModelIR:
             prog.split = None
         return prog
 
+    def jacobian_structure(self) -> List[List[bool]]:
+        """``S[i][j]``: f_i depends on y_j through its expression or any
+        intermediate it uses (a superset of the non-zero Jacobian entries; an
+        entry outside it is exactly 0 in a forward-difference Jacobian too,
+        since f_i is then computed from the same operands)."""
+        out = []
+        for e in self.model.derivatives.values():
+            deps = self._expr_state_deps(e)
+            out.append([y in deps for y in self.state_syms])
+        return out
+
+    def jacobian_program(self) -> Program:
+        """``compute_jacobian(states, time, jac)`` body: ``jac[i*n + j] =
+        d f_i / d y_j`` through every intermediate, each path counted once,
+        every entry written (zeros too).
+
+        The reference generates this override of ``ODE::compute_jacobian``
+        (``cpp/goss/ODE.h:71``) when ``code_params["generate_jacobian"]`` is
+        set (``python/goss/codegeneration.py:622-641``; gotran's
+        ``jacobian_expressions``).  The derivatives here are exact whatever
+        the linearisation rule of the diagonal in ``linearized``."""
+        ex = self if self.linearization == "exact" else ModelIR(
+            self.model, self.field_parameters, self.field_states, self.monitored, linearization="exact")
+        m = self.model
+        rhs = list(m.derivatives.values())
+        n = len(self.state_syms)
+        entries = [[ex.total_derivative(e, y) for y in self.state_syms] for e in rhs]
+        roots = [d for row in entries for d in row]
+        prog = Program("jacobian")
+        for s in ex._needed_intermediates(roots + [ex._dassigns[s] for s in ex._deriv_assign_order(roots)]):
+            prog.body.append(Assign(s.name, ex.inter_exprs[s], ex._cls[s]))
+        for s in ex._deriv_assign_order(roots):
+            prog.body.append(Assign(s.name, ex._dassigns[s], STATE))
+        for i in range(n):
+            for j in range(n):
+                prog.body.append(Output("jac", i * n + j, entries[i][j]))
+        return prog
+
     def monitored_program(self) -> Program:
         prog = Program("monitored")
         exprs = [self.inter_syms[k] for k in self.monitored]

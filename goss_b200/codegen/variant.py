@@ -2,8 +2,9 @@
 
 A *variant* is one ``.ode`` model combined with the code-generation choices
 that change the compiled code: the field parameters (read per node instead of
-from the uniform parameter block), the monitored intermediates and the
-linearisation rule.  Its directory holds
+from the uniform parameter block), the monitored intermediates, the
+linearisation rule and whether the analytic Jacobian is generated (the
+reference's ``code_params["generate_jacobian"]``).  Its directory holds
 
 ``model.json``        names, defaults, linear-term flags, op census
 ``device.cuh``        CUDA ``__device__`` model (templated on T)
@@ -27,25 +28,30 @@ from .emit import ModelSource, c_ident, model_class_name
 from .ir import ModelIR
 from .odeparse import ODEModel
 
-GENERATOR_VERSION = "1"
+GENERATOR_VERSION = "2"
 
 _CENSUS_KEYS = ("add", "mul", "div", "exp", "log", "sqrt", "pow", "cmp", "misc")
 
 
+def _key(field_parameters, monitored, linearization, jacobian) -> list:
+    key = [list(field_parameters), list(monitored), linearization]
+    return key + [{"jacobian": True}] if jacobian else key
+
+
 def variant_id(model: ODEModel, field_parameters: Sequence[str] = (), monitored: Sequence[str] = (),
-               linearization: str = "gotran") -> str:
+               linearization: str = "gotran", jacobian: bool = False) -> str:
     base = c_ident(model.name)
-    if not field_parameters and not monitored and linearization == "gotran":
+    if not field_parameters and not monitored and linearization == "gotran" and not jacobian:
         return base
-    key = json.dumps([list(field_parameters), list(monitored), linearization])
+    key = json.dumps(_key(field_parameters, monitored, linearization, jacobian))
     return f"{base}__{hashlib.sha1(key.encode()).hexdigest()[:8]}"
 
 
-def model_hash(model: ODEModel, field_parameters, monitored, linearization) -> str:
+def model_hash(model: ODEModel, field_parameters, monitored, linearization, jacobian: bool = False) -> str:
     h = hashlib.sha1()
     h.update(GENERATOR_VERSION.encode())
     h.update(model.signature().encode())
-    h.update(json.dumps([list(field_parameters), list(monitored), linearization]).encode())
+    h.update(json.dumps(_key(field_parameters, monitored, linearization, jacobian)).encode())
     return h.hexdigest()
 
 
@@ -107,6 +113,7 @@ def emit_module(src: ModelSource, ident: str) -> str:
         "        initial_conditions, default_parameters, linear_terms,",
         "        (1u << GOSS_NUM_SOLVERS) - 1u,",
         "        launch, eval, rows, op_lin, op_rhs, adjoint,",
+        f"        {1 if md['jacobian'] else 0}u, {md['lu_nnz']}u,",
         "    };",
         "    return &d;",
         "}",
@@ -116,16 +123,16 @@ def emit_module(src: ModelSource, ident: str) -> str:
 
 def write_variant(model: ODEModel, outdir: Path, field_parameters: Sequence[str] = (),
                   monitored: Sequence[str] = (), linearization: str = "gotran",
-                  ident: Optional[str] = None) -> Dict:
+                  ident: Optional[str] = None, jacobian: bool = False) -> Dict:
     """Write all generated sources of a variant into ``outdir``."""
-    ident = ident or variant_id(model, field_parameters, monitored, linearization)
+    ident = ident or variant_id(model, field_parameters, monitored, linearization, jacobian)
     ir = ModelIR(model, field_parameters=field_parameters, monitored=monitored, linearization=linearization)
-    src = ModelSource(ir)
+    src = ModelSource(ir, jacobian=jacobian)
     outdir = Path(outdir)
     outdir.mkdir(parents=True, exist_ok=True)
     md = src.metadata()
     md.update(variant=ident, linearization=linearization,
-              hash=model_hash(model, field_parameters, monitored, linearization),
+              hash=model_hash(model, field_parameters, monitored, linearization, jacobian),
               generator_version=GENERATOR_VERSION, class_name=model_class_name(model.name))
     files = {
         "device.cuh": src.emit_device(device_struct(ident)),

@@ -403,61 +403,17 @@ __global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ E
 // ---------------------------------------------------------------------------
 // dense linear algebra on one node's n x n matrix
 // ---------------------------------------------------------------------------
-// Matrix accessors: thread-local array or a node's slice of a component-major
-// global array (element (r, c) of node at base[(r*n + c)*ld + node]).
-template <int n>
-struct LocalMat {
-    double* m;
-    __device__ __forceinline__ double& operator()(int r, int c) const { return m[r * n + c]; }
-};
-template <int n>
-struct GlobalMat {
+// Newton matrices of the implicit solvers are stored packed (the model's
+// lu_nnz entries of the LU structure of I - h*alpha*J, generated with the
+// structure-aware factorisation and solve that reproduce ODE::lu_factorize and
+// ODE::forward_backward_subst, ODE.cpp:69-132): in a thread-local array, or in
+// a node's slice of component-major solver-state rows (entry k of the node at
+// base[k*ld + node]).
+struct PackedRows {
     double* base;
     uint64_t ld;
-    __device__ __forceinline__ double& operator()(int r, int c) const { return base[(uint64_t)(r * n + c) * ld]; }
+    __device__ __forceinline__ double& operator[](int k) const { return base[(uint64_t)k * ld]; }
 };
-
-// ODE::lu_factorize (ODE.cpp:69-100): Doolittle, no pivoting
-template <int n, class Mat>
-__device__ void lu_factorize(const Mat& A)
-{
-    for (int k = 1; k < n; k++) {
-        for (int i = 0; i <= k - 1; ++i) {
-            double sum = 0.0;
-            for (int r = 0; r <= i - 1; r++)
-                sum += A(i, r) * A(r, k);
-            A(i, k) -= sum;
-            sum = 0.0;
-            for (int r = 0; r <= i - 1; r++)
-                sum += A(k, r) * A(r, i);
-            A(k, i) = (A(k, i) - sum) / A(i, i);
-        }
-        double sum = 0.0;
-        for (int r = 0; r <= k - 1; r++)
-            sum += A(k, r) * A(r, k);
-        A(k, k) -= sum;
-    }
-}
-
-// ODE::forward_backward_subst (ODE.cpp:102-132); b and dx may alias
-template <int n, class Mat>
-__device__ void forward_backward_subst(const Mat& A, const double* b, double* dx)
-{
-    dx[0] = b[0];
-    for (int i = 1; i < n; ++i) {
-        double sum = 0.0;
-        for (int j = 0; j <= i - 1; ++j)
-            sum = sum + A(i, j) * dx[j];
-        dx[i] = b[i] - sum;
-    }
-    dx[n - 1] = dx[n - 1] / A(n - 1, n - 1);
-    for (int i = n - 2; i >= 0; i--) {
-        double sum = 0;
-        for (int j = i + 1; j < n; ++j)
-            sum = sum + A(i, j) * dx[j];
-        dx[i] = (dx[i] - sum) / A(i, i);
-    }
-}
 
 template <int n>
 __device__ __forceinline__ double l2norm(const double* v)
@@ -485,33 +441,40 @@ __device__ __forceinline__ void rhs64(const double* y, double t, const double* P
         M::template rhs<double>(y, t, P, P, F, out);
 }
 
-// ODE::compute_jacobian (ODE.cpp:47-67) into any matrix accessor: column i is
+// ODE::compute_jacobian (ODE.cpp:47-67) into the packed Newton matrix J:
+// the model's analytic Jacobian when it was generated with one (the
+// reference's generated override), else forward differences: column i is
 // (f(y + delta_i e_i) - f(y)) / delta_i with delta_i = sqrt(1e-15 max(1e-5, |y_i|)),
 // f1 = f(y, t) supplied by the caller (the reference evaluates it first with
-// the same arguments).  The perturbed state is built by selects over
-// compile-time indices, so y stays in registers (the reference perturbs y[i]
-// in place and restores it: the same values).
-template <class M, class Mat>
-__device__ void compute_jacobian(const double* y, double t, const double* P, const double* F, const Mat& J,
+// the same arguments), stored at the column's structural rows (the other
+// rows are exactly 0 in the reference too).  The perturbed state is built by
+// selects over compile-time indices, so y stays in registers (the reference
+// perturbs y[i] in place and restores it: the same values).
+template <class M, class A>
+__device__ void compute_jacobian(const double* y, double t, const double* P, const double* F, A J,
                                  const double* f1)
 {
     constexpr int n = M::num_states;
+    if constexpr (M::has_jacobian) {
+        (void)f1;
+        M::template jacobian<double>(y, t, P, P, F, J);
+    } else {
+        M::fd_clear(J);
 #pragma unroll 1
-    for (int i = 0; i < n; ++i) {
-        double ysafe = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double ysafe = 0.0;
 #pragma unroll
-        for (int k = 0; k < n; ++k)
-            ysafe = (k == i) ? y[k] : ysafe;
-        const double max = 1e-5 > fabs(ysafe) ? 1e-5 : fabs(ysafe);
-        const double delta = sqrt(1e-15 * max);
-        double yp[n], f2[n];
+            for (int k = 0; k < n; ++k)
+                ysafe = (k == i) ? y[k] : ysafe;
+            const double max = 1e-5 > fabs(ysafe) ? 1e-5 : fabs(ysafe);
+            const double delta = sqrt(1e-15 * max);
+            double yp[n], f2[n];
 #pragma unroll
-        for (int k = 0; k < n; ++k)
-            yp[k] = (k == i) ? ysafe + delta : y[k];
-        rhs64<M>(yp, t, P, F, f2);
-#pragma unroll
-        for (int j = 0; j < n; ++j)
-            J(j, i) = (f2[j] - f1[j]) / delta;
+            for (int k = 0; k < n; ++k)
+                yp[k] = (k == i) ? ysafe + delta : y[k];
+            rhs64<M>(yp, t, P, F, f2);
+            M::fd_column(i, f1, f2, delta, J);
+        }
     }
 }
 
@@ -535,8 +498,7 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
         return;
     const goss_solver_params& sp = a.sp;
     double y[n], z1[n], prev[n], ft1[n], yz[n], f1[n], b[n], dz[n];
-    double Jm[n * n];
-    const LocalMat<n> J{Jm};
+    double J[M::lu_nnz];
 #pragma unroll
     for (int i = 0; i < n; ++i)
         y[i] = a.states[i * a.ld + node];
@@ -554,8 +516,9 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
     // in every forward): it lives in the solver-state rows after the scalars
     double* const jrows = ss + (uint64_t)TH_ROWS * ld;
     if constexpr (IE) {
-        for (int k = 0; k < n * n; ++k)
-            Jm[k] = jrows[(uint64_t)k * ld];
+#pragma unroll
+        for (int k = 0; k < M::lu_nnz; ++k)
+            J[k] = jrows[(uint64_t)k * ld];
     }
 
     double t = a.t;
@@ -603,17 +566,12 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
             if (recompute || always) {
                 // compute_factorized_jacobian (ImplicitODESolver.cpp:92-105)
                 compute_jacobian<M>(yz, tn, a.P, F, J, f1);  // f1 = f(yz, tn) from the residual
-                const double scale = -ldt * alpha;
-                for (int i = 0; i < n; ++i)
-                    for (int j = 0; j < n; ++j)
-                        J(i, j) *= scale;
-                for (int i = 0; i < n; ++i)
-                    J(i, i) += 1.0 * 1.0;
-                lu_factorize<n>(J);
+                M::lu_shift(J, -ldt * alpha);
+                M::lu_factorize(J);
                 jac_comp += 1;
                 recompute = 0;
             }
-            forward_backward_subst<n>(J, b, dz);
+            M::lu_solve(J, b, dz);
             if (newton_iterations == 0) {
                 initial_residual = residual;
                 eta = eta > kGossEps ? eta : kGossEps;
@@ -684,8 +642,9 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
     if (!finite)
         status |= GOSS_FLAG_NONFINITE;
     if constexpr (IE) {
-        for (int k = 0; k < n * n; ++k)
-            jrows[(uint64_t)k * ld] = Jm[k];
+#pragma unroll
+        for (int k = 0; k < M::lu_nnz; ++k)
+            jrows[(uint64_t)k * ld] = J[k];
     }
     ss[TH_ETA * ld] = eta;
     ss[TH_RECOMPUTE * ld] = recompute;
@@ -705,7 +664,7 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
 // ---------------------------------------------------------------------------
 enum EsdirkRows {
     ES_PREV_DT = 0, ES_LOC_ERROR, ES_ETA, ES_NEWTON_IT, ES_FIRST, ES_NEWJAC, ES_JACCOMP, ES_REJECTS, ES_ACCEPTED,
-    ES_SCALARS  // jac[n*n] and jfac[n*n] follow
+    ES_SCALARS  // the packed jac[lu_nnz] and jfac[lu_nnz] follow
 };
 
 struct EsdirkCoef {
@@ -752,7 +711,7 @@ struct EsdirkNode {
     const double* F;
     const goss_solver_params* sp;
     EsdirkCoef c;
-    GlobalMat<n> jac, jfac;
+    PackedRows jac, jfac;
     double prev_dt, loc_error, eta, dt;
     int newton_iterations, first_step, new_jacobian;
     double jac_comp, rejects, accepted;
@@ -770,13 +729,8 @@ struct EsdirkNode {
     // ESDIRK23a::compute_factorized_jacobian(dt) (ESDIRK23a.cpp:101-115)
     __device__ void factorize(double h)
     {
-        const double scale = -h * c.a22;
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j)
-                jfac(i, j) = jac(i, j) * scale;
-        for (int i = 0; i < n; ++i)
-            jfac(i, i) += 1.0 * 1.0;
-        lu_factorize<n>(jfac);
+        M::lu_copy_shift(jac, jfac, -h * c.a22);
+        M::lu_factorize(jfac);
     }
     // ESDIRK23a::compute_stage_val (ESDIRK23a.cpp:201-258)
     __device__ bool stage(double* z, const double* y, double t_s, double h)
@@ -795,7 +749,7 @@ struct EsdirkNode {
                 b[i] = -z[i] + z_int[i];
             for (int i = 0; i < n; i++)
                 prev_dz[i] = dz[i];
-            forward_backward_subst<n>(jfac, b, dz);
+            M::lu_solve(jfac, b, dz);
             if (newton_iterations >= 1) {
                 const double theta = l2norm<n>(dz) / l2norm<n>(prev_dz);
                 if (!(theta <= 1)) {
@@ -843,7 +797,7 @@ struct EsdirkNode {
             for (int i = 0; i < n; i++)
                 yh[i] = h * ((c.b1 - c.bh1) * z1[i] + (c.b2 - c.bh2) * z2[i] + (c.b3 - c.gamma) * z3[i] +
                              c.gamma * z4[i]);
-            forward_backward_subst<n>(jfac, yh, yh);
+            M::lu_solve(jfac, yh, yh);
             loc_error = l2norm<n>(yh);
             if (loc_error > c.tol) {
                 rejects += 1;
@@ -902,8 +856,8 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
     s.F = F;
     s.sp = &a.sp;
     s.c = esdirk_coefficients();
-    s.jac = GlobalMat<n>{ss + (uint64_t)ES_SCALARS * ld, ld};
-    s.jfac = GlobalMat<n>{ss + (uint64_t)(ES_SCALARS + n * n) * ld, ld};
+    s.jac = PackedRows{ss + (uint64_t)ES_SCALARS * ld, ld};
+    s.jfac = PackedRows{ss + (uint64_t)(ES_SCALARS + M::lu_nnz) * ld, ld};
     s.prev_dt = ss[ES_PREV_DT * ld];
     s.loc_error = ss[ES_LOC_ERROR * ld];
     s.eta = ss[ES_ETA * ld];
@@ -991,11 +945,17 @@ __global__ void __launch_bounds__(128) eval_kernel(const __grid_constant__ EvalA
             a.out[i * a.ld + node] = double(o1[i]);
             a.out[(n + i) * a.ld + node] = double(o2[i]);
         }
-    } else if constexpr (M::num_monitored > 0) {
-        T mon[M::num_monitored];
-        M::template monitored_values<T>(y, t, a.P, a.PD, F, mon);
-        for (int i = 0; i < M::num_monitored; ++i)
-            a.out[i * a.ld + node] = double(mon[i]);
+    } else if (a.what == 2) {
+        if constexpr (M::num_monitored > 0) {
+            T mon[M::num_monitored];
+            M::template monitored_values<T>(y, t, a.P, a.PD, F, mon);
+            for (int i = 0; i < M::num_monitored; ++i)
+                a.out[i * a.ld + node] = double(mon[i]);
+        }
+    } else if constexpr (M::has_jacobian) {
+        T J[M::lu_nnz];
+        M::template jacobian<T>(y, t, a.P, a.PD, F, J);
+        M::lu_unpack(J, [&](int k, T v) { a.out[(uint64_t)k * a.ld + node] = double(v); });
     }
 }
 
@@ -1011,13 +971,12 @@ inline unsigned long explicit_num_steps(double ldt_0, double dt)
 template <class M>
 inline uint32_t solver_state_rows(int32_t solver)
 {
-    constexpr uint32_t n = M::num_states;
     if (solver == GOSS_THETA)
         return TH_ROWS;
     if (solver == GOSS_IMPLICIT_EULER)
-        return TH_ROWS + n * n;
+        return TH_ROWS + M::lu_nnz;
     if (solver == GOSS_ESDIRK23A)
-        return ES_SCALARS + 2 * n * n;
+        return ES_SCALARS + 2 * M::lu_nnz;
     return 0;
 }
 

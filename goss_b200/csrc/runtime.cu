@@ -1180,22 +1180,44 @@ extern "C" {
 
 GOSS_API uint64_t goss_model_eval_noalloc_capacity(void) { return GOSS_NOALLOC_SCRATCH_DOUBLES; }
 
+// Output rows per state of goss_model_eval for `what`, 0 when the model has
+// no such output (the caller reports it with eval_what_error).
+static uint32_t eval_width(const goss_model_desc* m, int32_t what)
+{
+    switch (what) {
+    case 0: return m->num_states;
+    case 1: return 2 * m->num_states;
+    case 2: return m->num_monitored;
+    case 3: return m->has_jacobian ? m->num_states * m->num_states : 0;
+    default: return 0;
+    }
+}
+
+static int eval_what_error(const goss_model_desc* m, int32_t what)
+{
+    if (what == 2)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "No monitored in the '%s' model.", m->name);
+    if (what == 3)
+        return fail(nullptr, GOSS_ERR_ARGUMENT,
+                    "the '%s' model was generated without the analytic Jacobian (generate_jacobian)", m->name);
+    return fail(nullptr, GOSS_ERR_ARGUMENT,
+                "what must be 0 (rhs), 1 (linearized), 2 (monitored) or 3 (analytic Jacobian)");
+}
+
 GOSS_API int goss_model_eval_noalloc(const goss_model_desc* m, int32_t what, int32_t precision, const double* params,
                                      const double* states, const double* field_params, const double* times,
                                      uint64_t count, double* out, void* stream)
 {
     if (!m || !states || !times || !out)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL argument");
-    if (what < 0 || what > 2)
-        return fail(nullptr, GOSS_ERR_ARGUMENT, "what must be 0 (rhs), 1 (linearized) or 2 (monitored)");
-    if (what == 2 && m->num_monitored == 0)
-        return fail(nullptr, GOSS_ERR_ARGUMENT, "No monitored in the '%s' model.", m->name);
+    const uint32_t width = eval_width(m, what);
+    if (!width)
+        return eval_what_error(m, what);
     if (count == 0)
         return 0;
     const uint32_t n = m->num_states, nfp = m->num_field_parameters;
     if (nfp > 32 && !field_params)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "models with more than 32 field parameters need field_params");
-    const uint32_t width = what == 0 ? n : (what == 1 ? 2 * n : m->num_monitored);
     const uint64_t ld = round_up(count, 32);
     const uint64_t need = (uint64_t)(n + nfp + width) * ld;
     if (count > 0xffffffffull || need > GOSS_NOALLOC_SCRATCH_DOUBLES)
@@ -1308,6 +1330,9 @@ GOSS_API int goss_model_eval(const goss_model_desc* m, int32_t what, int32_t pre
 {
     if (!m || !states || !times || !out)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL argument");
+    const uint32_t rows_out = eval_width(m, what);
+    if (!rows_out)
+        return eval_what_error(m, what);
     if (count == 0)
         return 0;
     if (count > 0xffffffffull)
@@ -1317,9 +1342,6 @@ GOSS_API int goss_model_eval(const goss_model_desc* m, int32_t what, int32_t pre
     CUDA_TRY(s, cudaSetDevice(device));
     const uint32_t n = m->num_states, nfp = m->num_field_parameters;
     const uint64_t ld = round_up(count, 32);
-    const uint32_t rows_out = what == 0 ? n : (what == 1 ? 2 * n : std::max<uint32_t>(m->num_monitored, 1));
-    if (what == 2 && m->num_monitored == 0)
-        return fail(nullptr, GOSS_ERR_ARGUMENT, "No monitored in the '%s' model.", m->name);
     double *d_states = nullptr, *d_fp = nullptr, *d_t = nullptr, *d_out = nullptr, *d_stage = nullptr;
     cudaStream_t st = nullptr;
     int rc = 0;

@@ -16,6 +16,7 @@ from typing import Dict, List, Optional, Sequence
 HERE = Path(__file__).resolve().parent
 
 # name, path of the .ode file inside the reference repository, field parameters
+# (optional: monitored intermediates, jacobian = the analytic Jacobian)
 SHIPPED: List[Dict] = [
     dict(name="tentusscher_panfilov_2006_M_cell", ode="demo/tentusscher_panfilov_2006_M_cell.ode",
          field_parameters=[]),
@@ -23,6 +24,8 @@ SHIPPED: List[Dict] = [
          field_parameters=["g_Kr", "g_Ks", "g_CaL", "g_to"]),
     dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode", field_parameters=[]),
     dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode", field_parameters=["g_Kr", "g_CaL"]),
+    dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode", field_parameters=["g_Kr", "g_CaL"],
+         jacobian=True),
     dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode",
          field_parameters=["g_Kr", "g_Na", "g_Ks"]),
     dict(name="tentusscher_2004_mcell", ode="tests/tentusscher_2004_mcell.ode",
@@ -43,12 +46,13 @@ def variant_dirs() -> List[Path]:
 
 
 def find_variant(name: str, field_parameters: Sequence[str] = (), monitored: Sequence[str] = (),
-                 linearization: str = "gotran") -> Optional[Path]:
+                 linearization: str = "gotran", jacobian: bool = False) -> Optional[Path]:
     """Shipped variant directory for a model name and code-generation choice."""
     for vdir in variant_dirs():
         md = json.loads((vdir / "model.json").read_text())
         if (md["name"] == name and md["field_parameter_names"] == list(field_parameters)
-                and md["monitored_names"] == list(monitored) and md.get("linearization", "gotran") == linearization):
+                and md["monitored_names"] == list(monitored) and md.get("linearization", "gotran") == linearization
+                and bool(md.get("jacobian", False)) == bool(jacobian)):
             return vdir
     return None
 

@@ -59,6 +59,165 @@ struct M_beeler_reuter_1977 {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
+  // Newton matrix: 24 packed entries (the Jacobian's 24 structural
+  // non-zeros, the diagonal and the LU fill-in; row-major over the structure)
+  static constexpr int lu_nnz = 24;
+  static constexpr bool has_jacobian = false;
+  // J := scale*J + I
+  template <class A>
+  __device__ static __forceinline__ void lu_shift(A J, const double scale)
+  {
+    for (int k = 0; k < 24; ++k) J[k] = J[k] * scale;
+    J[0] = J[0] + 1.0 * 1.0;
+    J[2] = J[2] + 1.0 * 1.0;
+    J[4] = J[4] + 1.0 * 1.0;
+    J[6] = J[6] + 1.0 * 1.0;
+    J[10] = J[10] + 1.0 * 1.0;
+    J[12] = J[12] + 1.0 * 1.0;
+    J[14] = J[14] + 1.0 * 1.0;
+    J[23] = J[23] + 1.0 * 1.0;
+  }
+  // D := scale*S + I
+  template <class A, class B>
+  __device__ static __forceinline__ void lu_copy_shift(A S, B D, const double scale)
+  {
+    for (int k = 0; k < 24; ++k) D[k] = S[k] * scale;
+    D[0] = D[0] + 1.0 * 1.0;
+    D[2] = D[2] + 1.0 * 1.0;
+    D[4] = D[4] + 1.0 * 1.0;
+    D[6] = D[6] + 1.0 * 1.0;
+    D[10] = D[10] + 1.0 * 1.0;
+    D[12] = D[12] + 1.0 * 1.0;
+    D[14] = D[14] + 1.0 * 1.0;
+    D[23] = D[23] + 1.0 * 1.0;
+  }
+  // in-place Doolittle LU without pivoting over the structure
+  template <class A>
+  __device__ static __forceinline__ void lu_factorize(A J)
+  {
+    { const double s = 0.0; J[16] = (J[16] - s) / J[0]; }
+    { const double s = 0.0; J[17] = (J[17] - s) / J[2]; }
+    { const double s = 0.0; J[18] = (J[18] - s) / J[4]; }
+    { const double s = 0.0; J[19] = (J[19] - s) / J[6]; }
+    { double s = 0.0; s = s + J[19] * J[7]; J[20] = (J[20] - s) / J[10]; }
+    { double s = 0.0; s = s + J[19] * J[8]; J[21] = (J[21] - s) / J[12]; }
+    { const double s = 0.0; J[22] = (J[22] - s) / J[14]; }
+    { double s = 0.0; s = s + J[16] * J[1]; s = s + J[17] * J[3]; s = s + J[18] * J[5]; s = s + J[19] * J[9]; s = s + J[20] * J[11]; s = s + J[21] * J[13]; s = s + J[22] * J[15]; J[23] -= s; }
+  }
+  // x = (LU)^-1 b, forward then backward substitution; b and x may alias
+  template <class A>
+  __device__ static __forceinline__ void lu_solve(A J, const double* b, double* x)
+  {
+    x[0] = b[0];
+    x[1] = b[1] - 0.0;
+    x[2] = b[2] - 0.0;
+    x[3] = b[3] - 0.0;
+    x[4] = b[4] - 0.0;
+    x[5] = b[5] - 0.0;
+    x[6] = b[6] - 0.0;
+    { double s = 0.0; s = s + J[16] * x[0]; s = s + J[17] * x[1]; s = s + J[18] * x[2]; s = s + J[19] * x[3]; s = s + J[20] * x[4]; s = s + J[21] * x[5]; s = s + J[22] * x[6]; x[7] = b[7] - s; }
+    x[7] = x[7] / J[23];
+    { double s = 0.0; s = s + J[15] * x[7]; x[6] = (x[6] - s) / J[14]; }
+    { double s = 0.0; s = s + J[13] * x[7]; x[5] = (x[5] - s) / J[12]; }
+    { double s = 0.0; s = s + J[11] * x[7]; x[4] = (x[4] - s) / J[10]; }
+    { double s = 0.0; s = s + J[7] * x[4]; s = s + J[8] * x[5]; s = s + J[9] * x[7]; x[3] = (x[3] - s) / J[6]; }
+    { double s = 0.0; s = s + J[5] * x[7]; x[2] = (x[2] - s) / J[4]; }
+    { double s = 0.0; s = s + J[3] * x[7]; x[1] = (x[1] - s) / J[2]; }
+    { double s = 0.0; s = s + J[1] * x[7]; x[0] = (x[0] - s) / J[0]; }
+  }
+  // forward differences: zero the entries outside the Jacobian's structure, then
+  // column i = (f2 - f1) / delta at its structural rows
+  template <class A>
+  __device__ static __forceinline__ void fd_clear(A J)
+  {
+    (void)J;
+  }
+  template <class A>
+  __device__ static __forceinline__ void fd_column(const int i, const double* f1, const double* f2,
+                                                   const double delta, A J)
+  {
+    switch (i) {
+    case 0: J[0] = (f2[0] - f1[0]) / delta; J[16] = (f2[7] - f1[7]) / delta; break;
+    case 1: J[2] = (f2[1] - f1[1]) / delta; J[17] = (f2[7] - f1[7]) / delta; break;
+    case 2: J[4] = (f2[2] - f1[2]) / delta; J[18] = (f2[7] - f1[7]) / delta; break;
+    case 3: J[6] = (f2[3] - f1[3]) / delta; J[19] = (f2[7] - f1[7]) / delta; break;
+    case 4: J[7] = (f2[3] - f1[3]) / delta; J[10] = (f2[4] - f1[4]) / delta; J[20] = (f2[7] - f1[7]) / delta; break;
+    case 5: J[8] = (f2[3] - f1[3]) / delta; J[12] = (f2[5] - f1[5]) / delta; J[21] = (f2[7] - f1[7]) / delta; break;
+    case 6: J[14] = (f2[6] - f1[6]) / delta; J[22] = (f2[7] - f1[7]) / delta; break;
+    case 7: J[1] = (f2[0] - f1[0]) / delta; J[3] = (f2[1] - f1[1]) / delta; J[5] = (f2[2] - f1[2]) / delta; J[9] = (f2[3] - f1[3]) / delta; J[11] = (f2[4] - f1[4]) / delta; J[13] = (f2[5] - f1[5]) / delta; J[15] = (f2[6] - f1[6]) / delta; J[23] = (f2[7] - f1[7]) / delta; break;
+    default: break;
+    }
+  }
+  // dense row-major copy: out(r*n + c, value) for every entry
+  template <typename T, class Out>
+  __device__ static __forceinline__ void lu_unpack(const T* J, Out&& out)
+  {
+    out(0, J[0]);
+    out(1, T(0.0));
+    out(2, T(0.0));
+    out(3, T(0.0));
+    out(4, T(0.0));
+    out(5, T(0.0));
+    out(6, T(0.0));
+    out(7, J[1]);
+    out(8, T(0.0));
+    out(9, J[2]);
+    out(10, T(0.0));
+    out(11, T(0.0));
+    out(12, T(0.0));
+    out(13, T(0.0));
+    out(14, T(0.0));
+    out(15, J[3]);
+    out(16, T(0.0));
+    out(17, T(0.0));
+    out(18, J[4]);
+    out(19, T(0.0));
+    out(20, T(0.0));
+    out(21, T(0.0));
+    out(22, T(0.0));
+    out(23, J[5]);
+    out(24, T(0.0));
+    out(25, T(0.0));
+    out(26, T(0.0));
+    out(27, J[6]);
+    out(28, J[7]);
+    out(29, J[8]);
+    out(30, T(0.0));
+    out(31, J[9]);
+    out(32, T(0.0));
+    out(33, T(0.0));
+    out(34, T(0.0));
+    out(35, T(0.0));
+    out(36, J[10]);
+    out(37, T(0.0));
+    out(38, T(0.0));
+    out(39, J[11]);
+    out(40, T(0.0));
+    out(41, T(0.0));
+    out(42, T(0.0));
+    out(43, T(0.0));
+    out(44, T(0.0));
+    out(45, J[12]);
+    out(46, T(0.0));
+    out(47, J[13]);
+    out(48, T(0.0));
+    out(49, T(0.0));
+    out(50, T(0.0));
+    out(51, T(0.0));
+    out(52, T(0.0));
+    out(53, T(0.0));
+    out(54, J[14]);
+    out(55, J[15]);
+    out(56, J[16]);
+    out(57, J[17]);
+    out(58, J[18]);
+    out(59, J[19]);
+    out(60, J[20]);
+    out(61, J[21]);
+    out(62, J[22]);
+    out(63, J[23]);
+  }
+
   // derived constants: parameter-only sub-expressions, evaluated once per
   // launch on the host in FP64 and stored after the parameters
   static void derived(const double* P, double* C)

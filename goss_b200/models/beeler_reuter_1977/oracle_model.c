@@ -143,5 +143,6 @@ const oracle_model* oracle_model_beeler_reuter_1977(void)
   model.ic = beeler_reuter_1977_ic;
   model.default_params = beeler_reuter_1977_defaults;
   model.linear_terms = beeler_reuter_1977_linear_terms;
+  model.jacobian = 0;
   return &model;
 }

@@ -29,6 +29,69 @@ struct M_fhn {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
+  // Newton matrix: 4 packed entries (the Jacobian's 4 structural
+  // non-zeros, the diagonal and the LU fill-in; row-major over the structure)
+  static constexpr int lu_nnz = 4;
+  static constexpr bool has_jacobian = false;
+  // J := scale*J + I
+  template <class A>
+  __device__ static __forceinline__ void lu_shift(A J, const double scale)
+  {
+    for (int k = 0; k < 4; ++k) J[k] = J[k] * scale;
+    J[0] = J[0] + 1.0 * 1.0;
+    J[3] = J[3] + 1.0 * 1.0;
+  }
+  // D := scale*S + I
+  template <class A, class B>
+  __device__ static __forceinline__ void lu_copy_shift(A S, B D, const double scale)
+  {
+    for (int k = 0; k < 4; ++k) D[k] = S[k] * scale;
+    D[0] = D[0] + 1.0 * 1.0;
+    D[3] = D[3] + 1.0 * 1.0;
+  }
+  // in-place Doolittle LU without pivoting over the structure
+  template <class A>
+  __device__ static __forceinline__ void lu_factorize(A J)
+  {
+    { const double s = 0.0; J[2] = (J[2] - s) / J[0]; }
+    { double s = 0.0; s = s + J[2] * J[1]; J[3] -= s; }
+  }
+  // x = (LU)^-1 b, forward then backward substitution; b and x may alias
+  template <class A>
+  __device__ static __forceinline__ void lu_solve(A J, const double* b, double* x)
+  {
+    x[0] = b[0];
+    { double s = 0.0; s = s + J[2] * x[0]; x[1] = b[1] - s; }
+    x[1] = x[1] / J[3];
+    { double s = 0.0; s = s + J[1] * x[1]; x[0] = (x[0] - s) / J[0]; }
+  }
+  // forward differences: zero the entries outside the Jacobian's structure, then
+  // column i = (f2 - f1) / delta at its structural rows
+  template <class A>
+  __device__ static __forceinline__ void fd_clear(A J)
+  {
+    (void)J;
+  }
+  template <class A>
+  __device__ static __forceinline__ void fd_column(const int i, const double* f1, const double* f2,
+                                                   const double delta, A J)
+  {
+    switch (i) {
+    case 0: J[0] = (f2[0] - f1[0]) / delta; J[2] = (f2[1] - f1[1]) / delta; break;
+    case 1: J[1] = (f2[0] - f1[0]) / delta; J[3] = (f2[1] - f1[1]) / delta; break;
+    default: break;
+    }
+  }
+  // dense row-major copy: out(r*n + c, value) for every entry
+  template <typename T, class Out>
+  __device__ static __forceinline__ void lu_unpack(const T* J, Out&& out)
+  {
+    out(0, J[0]);
+    out(1, J[1]);
+    out(2, J[2]);
+    out(3, J[3]);
+  }
+
   // derived constants: parameter-only sub-expressions, evaluated once per
   // launch on the host in FP64 and stored after the parameters
   static void derived(const double* P, double* C)

@@ -77,5 +77,6 @@ const oracle_model* oracle_model_fhn(void)
   model.ic = fhn_ic;
   model.default_params = fhn_defaults;
   model.linear_terms = fhn_linear_terms;
+  model.jacobian = 0;
   return &model;
 }

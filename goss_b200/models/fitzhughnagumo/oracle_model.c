@@ -77,5 +77,6 @@ const oracle_model* oracle_model_fitzhughnagumo(void)
   model.ic = fitzhughnagumo_ic;
   model.default_params = fitzhughnagumo_defaults;
   model.linear_terms = fitzhughnagumo_linear_terms;
+  model.jacobian = 0;
   return &model;
 }

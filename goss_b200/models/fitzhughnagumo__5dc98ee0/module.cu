@@ -31,6 +31,7 @@ extern "C" GOSS_API const goss_model_desc* goss_b200_model_fitzhughnagumo__5dc98
         initial_conditions, default_parameters, linear_terms,
         (1u << GOSS_NUM_SOLVERS) - 1u,
         launch, eval, rows, op_lin, op_rhs, adjoint,
+        0u, 4u,
     };
     return &d;
 }

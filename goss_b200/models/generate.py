@@ -24,8 +24,10 @@ def main() -> int:
         model = load_ode(ref / entry["ode"])
         assert model.name == entry["name"], (model.name, entry["name"])
         mon = entry.get("monitored", [])
-        ident = variant_id(model, entry["field_parameters"], mon)
-        md = write_variant(model, HERE / ident, field_parameters=entry["field_parameters"], monitored=mon)
+        jac = entry.get("jacobian", False)
+        ident = variant_id(model, entry["field_parameters"], mon, jacobian=jac)
+        md = write_variant(model, HERE / ident, field_parameters=entry["field_parameters"], monitored=mon,
+                           jacobian=jac)
         print(f"{ident}: {len(md['state_names'])} states, {len(md['parameter_names'])} parameters, "
               f"field parameters {md['field_parameter_names']}")
     # batch modules over shipped variants

@@ -50,5 +50,6 @@ const oracle_model* oracle_model_oscilator(void)
   model.ic = oscilator_ic;
   model.default_params = oscilator_defaults;
   model.linear_terms = oscilator_linear_terms;
+  model.jacobian = 0;
   return &model;
 }

@@ -31,6 +31,7 @@ extern "C" GOSS_API const goss_model_desc* goss_b200_model_tentusscher_2004_mcel
         initial_conditions, default_parameters, linear_terms,
         (1u << GOSS_NUM_SOLVERS) - 1u,
         launch, eval, rows, op_lin, op_rhs, adjoint,
+        0u, 71u,
     };
     return &d;
 }

@@ -48,7 +48,8 @@ class ODE:
     """
 
     def __init__(self, *args, field_states: Sequence[str] = (), field_parameters: Sequence[str] = (),
-                 monitored: Sequence[str] = (), linearization: str = "gotran", **kwargs):
+                 monitored: Sequence[str] = (), linearization: str = "gotran", code_params: Optional[dict] = None,
+                 **kwargs):
         if not args:
             raise ValueError("ODE needs a model")
         src = args[0]
@@ -60,7 +61,7 @@ class ODE:
         if isinstance(src, (ODEModel, os.PathLike, str)):
             try:
                 self._module = jit(src, field_parameters=field_parameters, monitored=monitored,
-                                   linearization=linearization)
+                                   linearization=linearization, code_params=code_params)
             except ODEParseError as exc:
                 raise ValueError(str(exc)) from exc
             except ValueError:
@@ -126,7 +127,7 @@ class ODE:
         count = states.shape[0]
         times = np.ascontiguousarray(np.broadcast_to(np.asarray(times, dtype=np.float64), (count,)))
         n = self.num_states
-        width = {0: n, 1: 2 * n, 2: max(len(self._meta["monitored_names"]), 1)}[what]
+        width = {0: n, 1: 2 * n, 2: max(len(self._meta["monitored_names"]), 1), 3: n * n}[what]
         out = np.zeros((count, width))
         fp_ptr = None
         if field_params is not None:
@@ -174,12 +175,20 @@ class ODE:
             return LinearizedEval(rhs=rhs)
         return LinearizedEval(linear=linear, rhs=rhs)
 
-    def compute_jacobian(self, states, time: float) -> np.ndarray:
-        """Forward-difference Jacobian (ODE::compute_jacobian, ODE.cpp:47-67).
+    @property
+    def has_jacobian(self) -> bool:
+        """Generated with the analytic Jacobian (``code_params={"generate_jacobian": True}``)."""
+        return bool(self._meta.get("jacobian", False))
 
-        The n+1 right-hand sides are evaluated in one batched kernel."""
+    def compute_jacobian(self, states, time: float) -> np.ndarray:
+        """Jacobian ``jac[i, j] = d f_i / d y_j``: the generated analytic one
+        when the model has it (the reference's generated override), else
+        forward differences (ODE::compute_jacobian, ODE.cpp:47-67) with the n+1
+        right-hand sides evaluated in one batched kernel."""
         y = self._check_state_input(states)
         n = self.num_states
+        if self.has_jacobian:
+            return self._eval(3, y, time)[0].reshape(n, n)
         deltas = np.sqrt(1e-15 * np.maximum(1e-5, np.abs(y)))
         batch = np.repeat(y[None, :], n + 1, axis=0)
         batch[np.arange(1, n + 1), np.arange(n)] += deltas

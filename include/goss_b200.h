@@ -35,7 +35,7 @@ extern "C" {
 #define GOSS_API
 #endif
 
-#define GOSS_B200_ABI_VERSION 1u
+#define GOSS_B200_ABI_VERSION 2u
 
 /* Solver kinds: the reference solver classes on this path. */
 enum goss_solver_kind {
@@ -112,7 +112,10 @@ typedef struct goss_launch {
 } goss_launch;
 
 /* Batched evaluation of the model on device arrays (used by ODE.eval and the
- * tests): out = rhs (what = 0) or [linear; rhs] (what = 1). */
+ * tests): out = rhs (what = 0), [linear; rhs] (what = 1), the monitored values
+ * (what = 2) or, for a model with has_jacobian, the analytic Jacobian
+ * [num_states * num_states][ld], entry (i, j) = d f_i / d y_j in row
+ * i * num_states + j (what = 3). */
 typedef struct goss_eval_launch {
     int32_t what;
     int32_t precision;
@@ -121,7 +124,7 @@ typedef struct goss_eval_launch {
     const double* states;       /* device [num_states][ld] */
     const double* field_params; /* device [nfp][ld] or NULL */
     const double* times;        /* device [num_nodes] */
-    double* out;                /* device [num_states][ld] (what=0) or [2*num_states][ld] */
+    double* out;                /* device [rows][ld], rows as listed above */
     const double* params;       /* host [num_parameters] */
     void* stream;
 } goss_eval_launch;
@@ -194,6 +197,14 @@ typedef struct goss_model_desc {
     const uint32_t* op_census_rhs;
     /* GRL1 trajectory adjoint (goss_adjoint_launch) */
     int (*adjoint)(const goss_adjoint_launch* launch);
+    /* 1: generated with the analytic Jacobian (the reference's code_params
+     * "generate_jacobian", python/goss/codegeneration.py:622-641): eval what=3
+     * returns it and ThetaSolver/ImplicitEuler/ESDIRK23a use it in place of
+     * forward differences (ODE::compute_jacobian, ODE.cpp:47-67) */
+    uint32_t has_jacobian;
+    /* packed entries of the implicit solvers' Newton matrix: the Jacobian's
+     * structural non-zeros, the diagonal and the LU fill-in */
+    uint32_t lu_nnz;
 } goss_model_desc;
 
 /* One population of a heterogeneous batch (filled by the runtime). */
@@ -310,8 +321,9 @@ GOSS_API int goss_system_forward_async(goss_system* sys, double t, double interv
 GOSS_API int goss_system_synchronize(goss_system* sys);
 
 /* Batched model evaluation on host arrays: states [count][n], times [count],
- * field_params [count][nfp] (may be NULL), out [count][n] (what=0) or
- * [count][2n] = (linear, rhs) (what=1). */
+ * field_params [count][nfp] (may be NULL), out [count][n] (what=0),
+ * [count][2n] = (linear, rhs) (what=1), [count][num_monitored] (what=2) or
+ * [count][n*n] = the analytic Jacobian, row-major (what=3, has_jacobian). */
 GOSS_API int goss_model_eval(const goss_model_desc* model, int32_t what, int32_t precision, const double* params,
                              const double* states, const double* field_params, const double* times, uint64_t count,
                              double* out, int32_t device);
@@ -352,7 +364,8 @@ GOSS_API const char* goss_batch_last_error(const goss_batch* batch);
  * Same arithmetic as goss_model_eval, but every pointer is DEVICE memory on
  * the current device: states [count][n], field_params [count][nfp] (NULL:
  * the parameter values), times [count], out [count][width] with width n
- * (what = 0), 2n (what = 1: linear then rhs) or num_monitored (what = 2).
+ * (what = 0), 2n (what = 1: linear then rhs), num_monitored (what = 2) or
+ * n*n (what = 3: the analytic Jacobian of a model with has_jacobian).
  * params is a HOST array of num_parameters values (NULL: defaults).
  *
  * Working arrays live in one fixed file-scope device array of

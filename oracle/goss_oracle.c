@@ -156,11 +156,17 @@ void oracle_system_counters(oracle_system* s, int64_t* jac_comp, int64_t* reject
 /* ---------------------------------------------------------------------- */
 
 /* ODE::compute_jacobian (ODE.cpp:47-67): forward differences, column i
- * perturbed by sqrt(1e-15*max(1e-5,|y_i|)), stored row-major jac[j*n+i]. */
+ * perturbed by sqrt(1e-15*max(1e-5,|y_i|)), stored row-major jac[j*n+i];
+ * a model generated with the analytic Jacobian overrides it (the plugin's
+ * compute_jacobian, which leaves f1 untouched). */
 void oracle_compute_jacobian(const oracle_model* m, const double* params, double* states, double time,
                              double* jac, double* f1, double* f2)
 {
     int n = m->num_states;
+    if (m->jacobian) {
+        m->jacobian(states, time, params, jac);
+        return;
+    }
     m->rhs(states, time, params, f1);
     for (int i = 0; i < n; ++i) {
         double ysafe = states[i];

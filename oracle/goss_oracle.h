@@ -39,6 +39,9 @@ typedef struct oracle_model {
     const double* ic;
     const double* default_params;
     const unsigned char* linear_terms;
+    /* analytic Jacobian jac[i*n + j] = d f_i / d y_j, the generated override
+     * of ODE::compute_jacobian (ODE.h:71); NULL: forward differences */
+    void (*jacobian)(const double* states, double time, const double* params, double* jac);
 } oracle_model;
 
 enum {

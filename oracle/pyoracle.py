@@ -40,6 +40,7 @@ class _Model(C.Structure):
         ("ic", _dp),
         ("default_params", _dp),
         ("linear_terms", C.POINTER(C.c_ubyte)),
+        ("jacobian", C.CFUNCTYPE(None, _dp, C.c_double, _dp, _dp)),
     ]
 
 
@@ -134,6 +135,17 @@ class OracleModel:
         f1, f2 = np.zeros(self.n), np.zeros(self.n)
         self.lib.oracle_compute_jacobian(self.ptr, _ptr(p), _ptr(y), float(t), _ptr(jac), _ptr(f1), _ptr(f2))
         return jac
+
+    def lu_factorize(self, mat: np.ndarray) -> None:
+        """ODE::lu_factorize restated (dense, in place)."""
+        assert mat.dtype == np.float64 and mat.flags.c_contiguous and mat.shape == (self.n, self.n)
+        self.lib.oracle_lu_factorize(self.n, _ptr(mat))
+
+    def forward_backward_subst(self, mat: np.ndarray, b: np.ndarray) -> np.ndarray:
+        x = np.zeros(self.n)
+        self.lib.oracle_forward_backward_subst(self.n, _ptr(np.ascontiguousarray(mat)),
+                                               _ptr(np.ascontiguousarray(b, dtype=np.float64)), _ptr(x))
+        return x
 
     def solver_params(self, solver: str, **overrides) -> SolverParams:
         sp = SolverParams()
@@ -327,6 +339,9 @@ class RefSystem:
             L.ref_last_error.argtypes = [C.c_void_p]
             L.ref_last_error.restype = C.c_char_p
             L.ref_num_jac_comp.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+            L.ref_compute_jacobian.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
+            L.ref_lu_factorize.argtypes = [C.c_void_p, _dp]
+            L.ref_forward_backward_subst.argtypes = [C.c_void_p, _dp, _dp, _dp]
             cls._lib = L
         return cls._lib
 
@@ -360,6 +375,23 @@ class RefSystem:
 
     def forward(self, t: float, interval: float) -> int:
         return self.lib().ref_forward(self.h, float(t), float(interval))
+
+    def compute_jacobian(self, y: np.ndarray, t: float) -> np.ndarray:
+        """The plugin's ODE::compute_jacobian at the default parameters."""
+        y = np.array(y, dtype=np.float64)
+        jac = np.zeros((self.n, self.n))
+        self.lib().ref_compute_jacobian(self.h, _ptr(y), float(t), _ptr(jac))
+        return jac
+
+    def lu_factorize(self, mat: np.ndarray) -> None:
+        assert mat.dtype == np.float64 and mat.flags.c_contiguous and mat.shape == (self.n, self.n)
+        self.lib().ref_lu_factorize(self.h, _ptr(mat))
+
+    def forward_backward_subst(self, mat: np.ndarray, b: np.ndarray) -> np.ndarray:
+        x = np.zeros(self.n)
+        self.lib().ref_forward_backward_subst(self.h, _ptr(np.ascontiguousarray(mat)),
+                                              _ptr(np.ascontiguousarray(b, dtype=np.float64)), _ptr(x))
+        return x
 
     def num_jac_comp(self) -> np.ndarray:
         out = np.zeros(self.N, dtype=np.int64)

@@ -296,4 +296,27 @@ __attribute__((visibility("default"))) int ref_num_jac_comp(void* h, int64_t* ou
     return 0;
 }
 
+// ODE::compute_jacobian (ODE.h:71) of the plugin model with its default
+// parameters: the generated analytic override when the plugin has one, else
+// the reference's forward differences (ODE.cpp:47-67); jac is row-major n x n.
+__attribute__((visibility("default"))) void ref_compute_jacobian(void* h, double* states, double time, double* jac)
+{
+    auto* r = static_cast<RefSystem*>(h);
+    auto ode = std::dynamic_pointer_cast<goss::ParameterizedODE>(r->ode->copy());
+    ode->compute_jacobian(states, time, jac);
+}
+
+// ODE::lu_factorize (ODE.cpp:69-100) and ODE::forward_backward_subst
+// (ODE.cpp:102-132) of the plugin model, in place on a row-major n x n matrix.
+__attribute__((visibility("default"))) void ref_lu_factorize(void* h, double* mat)
+{
+    static_cast<RefSystem*>(h)->ode->lu_factorize(mat);
+}
+
+__attribute__((visibility("default"))) void ref_forward_backward_subst(void* h, const double* mat, const double* b,
+                                                                      double* x)
+{
+    static_cast<RefSystem*>(h)->ode->forward_backward_subst(mat, b, x);
+}
+
 }  // extern "C"

@@ -14,9 +14,9 @@ ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = ROOT / "tests" / "golden"
 
 
-def variant_dir(name: str, field_parameters=()) -> Path:
-    d = models.find_variant(name, list(field_parameters))
-    assert d is not None, f"no shipped variant {name} {field_parameters}"
+def variant_dir(name: str, field_parameters=(), jacobian: bool = False) -> Path:
+    d = models.find_variant(name, list(field_parameters), jacobian=jacobian)
+    assert d is not None, f"no shipped variant {name} {field_parameters}" + (" with the Jacobian" if jacobian else "")
     return d
 
 
@@ -25,21 +25,21 @@ def meta(vdir: Path) -> dict:
 
 
 @lru_cache(maxsize=None)
-def oracle_model(name: str, field_parameters=()) -> pyoracle.OracleModel:
-    vdir = variant_dir(name, field_parameters)
+def oracle_model(name: str, field_parameters=(), jacobian: bool = False) -> pyoracle.OracleModel:
+    vdir = variant_dir(name, field_parameters, jacobian)
     md = meta(vdir)
     return pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
 
 
-def ref_system(name: str, solver: str, num_nodes: int, field_parameters=(), **sp):
+def ref_system(name: str, solver: str, num_nodes: int, field_parameters=(), jacobian: bool = False, **sp):
     """The reference's compiled solvers, or None when oracle/_ref is not built."""
-    vdir = variant_dir(name, field_parameters)
+    vdir = variant_dir(name, field_parameters, jacobian)
     if not pyoracle.ref_available():
         return None
     plug = pyoracle.build_ref_plugin(vdir)
     if plug is None or not plug.exists():
         return None
-    om = oracle_model(name, tuple(field_parameters))
+    om = oracle_model(name, tuple(field_parameters), jacobian)
     return pyoracle.RefSystem(plug, meta(vdir)["class_name"], solver, num_nodes, om.solver_params(solver, **sp))
 
 

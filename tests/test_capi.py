@@ -67,7 +67,9 @@ def test_model_descriptor_matches_metadata(vdir):
     assert [d.linear_terms[i] for i in range(n)] == md["linear_terms"]
     assert d.supported_solvers == (1 << 10) - 1
     assert d.solver_state_rows(_capi.GOSS_GRL1) == 0
-    assert d.solver_state_rows(_capi.GOSS_ESDIRK23A) == 9 + 2 * n * n
+    assert d.lu_nnz == md["lu_nnz"] and d.has_jacobian == int(md["jacobian"])
+    assert d.solver_state_rows(_capi.GOSS_ESDIRK23A) == 9 + 2 * md["lu_nnz"]
+    assert d.solver_state_rows(_capi.GOSS_IMPLICIT_EULER) == 7 + md["lu_nnz"]
 
 
 def test_host_lu_matches_oracle():

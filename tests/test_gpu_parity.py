@@ -22,15 +22,16 @@ TOL64 = 1e-10
 
 
 def run_pair(model, solver_name, N, steps, dt, ldt, field_parameters=(), fp=None, seed=11, spread=0.02,
-             precision="double", t0=0.0, solver_params=None):
+             precision="double", t0=0.0, solver_params=None, jacobian=False):
     rng = np.random.default_rng(seed)
-    ode = goss.ParameterizedODE(model, field_parameters=list(field_parameters))
+    ode = goss.ParameterizedODE(model, field_parameters=list(field_parameters),
+                                code_params={"generate_jacobian": True} if jacobian else None)
     solver = goss.solvers.solver_mapper[solver_name](ode)
     solver.internal_time_step = ldt
     for k, v in (solver_params or {}).items():
         solver.set_parameter(k, v)
     system = goss.ODESystemSolver(N, solver, ode, precision=precision)
-    om = oracle_model(model, tuple(field_parameters))
+    om = oracle_model(model, tuple(field_parameters), jacobian)
     y0 = perturbed_states(om.ic, N, rng, spread)
     system.set_states(y0)
     o = pyoracle.OracleSystem(om, solver_name, N, ldt=ldt, **(solver_params or {}))
@@ -198,3 +199,39 @@ def test_implicit_euler_rejects_fp32():
     ode = goss.ParameterizedODE("tentusscher_2004_mcell")
     with pytest.raises(Exception):
         goss.ODESystemSolver(4, goss.solvers.ImplicitEuler(ode), ode, precision="single")
+
+
+# Analytic Jacobian (code_params generate_jacobian): the implicit kernels use
+# the generated Jacobian in place of forward differences; the oracle runs the
+# same generated Jacobian (bit-identical to the reference's plugin override,
+# tests/test_jacobian.py).
+@pytest.mark.parametrize("solver,steps,ldt", [
+    ("ThetaSolver", 40, 0.1),
+    ("ImplicitEuler", 40, 0.1),
+    ("ImplicitEuler", 30, -1.0),
+    ("ESDIRK23a", 30, -1.0),
+])
+def test_tt04_implicit_analytic_jacobian_fp64(solver, steps, ldt):
+    fps = ("g_Kr", "g_CaL")
+    md = meta(variant_dir("tentusscher_2004_mcell", fps, True))
+    rng = np.random.default_rng(17)
+    N = 16
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * (1 + rng.uniform(-0.05, 0.05, (N, 2)))
+    gpu, cpu, system = run_pair("tentusscher_2004_mcell", solver, N, steps, 0.1, ldt, fps, fp, jacobian=True)
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+    assert system.ode.has_jacobian
+
+
+def test_analytic_jacobian_eval_matches_oracle():
+    fps = ("g_Kr", "g_CaL")
+    ode = goss.ParameterizedODE("tentusscher_2004_mcell", field_parameters=list(fps),
+                                code_params={"generate_jacobian": True})
+    om = oracle_model("tentusscher_2004_mcell", fps, True)
+    rng = np.random.default_rng(3)
+    for y in perturbed_states(om.ic, 4, rng, 0.05):
+        a, b = ode.compute_jacobian(y, 1.5), om.jacobian(y, 1.5)
+        scale = np.maximum(np.abs(b).max(axis=1, keepdims=True), 1e-300)
+        assert np.max(np.abs(a - b) / scale) < 1e-12
+    plain = goss.ParameterizedODE("tentusscher_2004_mcell", field_parameters=list(fps))
+    assert not plain.has_jacobian
