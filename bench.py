@@ -50,16 +50,42 @@ def _args():
     ap.add_argument("--impl", default="goss_b200", choices=["goss_b200", "reference"])
     ap.add_argument("--nodes", type=int, default=N_NODES)
     ap.add_argument("--skip-fp64", action="store_true", help=argparse.SUPPRESS)
-    ap.add_argument("--profile", choices=["single", "double", "adjoint-single", "adjoint-double"], default=None,
-                    help="only run the timed forward loop in one precision, or one adjoint gradient "
-                         "(65,536 nodes x 2,000 steps), for ncu captures")
+    ap.add_argument("--profile", choices=["single", "double", "adjoint-single", "adjoint-double"] + list(_IMPLICIT_PROFILES),
+                    default=None,
+                    help="only run the timed forward loop in one precision, one adjoint gradient "
+                         "(65,536 nodes x 2,000 steps) or W+K intervals of one implicit solver on "
+                         "65,536 nodes of the implicit workload, for ncu captures")
     return ap.parse_args()
+
+
+# --profile choice -> label of IMPLICIT_SOLVERS
+_IMPLICIT_PROFILES = {"theta": "ThetaSolver", "esdirk": "ESDIRK23a", "theta-jacobian": "ThetaSolver+jacobian",
+                      "ie-jacobian": "ImplicitEuler+jacobian", "esdirk-jacobian": "ESDIRK23a+jacobian"}
 
 
 def profile_run(args):
     """Minimal run for profiler captures: W+K forward calls of one precision,
-    or one record + backward pass of the adjoint workload shortened to 20 ms."""
+    one record + backward pass of the adjoint workload shortened to 20 ms, or
+    W+K 0.1 ms intervals of one implicit solver on 65,536 nodes."""
     import goss_b200 as goss
+
+    if args.profile in _IMPLICIT_PROFILES:
+        label = _IMPLICIT_PROFILES[args.profile]
+        _, name, ldt, _, jac = next(c for c in IMPLICIT_SOLVERS if c[0] == label)
+        nodes = 65_536
+        md, y0, fp = implicit_inputs(nodes)
+        ode = goss.ParameterizedODE(IMPLICIT_MODEL, field_parameters=IMPLICIT_FIELDS,
+                                    code_params={"generate_jacobian": jac})
+        solver = goss.solvers.solver_mapper[name](ode)
+        solver.internal_time_step = ldt
+        system = goss.ODESystemSolver(nodes, solver, ode)
+        system.set_states(y0)
+        system.field_parameters = fp
+        for k in range(args.warmup + args.steps):
+            system.forward(k * IMPLICIT_DT, IMPLICIT_DT)
+        print(json.dumps({"profile": args.profile, "nodes": nodes, "intervals": args.warmup + args.steps,
+                          "finite": bool(np.isfinite(system.states).all())}))
+        return
 
     if args.profile.startswith("adjoint"):
         import torch

@@ -432,6 +432,10 @@ __device__ __forceinline__ double l2norm(const double* v)
 #ifndef GOSS_IMPLICIT_SPLIT
 #define GOSS_IMPLICIT_SPLIT 1
 #endif
+// Inlined at every call site: on TT04 with the analytic Jacobian, called
+// (__noinline__) versions of these two measured 1.3x slower, and capping the
+// kernels at 128 or 170 registers (3 or 4 blocks of 128 per SM) 1.3-1.4x
+// slower, than the 255-register inlined kernel.
 template <class M>
 __device__ __forceinline__ void rhs64(const double* y, double t, const double* P, const double* F, double* out)
 {
@@ -439,6 +443,12 @@ __device__ __forceinline__ void rhs64(const double* y, double t, const double* P
         M::template rhs_split<double>(y, t, P, P, F, out);
     else
         M::template rhs<double>(y, t, P, P, F, out);
+}
+
+template <class M, class A>
+__device__ __forceinline__ void jacobian64(const double* y, double t, const double* P, const double* F, A J)
+{
+    M::template jacobian<double>(y, t, P, P, F, J);
 }
 
 // ODE::compute_jacobian (ODE.cpp:47-67) into the packed Newton matrix J:
@@ -457,7 +467,7 @@ __device__ void compute_jacobian(const double* y, double t, const double* P, con
     constexpr int n = M::num_states;
     if constexpr (M::has_jacobian) {
         (void)f1;
-        M::template jacobian<double>(y, t, P, P, F, J);
+        jacobian64<M>(y, t, P, F, J);
     } else {
         M::fd_clear(J);
 #pragma unroll 1
@@ -497,7 +507,10 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
     if (node >= a.N)
         return;
     const goss_solver_params& sp = a.sp;
-    double y[n], z1[n], prev[n], ft1[n], yz[n], f1[n], b[n], dz[n];
+    // y: the state, z1: the Newton increment, prev: (1 - theta) f(y);
+    // yz, f1, b: one Newton iteration's point, f(yz) and residual (the
+    // correction dz is solved into b in place)
+    double y[n], z1[n], prev[n], yz[n], f1[n], b[n];
     double J[M::lu_nnz];
 #pragma unroll
     for (int i = 0; i < n; ++i)
@@ -540,9 +553,9 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
         for (int i = 0; i < n; ++i)
             z1[i] = 0.0;
         if (!IE && fabs(sp.theta - 1.0) > kGossEps) {
-            rhs64<M>(y, t, a.P, F, ft1);
+            rhs64<M>(y, t, a.P, F, f1);
             for (int i = 0; i < n; ++i)
-                prev[i] = (1 - sp.theta) * ft1[i];
+                prev[i] = (1 - sp.theta) * f1[i];
         }
         if (IE ? num_refinements > sp.num_refinements_without_always_recomputing_jacobian
                : num_refinements <= sp.num_refinements_without_always_recomputing_jacobian)
@@ -571,7 +584,7 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
                 jac_comp += 1;
                 recompute = 0;
             }
-            M::lu_solve(J, b, dz);
+            M::lu_solve(J, b, b);  // b := dz
             if (newton_iterations == 0) {
                 initial_residual = residual;
                 eta = eta > kGossEps ? eta : kGossEps;
@@ -598,7 +611,7 @@ __global__ void __launch_bounds__(128) theta_kernel(const __grid_constant__ Impl
                 break;
             }
             for (int i = 0; i < n; ++i)
-                z1[i] += dz[i];
+                z1[i] += b[i];
             relative_residual = residual / initial_residual;
             previous_residual = residual;
             newton_iterations++;
