@@ -177,6 +177,7 @@ _PROTOS = {
                                     C.c_int32, C.POINTER(C.c_void_p)]),
     "goss_batch_destroy": (C.c_int, [C.c_void_p]),
     "goss_batch_set_config": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, _u32p]),
+    "goss_batch_set_forwards_per_launch": (C.c_int, [C.c_void_p, C.c_uint32]),
     "goss_batch_forward": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
     "goss_batch_capture": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_uint32]),
     "goss_batch_replay": (C.c_int, [C.c_void_p]),

@@ -2,10 +2,11 @@
 
 For a :class:`~goss_b200.batch.BatchSolver` it searches the tile size
 (threads per block = nodes per tile), the persistent grid size, the tile
-schedule (round-robin or an atomic work counter) and the order in which the
-populations' tiles are laid out (as given, or most expensive first by the
-generator's operation census), timing each candidate with CUDA events on
-the batch stream over a few forwards.  For a single system it searches the
+schedule (round-robin, an atomic work counter or prefetching CTAs) and the
+order in which the populations' tiles are laid out (as given, or most
+expensive first by the generator's operation census), timing each candidate
+with CUDA events on the batch stream over a few graph-captured forwards (all
+in one launch unless the candidate sets ``forwards_per_launch``).  For a single system it searches the
 block size.  The states are saved before and restored after tuning, so
 tuning does not advance the simulation.  Results are cached in
 ``goss_b200/_jit/autotune.json`` keyed by the device, the module and the
@@ -72,7 +73,8 @@ def tune_batch(batch: BatchSolver, interval: float, t0: float = 0.0, steps: int 
     if use_cache:
         hit = _load_cache().get(key)
         if hit:
-            batch.set_config(hit["block"], hit["grid"], hit["schedule"], hit["order"])
+            batch.set_config(hit["block"], hit["grid"], hit["schedule"], hit["order"],
+                             hit.get("forwards_per_launch", 0))
             return dict(hit, cached=True)
     saved = [s.states for s in batch.systems]
     costs = [_cost(s) for s in batch.systems]
@@ -100,7 +102,7 @@ def tune_batch(batch: BatchSolver, interval: float, t0: float = 0.0, steps: int 
     finally:
         for s, y in zip(batch.systems, saved):
             s.set_states(y)
-    batch.set_config(best["block"], best["grid"], best["schedule"], best["order"])
+    batch.set_config(best["block"], best["grid"], best["schedule"], best["order"], best.get("forwards_per_launch", 0))
     _store(key, best)
     return dict(best, cached=False, tried=len(candidates))
 

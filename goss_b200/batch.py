@@ -131,7 +131,7 @@ class BatchSolver:
                                         C.byref(h)))
         self._h = h
         self._kinds = kinds
-        self.config = dict(block=128, grid=0, schedule=1, order=None)
+        self.config = dict(block=128, grid=0, schedule=1, order=None, forwards_per_launch=0)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -142,11 +142,17 @@ class BatchSolver:
                 pass
             self._h = None
 
-    def set_config(self, block: int = 128, grid: int = 0, schedule: int = 1, order: Optional[Sequence[int]] = None):
+    def set_config(self, block: int = 128, grid: int = 0, schedule: int = 1, order: Optional[Sequence[int]] = None,
+                   forwards_per_launch: int = 0):
+        """Launch configuration: nodes per tile, persistent grid (0: a block
+        per tile), tile schedule, population order, and how many consecutive
+        forwards of a captured graph one launch performs (0: all of them, the
+        states kept on chip in between; 1: a launch per forward)."""
         o = None if order is None else (C.c_uint32 * len(order))(*order)
         _check(_lib().goss_batch_set_config(self._h, int(block), int(grid), int(schedule), o), self._h)
+        _check(_lib().goss_batch_set_forwards_per_launch(self._h, int(forwards_per_launch)), self._h)
         self.config = dict(block=int(block), grid=int(grid), schedule=int(schedule),
-                           order=None if order is None else list(order))
+                           order=None if order is None else list(order), forwards_per_launch=int(forwards_per_launch))
 
     def _sync(self):
         for s in self.systems:
@@ -157,7 +163,8 @@ class BatchSolver:
         _check(_lib().goss_batch_forward(self._h, float(t), float(interval)), self._h)
 
     def capture(self, t0: float, interval: float, num_steps: int) -> None:
-        """Record num_steps forwards (t0 + k*interval) into a CUDA graph."""
+        """Record num_steps forwards (t0 + k*interval) into a CUDA graph,
+        ``config["forwards_per_launch"]`` of them per launch."""
         self._sync()
         _check(_lib().goss_batch_capture(self._h, float(t0), float(interval), int(num_steps)), self._h)
 

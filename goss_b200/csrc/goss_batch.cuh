@@ -269,7 +269,7 @@ inline int launch_batch_t(const goss_batch_launch* L)
                 a.P[off + k] = T(a.PD[off + k]);
         const unsigned long nsteps = explicit_num_steps(q.solver_params->ldt, L->interval);
         p.io = NodeIO{q.states, q.field_params, q.node_status, q.flags, q.ld, nsteps, L->t, L->interval / nsteps,
-                      q.solver_params->delta};
+                      q.solver_params->delta, L->forwards ? L->forwards : 1u, L->first_forward, L->interval};
         p.kind = q.kind;
         p.num_nodes = q.num_nodes;
         Dispatch::row_counts(q.kind, &p.state_rows, &p.field_rows);

@@ -163,6 +163,7 @@ struct Acc<double> {
     __device__ __forceinline__ double value() const { return y; }
     __device__ __forceinline__ double plus(double d) const { return y + d; }
     __device__ __forceinline__ void add(double d) { y = y + d; }
+    __device__ __forceinline__ void renormalize() {}
 };
 
 template <>
@@ -185,6 +186,11 @@ struct Acc<float> {
         lo = __fsub_rn(y, __fsub_rn(t, hi));
         hi = t;
     }
+    // between two forwards of one launch: exactly what store() to the FP64
+    // state array and load() by the next launch do.  An FP32 two-sum is not
+    // enough: when lo lies below FP64 precision of hi, the FP64 round trip
+    // rounds lo away and the two-sum keeps it
+    __device__ __forceinline__ void renormalize() { load(store()); }
 };
 
 // Where one node's explicit solve reads and writes (shared by the
@@ -195,10 +201,15 @@ struct NodeIO {
     uint8_t* node_status;   // [ld]
     uint32_t* flags;
     uint64_t ld;
-    uint64_t nsteps;
+    uint64_t nsteps;        // internal steps of one forward
     double t;
     double ldt;
     double delta;
+    // consecutive forwards of one launch: forward f starts at
+    // t + (first + f) * interval (the host loop's t0 + k * interval)
+    uint32_t forwards = 1;
+    uint64_t first = 0;
+    double interval = 0.0;
 };
 
 // The model evaluations the explicit steps use.  FP32 kernels take the split
@@ -338,10 +349,18 @@ __device__ __forceinline__ void explicit_node_core(const NodeIO& a, uint32_t nod
     constexpr int n = M::num_states;
     const double ldt = a.ldt;
     const T delta = T(a.delta);
-    double lt = a.t;
-    for (uint64_t step = 0; step < a.nsteps; ++step) {
-        explicit_step<M, T, S>(y, lt, ldt, P, PD, F, delta);
-        lt += ldt;
+    for (uint32_t f = 0; f < a.forwards; ++f) {
+        if (f) {
+#pragma unroll
+            for (int i = 0; i < n; ++i)
+                y[i].renormalize();
+        }
+        // rounded like the host's t0 + k * interval (no fused multiply-add)
+        double lt = __dadd_rn(a.t, __dmul_rn(double(a.first + f), a.interval));
+        for (uint64_t step = 0; step < a.nsteps; ++step) {
+            explicit_step<M, T, S>(y, lt, ldt, P, PD, F, delta);
+            lt += ldt;
+        }
     }
     bool finite = true;
 #pragma unroll

@@ -151,6 +151,7 @@ struct goss_batch {
     int32_t precision = 0;
     int32_t device = 0;
     uint32_t block = 128, grid = 0, schedule = 1;
+    uint32_t forwards_per_launch = 0;  // of a captured graph; 0: all
     uint32_t* d_counters = nullptr;
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -443,7 +444,9 @@ int batch_fail(goss_batch* b, int code, const char* msg)
     return fail(b ? &b->last_error : nullptr, code, "%s", msg);
 }
 
-int batch_launch(goss_batch* b, double t, double interval)
+// count consecutive forwards in one launch, forward f on
+// [t + (first + f) * interval, + interval)
+int batch_launch(goss_batch* b, double t, double interval, uint64_t first = 0, uint32_t count = 1)
 {
     std::vector<goss_batch_pop> pops(b->systems.size());
     for (size_t i = 0; i < pops.size(); ++i) {
@@ -470,6 +473,8 @@ int batch_launch(goss_batch* b, double t, double interval)
     L.counters = b->d_counters;
     L.t = t;
     L.interval = interval;
+    L.first_forward = first;
+    L.forwards = count;
     L.stream = b->stream;
     const int rc = b->d->launch(&L);
     if (rc)
@@ -618,8 +623,9 @@ GOSS_API int goss_batch_capture(goss_batch* b, double t0, double interval, uint3
     if (e != cudaSuccess)
         return fail(&b->last_error, GOSS_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
     int rc = 0;
-    for (uint32_t k = 0; k < num_steps && !rc; ++k)
-        rc = batch_launch(b, t0 + k * interval, interval);
+    const uint32_t per = b->forwards_per_launch ? b->forwards_per_launch : num_steps;
+    for (uint32_t k = 0; k < num_steps && !rc; k += per)
+        rc = batch_launch(b, t0, interval, k, std::min(per, num_steps - k));
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(b->stream, &g);
     if (rc) {
@@ -633,6 +639,14 @@ GOSS_API int goss_batch_capture(goss_batch* b, double t0, double interval, uint3
     e = cudaGraphInstantiate(&b->graph_exec, b->graph, 0);
     if (e != cudaSuccess)
         return fail(&b->last_error, GOSS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return 0;
+}
+
+GOSS_API int goss_batch_set_forwards_per_launch(goss_batch* b, uint32_t forwards)
+{
+    if (!b)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL batch");
+    b->forwards_per_launch = forwards;
     return 0;
 }
 

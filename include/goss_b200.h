@@ -232,8 +232,11 @@ typedef struct goss_batch_launch {
                                 2: persistent CTAs staging the next tile's rows in shared memory
                                    with bulk asynchronous copies (grid 0: all resident CTAs) */
     uint32_t* counters;      /* device [2], zero before the first launch */
-    double t;
-    double interval;
+    double t;                /* forward f of this launch runs on */
+    double interval;         /* [t + (first_forward + f) * interval, + interval) */
+    uint64_t first_forward;
+    uint32_t forwards;       /* consecutive forwards in this launch (0 or 1: one), the
+                                states kept on chip in between */
     void* stream;
 } goss_batch_launch;
 
@@ -349,6 +352,12 @@ GOSS_API int goss_batch_set_config(goss_batch* batch, uint32_t block, uint32_t g
                                    const uint32_t* order);
 GOSS_API int goss_batch_forward(goss_batch* batch, double t, double interval);
 GOSS_API int goss_batch_capture(goss_batch* batch, double t0, double interval, uint32_t num_steps);
+/* Forwards one launch of a captured graph performs (0, the default: all
+ * num_steps of the capture in one launch; 1: one launch per forward).  Every
+ * node's states stay in registers across the forwards of a launch; forward k
+ * still runs on [t0 + k*interval, t0 + (k+1)*interval) with the solver's
+ * internal steps, so the results do not depend on this setting. */
+GOSS_API int goss_batch_set_forwards_per_launch(goss_batch* batch, uint32_t forwards);
 GOSS_API int goss_batch_replay(goss_batch* batch);
 GOSS_API int goss_batch_time(goss_batch* batch, double t0, double interval, uint32_t num_steps, int32_t use_graph,
                              float* ms);

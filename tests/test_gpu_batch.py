@@ -99,6 +99,27 @@ def test_batch_graph_replay_equals_forwards():
         assert np.array_equal(x.states, y.states)
 
 
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_fused_forwards_bit_identical_to_one_launch_per_forward(precision):
+    """A captured graph runs its forwards all in one launch (the default),
+    one per launch, or in ragged groups: the states stay on chip between the
+    forwards of a launch (FP32 accumulators renormalised as a store and reload
+    would), so every grouping gives the direct forwards' states bit for bit."""
+    direct = make_pops(precision)
+    bd = goss.BatchSolver(direct)
+    for k in range(11):
+        bd.forward(0.5 + k * 0.02, 0.02)
+    for per, cfg in ((0, dict(block=128, grid=0, schedule=0)), (1, dict(block=64, grid=296, schedule=1)),
+                     (3, dict(block=128, grid=0, schedule=2)), (4, dict(block=96, grid=7, schedule=1))):
+        pops = make_pops(precision)
+        b = goss.BatchSolver(pops)
+        b.set_config(**cfg, forwards_per_launch=per)
+        b.capture(0.5, 0.02, 11)
+        b.replay()
+        for x, y in zip(direct, pops):
+            assert np.array_equal(x.states, y.states), (per, cfg)
+
+
 def test_system_graph_replay_equals_forwards():
     ode = goss.ParameterizedODE("tentusscher_panfilov_2006_M_cell")
     s1 = goss.ODESystemSolver(300, goss.solvers.GRL1(ode), ode)
