@@ -186,11 +186,37 @@ struct Acc<float> {
         lo = __fsub_rn(y, __fsub_rn(t, hi));
         hi = t;
     }
-    // between two forwards of one launch: exactly what store() to the FP64
-    // state array and load() by the next launch do.  An FP32 two-sum is not
-    // enough: when lo lies below FP64 precision of hi, the FP64 round trip
-    // rounds lo away and the two-sum keeps it
-    __device__ __forceinline__ void renormalize() { load(store()); }
+    // between two forwards of one launch: bit for bit what store() to the
+    // FP64 state array and load() by the next launch do, in FP32 arithmetic
+    // (five FP64 conversions per state would double the XU pipe's work on a
+    // one-step forward).  hi' = hi + lo rounded to FP32 and e its exact error
+    // (two-sum); the FP64 round trip keeps e only to the FP64 grid of hi + lo,
+    // g = 2^(floor(log2|hi + lo|) - 52), so e is rounded to a multiple of g
+    // (ties to even) by adding and subtracting P = 2^23 g with e's sign, which
+    // is exact for |e| < P; larger e are multiples of g already.  hi + lo lies
+    // one binade below hi' when hi' is a power of two and e has the opposite
+    // sign.  Sums below 2^-72 (where flushed FP32 subnormals would differ
+    // from the FP64 grid) and non-finite sums take the FP64 round trip itself.
+    __device__ __forceinline__ void renormalize()
+    {
+        const float t = __fadd_rn(hi, lo);
+        const float at = fabsf(t);
+        if (!(at >= 0x1p-72f && at <= 3.402823466e38f)) {
+            load(store());
+            return;
+        }
+        const float bp = __fsub_rn(t, hi);
+        const float ap = __fsub_rn(t, bp);
+        const float e = __fadd_rn(__fsub_rn(hi, ap), __fsub_rn(lo, bp));
+        const float pow2 = __uint_as_float(__float_as_uint(t) & 0x7f800000u);
+        float P = __fmul_rn(pow2, 0x1p-29f);
+        if (at == pow2 && e != 0.0f && signbit(e) != signbit(t))
+            P = __fmul_rn(P, 0.5f);
+        const float C = copysignf(P, e);
+        const float r = __fsub_rn(__fadd_rn(e, C), C);
+        lo = fabsf(e) < P ? r : e;
+        hi = t;
+    }
 };
 
 // Where one node's explicit solve reads and writes (shared by the
