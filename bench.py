@@ -428,14 +428,30 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
         torch.cuda.synchronize()
         return g.cpu().numpy(), e0.elapsed_time(e1), e2.elapsed_time(e3), float(((v - target) ** 2).sum())
 
-    tr64 = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="double")
+    def tape_bytes(tr):
+        return 0 if tr._tape is None else tr._tape.numel() * tr._tape.element_size()
+
+    # the record pass tapes as many of the last segments as the free HBM holds
+    torch.cuda.empty_cache()
+    tr64 = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="double",
+                     tape_bytes="auto")
     target = tr64.run_forward(fb, y0t).clone()
     g64, fwd64, bwd64, loss64 = grad(tr64, warm=False)
+    tape64 = (tr64.taped_segments, tape_bytes(tr64))
     del tr64
-    tr32 = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="single")
+    torch.cuda.empty_cache()
+    tr32 = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="single",
+                     tape_bytes="auto")
     g32, fwd32, bwd32, loss32 = grad(tr32)
     cp_bytes = tr32._checkpoints.numel() * tr32._checkpoints.element_size()
+    tape32 = (tr32.taped_segments, tape_bytes(tr32))
     del tr32
+    torch.cuda.empty_cache()
+    # every segment recomputed from its checkpoint (no tape)
+    tr32r = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="single")
+    g32r, fwd32r, bwd32r, _ = grad(tr32r)
+    del tr32r
+    torch.cuda.empty_cache()
 
     # one plain FP32 forward solve of the same loop (ODESystemSolver, persistent kernel per interval)
     solver = goss.solvers.GRL1(ode)
@@ -464,11 +480,18 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
         "workload": f"TP06 GRL1 dt=0.01ms, {nodes} nodes, {num_intervals} ms ({num_intervals * steps_per_interval} "
                     f"steps), V every 1 ms, 4 lognormal conductance fields, checkpoints every {checkpoint_every} "
                     "steps",
-        "fp32": {"forward_record_ms": fwd32, "backward_ms": bwd32, "loss": loss32},
-        "fp64": {"forward_record_ms": fwd64, "backward_ms": bwd64, "loss": loss64},
+        "fp32": {"forward_record_ms": fwd32, "backward_ms": bwd32, "loss": loss32,
+                 "taped_segments": tape32[0], "tape_bytes": int(tape32[1])},
+        "fp64": {"forward_record_ms": fwd64, "backward_ms": bwd64, "loss": loss64,
+                 "taped_segments": tape64[0], "tape_bytes": int(tape64[1]),
+                 "gradient_over_record": (fwd64 + bwd64) / fwd64},
+        "segments": -(-num_intervals * steps_per_interval // checkpoint_every),
         "plain_forward_fp32_ms": plain,
         "backward_over_plain_forward": bwd32 / plain,
         "gradient_over_plain_forward": (fwd32 + bwd32) / plain,
+        "fp32_recompute_all": {"forward_record_ms": fwd32r, "backward_ms": bwd32r,
+                               "gradient_over_plain_forward": (fwd32r + bwd32r) / plain,
+                               "max_rel_diff_vs_taped": float(np.abs(g32 - g32r).max() / np.abs(g32r).max())},
         "checkpoint_bytes_fp32": int(cp_bytes),
         "grad_rel_err_fp32_vs_fp64": {"per_field_scaled_max": {f: float(e) for f, e in zip(FIELDS, col_err)},
                                       "elementwise_median": float(np.median(elem)),

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import numbers
 from typing import Optional, Tuple
 
 import numpy as np
@@ -43,13 +44,22 @@ class SolverTrace:
     interval), num_intervals, checkpoint_every (internal steps; a multiple of
     steps_per_interval), trace_state (state name), precision ("single" or
     "double"), t0, device, solver ("GRL1" or "RK4").
+
+    tape_bytes: device memory for a tape of every step's input state over the
+    last checkpoint segments (0, the default: none; an int: at most that many
+    bytes; ``"auto"``: the free device memory less ``tape_reserve`` bytes).
+    The record pass writes the tape and the backward reads it instead of
+    recomputing those segments from their checkpoints; the tape holds the
+    values the recompute produces, so the gradient does not depend on it
+    beyond rounding.  ``taped_segments`` reports how many segments fit.
     """
 
     SOLVERS = {"GRL1": _capi.GOSS_GRL1, "RK4": _capi.GOSS_RK4}
 
     def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
                  num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
-                 t0: float = 0.0, device: int = 0, solver: str = "GRL1"):
+                 t0: float = 0.0, device: int = 0, solver: str = "GRL1", tape_bytes=0,
+                 tape_reserve: int = 2 << 30):
         import torch
 
         if solver not in self.SOLVERS:
@@ -78,7 +88,16 @@ class SolverTrace:
         rows = 2 * self.n if self.precision == _capi.GOSS_FP32 else self.n
         dev = self.device
         self._checkpoints = torch.zeros((self.num_checkpoints, rows, self.ld), dtype=cp_dtype, device=dev)
-        self._scratch = torch.zeros((self.K, self.n, (self.N + 255) // 256 * 256 + 256), dtype=cp_dtype, device=dev)
+        sld = (self.N + 255) // 256 * 256 + 256
+        self._scratch = torch.zeros((self.K, self.n, sld), dtype=cp_dtype, device=dev)
+        segment_bytes = self.K * self.n * sld * self._scratch.element_size()
+        if tape_bytes == "auto":
+            tape_bytes = torch.cuda.mem_get_info(dev)[0] - int(tape_reserve)
+        elif not isinstance(tape_bytes, numbers.Integral) or isinstance(tape_bytes, bool):
+            raise TypeError("tape_bytes must be an int or 'auto'")
+        self.taped_segments = int(min(self.num_checkpoints, max(0, int(tape_bytes)) // segment_bytes))
+        self._tape = (torch.empty((self.taped_segments, self.K, self.n, sld), dtype=cp_dtype, device=dev)
+                      if self.taped_segments else None)
         self._states = torch.zeros((self.n, self.ld), dtype=torch.float64, device=dev)
         self._fp = torch.zeros((max(self.nfp, 1), self.ld), dtype=torch.float64, device=dev)
         self._trace = torch.zeros((self.J, self.ld), dtype=torch.float64, device=dev)
@@ -116,6 +135,8 @@ class SolverTrace:
         L.field_params_bar = fp_bar.data_ptr() if fp_bar is not None else None
         L.states_bar = states_bar.data_ptr() if states_bar is not None else None
         L.flags = self._flags.data_ptr()
+        L.tape = self._tape.data_ptr() if self._tape is not None else None
+        L.taped_segments = self.taped_segments
         L.stream = torch.cuda.current_stream(self.device).cuda_stream
         rc = self._fn(C.byref(L))
         _capi.check(rc)
@@ -158,9 +179,10 @@ class GRL1Trace(SolverTrace):
 
     def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
                  num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
-                 t0: float = 0.0, device: int = 0):
+                 t0: float = 0.0, device: int = 0, tape_bytes=0, tape_reserve: int = 2 << 30):
         super().__init__(ode, num_nodes, interval, steps_per_interval, num_intervals, checkpoint_every,
-                         trace_state, precision, t0, device, solver="GRL1")
+                         trace_state, precision, t0, device, solver="GRL1", tape_bytes=tape_bytes,
+                         tape_reserve=tape_reserve)
 
 
 class RK4Trace(SolverTrace):
@@ -168,9 +190,10 @@ class RK4Trace(SolverTrace):
 
     def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
                  num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
-                 t0: float = 0.0, device: int = 0):
+                 t0: float = 0.0, device: int = 0, tape_bytes=0, tape_reserve: int = 2 << 30):
         super().__init__(ode, num_nodes, interval, steps_per_interval, num_intervals, checkpoint_every,
-                         trace_state, precision, t0, device, solver="RK4")
+                         trace_state, precision, t0, device, solver="RK4", tape_bytes=tape_bytes,
+                         tape_reserve=tape_reserve)
 
 
 def _function():

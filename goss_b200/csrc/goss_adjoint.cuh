@@ -124,6 +124,7 @@ struct AdjointArgs {
     double* trace;             // [J][ld]
     const double* trace_bar;   // [J][ld]
     T* scratch;                // [K][n][sld], sld = num_nodes rounded up to 256, plus 256
+    T* tape;                   // [taped_segments][K][n][sld]: step inputs of the last segments
     double* fparams_bar;       // [nfp][ld]
     double* states_bar;        // [n][ld]
     uint32_t* flags;
@@ -134,6 +135,7 @@ struct AdjointArgs {
     uint32_t steps_per_interval;  // S
     uint32_t checkpoint_every;    // K (multiple of S)
     uint32_t trace_state;
+    uint32_t taped_segments;
     double t0;
     double interval;
     T P[Dims<M>::np];
@@ -186,6 +188,12 @@ __global__ void __launch_bounds__(128) record_kernel(const __grid_constant__ Adj
     const uint32_t S_ = a.steps_per_interval, K = a.checkpoint_every;
     const double ldt = a.interval / S_;
     constexpr int rows = cp_rows<T>(n);
+    // the last taped_segments segments keep every step's input state: the
+    // values the backward's recompute would write to its scratch
+    const uint64_t total = (uint64_t)a.num_intervals * S_;
+    const uint64_t num_cp = (total + K - 1) / K;
+    const uint64_t tape_from = (num_cp - a.taped_segments) * K;
+    T* const tape = a.tape + node;
     for (uint32_t j = 0; j < a.num_intervals; ++j) {
         const uint64_t g = (uint64_t)j * S_;
         if (g % K == 0) {
@@ -195,6 +203,11 @@ __global__ void __launch_bounds__(128) record_kernel(const __grid_constant__ Adj
         }
         double lt = a.t0 + j * a.interval;
         for (uint32_t s = 0; s < S_; ++s) {
+            if (g + s >= tape_from) {
+                const uint64_t row = (g + s - tape_from) * n;
+                for (int i = 0; i < n; ++i)
+                    tape[(row + i) * a.sld] = y[i].value();
+            }
             explicit_step<M, T, S>(y, lt, ldt, a.P, a.PD, F, T(kGrlDelta));
             lt += ldt;
         }
@@ -336,19 +349,25 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
             }
         }
         __syncthreads();
-        // recompute the segment, keeping the input state of every step
-        Acc<T> y[n];
-        for (int i = 0; i < n; ++i)
-            cp_load(a.checkpoints, ((uint64_t)c * rows + i) * a.ld + src, ((uint64_t)c * rows + n + i) * a.ld + src,
-                    y[i]);
-        for (uint32_t k = 0; k < len; ++k) {
+        // the input state of every step of the segment: from the record's
+        // tape, or recomputed from the checkpoint into scratch
+        const T* seg = scratch;
+        if ((uint32_t)c >= num_cp - a.taped_segments) {
+            seg = a.tape + (uint64_t)(c - (num_cp - a.taped_segments)) * K * n * a.sld + src;
+        } else {
+            Acc<T> y[n];
             for (int i = 0; i < n; ++i)
-                scratch[((uint64_t)k * n + i) * a.sld] = y[i].value();
-            if (k + 1 < len)
-                explicit_step<M, T, S>(y, s_time[k], ldt, a.P, a.PD, F, T(kGrlDelta));
+                cp_load(a.checkpoints, ((uint64_t)c * rows + i) * a.ld + src,
+                        ((uint64_t)c * rows + n + i) * a.ld + src, y[i]);
+            for (uint32_t k = 0; k < len; ++k) {
+                for (int i = 0; i < n; ++i)
+                    scratch[((uint64_t)k * n + i) * a.sld] = y[i].value();
+                if (k + 1 < len)
+                    explicit_step<M, T, S>(y, s_time[k], ldt, a.P, a.PD, F, T(kGrlDelta));
 #if GOSS_ADJOINT_LOCKSTEP
-            __syncthreads();
+                __syncthreads();
 #endif
+            }
         }
         // reverse through the segment
         for (int k = (int)len - 1; k >= 0; --k) {
@@ -359,7 +378,7 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
             }
             T yt[n];
             for (int i = 0; i < n; ++i)
-                yt[i] = scratch[((uint64_t)k * n + i) * a.sld];
+                yt[i] = seg[((uint64_t)k * n + i) * a.sld];
             if constexpr (S == Explicit::GRL1)
                 reverse_step_grl1<M, T>(yt, s_time[k], ldt, a.P, a.PD, F, lam, gF);
             else
@@ -420,6 +439,8 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
     a.trace = L->trace;
     a.trace_bar = L->trace_bar;
     a.scratch = static_cast<T*>(L->scratch);
+    a.tape = static_cast<T*>(L->tape);
+    a.taped_segments = L->taped_segments;
     a.fparams_bar = L->field_params_bar;
     a.states_bar = L->states_bar;
     a.flags = L->flags;
@@ -437,6 +458,12 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
     if (a.steps_per_interval == 0 || a.checkpoint_every == 0 || a.checkpoint_every % a.steps_per_interval ||
         a.trace_state >= (uint32_t)M::num_states)
         return GOSS_ERR_ARGUMENT;
+    {
+        const uint64_t total = (uint64_t)a.num_intervals * a.steps_per_interval;
+        const uint64_t num_cp = (total + a.checkpoint_every - 1) / a.checkpoint_every;
+        if (a.taped_segments > num_cp || (a.taped_segments && !a.tape))
+            return GOSS_ERR_ARGUMENT;
+    }
     // room for grid * block <= round_up(num_nodes, block) for any block <= 256
     a.sld = ((uint64_t)L->num_nodes + 255) / 256 * 256 + 256;
     if (L->num_nodes == 0)

@@ -35,7 +35,7 @@ extern "C" {
 #define GOSS_API
 #endif
 
-#define GOSS_B200_ABI_VERSION 2u
+#define GOSS_B200_ABI_VERSION 3u
 
 /* Solver kinds: the reference solver classes on this path. */
 enum goss_solver_kind {
@@ -140,7 +140,12 @@ typedef struct goss_eval_launch {
  *   mode 1 (backward): trace_bar [J][ld] = dLoss/dtrace -> field_params_bar
  *     [nfp][ld] = dLoss/dfield_params and states_bar [n][ld] = dLoss/dstates
  *     (initial); scratch holds [K][n][round_up(num_nodes, 256) + 256] values
- *     of the arithmetic type (K = checkpoint_every). */
+ *     of the arithmetic type (K = checkpoint_every).
+ *   tape (both modes, may be NULL with taped_segments 0): the input state of
+ *     every step of the last taped_segments checkpoint segments, written by
+ *     the record and read by the backward in place of recomputing those
+ *     segments; [taped_segments][K][n][round_up(num_nodes, 256) + 256]
+ *     values of the arithmetic type (the scratch layout per segment). */
 typedef struct goss_adjoint_launch {
     int32_t mode;
     int32_t solver;           /* GOSS_GRL1 */
@@ -167,6 +172,8 @@ typedef struct goss_adjoint_launch {
     double* states_bar;
     uint32_t* flags;
     void* stream;
+    void* tape;
+    uint32_t taped_segments;  /* <= C */
 } goss_adjoint_launch;
 
 /* A compiled model: produced by the code generator for one .ode model and one

@@ -142,7 +142,7 @@ CASES = [  # model, field parameters, solver, steps per 1 ms interval, intervals
 CASE_IDS = [f"{m.split('_')[0]}-{s}" for m, _, s, _, _ in CASES]
 
 
-def case_setup(case, precision="double", nodes=16, K=None, seed=4):
+def case_setup(case, precision="double", nodes=16, K=None, seed=4, tape_segments=0):
     import torch
     from goss_b200.adjoint import SolverTrace
 
@@ -154,7 +154,10 @@ def case_setup(case, precision="double", nodes=16, K=None, seed=4):
     fp_target = defaults[None, :] * np.exp(0.2 * rng.standard_normal((nodes, len(fields))))
     y0 = ode.get_ic()[None, :] * (1 + rng.uniform(-0.02, 0.02, (nodes, ode.num_states)))
     K = K or steps * 4
-    tr = SolverTrace(ode, nodes, 1.0, steps, intervals, K, precision=precision, solver=solver)
+    sld = (nodes + 255) // 256 * 256 + 256
+    segment_bytes = K * ode.num_states * sld * (4 if precision == "single" else 8)
+    tr = SolverTrace(ode, nodes, 1.0, steps, intervals, K, precision=precision, solver=solver,
+                     tape_bytes=tape_segments * segment_bytes)
     target = tr.run_forward(torch.tensor(fp_target, device="cuda"), torch.tensor(y0, device="cuda")).clone()
     return ode, tr, fp, y0, target
 
@@ -199,3 +202,34 @@ def test_case_fp32_adjoint_close_to_tangent_linear(case):
     _, tr32, _, _, _ = case_setup(case, "single")
     _, g32, _ = loss_grad(tr32, fp, y0, target)
     assert column_rel_err(g32, ref) < 2e-3
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("case", CASES, ids=CASE_IDS)
+def test_case_tape_does_not_change_gradient(case, precision):
+    """Segments taped by the record pass (all of them, or the last half) give
+    the gradient of the recomputed segments: the tape holds the states the
+    recompute reproduces."""
+    ode, tr0, fp, y0, target = case_setup(case, precision)
+    assert tr0.taped_segments == 0
+    _, g0, s0 = loss_grad(tr0, fp, y0, target, with_states=True)
+    num_cp = tr0.num_checkpoints
+    for segments in (num_cp, num_cp // 2):
+        _, tr, _, _, _ = case_setup(case, precision, tape_segments=segments)
+        assert tr.taped_segments == segments
+        _, g, s = loss_grad(tr, fp, y0, target, with_states=True)
+        bar = 1e-10 if precision == "double" else 1e-6
+        assert np.abs(g - g0).max() <= bar * np.abs(g0).max(), (segments, np.abs(g - g0).max() / np.abs(g0).max())
+        assert np.abs(s - s0).max() <= bar * np.abs(s0).max(), (segments, np.abs(s - s0).max() / np.abs(s0).max())
+
+
+def test_tape_size_arguments():
+    from goss_b200.adjoint import SolverTrace
+
+    ode = goss.ParameterizedODE(MODEL, field_parameters=F4)
+    t = SolverTrace(ode, 24, INTERVAL, S, J, 400, tape_bytes=1 << 40)
+    assert t.taped_segments == t.num_checkpoints == 4  # clamped to the segments there are
+    assert SolverTrace(ode, 24, INTERVAL, S, J, 400, tape_bytes=1000).taped_segments == 0
+    assert SolverTrace(ode, 24, INTERVAL, S, J, 400, tape_bytes="auto").taped_segments == 4
+    with pytest.raises(TypeError):
+        SolverTrace(ode, 24, INTERVAL, S, J, 400, tape_bytes=1.5)
