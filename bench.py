@@ -387,9 +387,11 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
     TP06 M-cell, GRL1 dt = 0.01 ms, 65,536 nodes, 400 ms (40,000 steps), V
     sampled every 1 ms; fields lognormal sigma 0.2 (seed A), the target trace
     from an FP64 solve with seed-B fields; loss = sum (V - V_target)^2;
-    checkpoints every 100 steps.  Times (CUDA events on the launch stream)
-    the FP32 recording forward, the FP32 adjoint and, for the cost ratio, one
-    plain FP32 forward solve of the same 400 ms loop through ODESystemSolver;
+    checkpoints every 100 steps, the last segments that fit in free HBM taped
+    by the record pass.  Times (CUDA events on the launch stream) the FP32
+    recording forward, the FP32 adjoint (with and without the tape) and, for
+    the cost ratio, one plain FP32 forward solve of the same 400 ms loop
+    through ODESystemSolver;
     the FP32 gradient is compared with the FP64 adjoint's (itself checked
     against the FP64 tangent-linear reference in the tests)."""
     import torch
