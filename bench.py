@@ -50,11 +50,14 @@ def _args():
     ap.add_argument("--impl", default="goss_b200", choices=["goss_b200", "reference"])
     ap.add_argument("--nodes", type=int, default=N_NODES)
     ap.add_argument("--skip-fp64", action="store_true", help=argparse.SUPPRESS)
-    ap.add_argument("--profile", choices=["single", "double", "adjoint-single", "adjoint-double"] + list(_IMPLICIT_PROFILES),
+    ap.add_argument("--profile", choices=["single", "double", "adjoint-single", "adjoint-double", "batch"]
+                    + list(_IMPLICIT_PROFILES),
                     default=None,
                     help="only run the timed forward loop in one precision, one adjoint gradient "
-                         "(65,536 nodes x 2,000 steps) or W+K intervals of one implicit solver on "
-                         "65,536 nodes of the implicit workload, for ncu captures")
+                         "(65,536 nodes x 2,000 steps), W+K intervals of one implicit solver on "
+                         "65,536 nodes of the implicit workload, or W+K launches of a 20-forward "
+                         "batch graph over the six populations at a quarter of their sizes, for ncu "
+                         "captures")
     return ap.parse_args()
 
 
@@ -85,6 +88,27 @@ def profile_run(args):
             system.forward(k * IMPLICIT_DT, IMPLICIT_DT)
         print(json.dumps({"profile": args.profile, "nodes": nodes, "intervals": args.warmup + args.steps,
                           "finite": bool(np.isfinite(system.states).all())}))
+        return
+
+    if args.profile == "batch":
+        rng = np.random.default_rng(SEED)
+        systems = []
+        for model, fps, solver_name, n in BATCH_POPS:
+            n = max(3, n // 4)
+            ode = goss.ParameterizedODE(model, field_parameters=fps)
+            s = goss.solvers.solver_mapper[solver_name](ode)
+            s.internal_time_step = LDT
+            sysm = goss.ODESystemSolver(n, s, ode, precision="single")
+            sysm.set_states(ode.get_ic()[None, :] * (1 + rng.uniform(-0.1, 0.1, (n, ode.num_states))))
+            systems.append(sysm)
+        batch = goss.BatchSolver(systems)
+        batch.set_config(block=128, grid=0, schedule=0)
+        batch.capture(0.0, LDT, 20)  # 20 one-step forwards, one launch
+        for _ in range(args.warmup + args.steps):
+            batch.replay()
+        states = [s.states for s in systems]
+        print(json.dumps({"profile": args.profile, "nodes": batch.total_nodes, "launches": args.warmup + args.steps,
+                          "finite": bool(all(np.isfinite(y).all() for y in states))}))
         return
 
     if args.profile.startswith("adjoint"):

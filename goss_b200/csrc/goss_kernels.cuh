@@ -193,10 +193,11 @@ struct Acc<float> {
     // (two-sum); the FP64 round trip keeps e only to the FP64 grid of hi + lo,
     // g = 2^(floor(log2|hi + lo|) - 52), so e is rounded to a multiple of g
     // (ties to even) by adding and subtracting P = 2^23 g with e's sign, which
-    // is exact for |e| < P; larger e are multiples of g already.  hi + lo lies
-    // one binade below hi' when hi' is a power of two and e has the opposite
-    // sign.  Sums below 2^-72 (where flushed FP32 subnormals would differ
-    // from the FP64 grid) and non-finite sums take the FP64 round trip itself.
+    // is exact for |e| < P; larger e are multiples of g already.  The binade
+    // of hi + lo is that of hi' + e rounded toward zero (one below hi' when
+    // hi' is a power of two and e has the opposite sign).  Sums below 2^-72
+    // (where flushed FP32 subnormals would differ from the FP64 grid) and
+    // non-finite sums take the FP64 round trip itself.
     __device__ __forceinline__ void renormalize()
     {
         const float t = __fadd_rn(hi, lo);
@@ -208,10 +209,8 @@ struct Acc<float> {
         const float bp = __fsub_rn(t, hi);
         const float ap = __fsub_rn(t, bp);
         const float e = __fadd_rn(__fsub_rn(hi, ap), __fsub_rn(lo, bp));
-        const float pow2 = __uint_as_float(__float_as_uint(t) & 0x7f800000u);
-        float P = __fmul_rn(pow2, 0x1p-29f);
-        if (at == pow2 && e != 0.0f && signbit(e) != signbit(t))
-            P = __fmul_rn(P, 0.5f);
+        const float pow2 = __uint_as_float(__float_as_uint(__fadd_rz(t, e)) & 0x7f800000u);
+        const float P = __fmul_rn(pow2, 0x1p-29f);
         const float C = copysignf(P, e);
         const float r = __fsub_rn(__fadd_rn(e, C), C);
         lo = fabsf(e) < P ? r : e;

@@ -22,6 +22,15 @@ def round_trip(hi, lo):
     return h, lo2
 
 
+def add_rz(a, b):
+    """FP32 a + b rounded toward zero (the sum is exact in FP64 here: |b| is
+    at most half an FP32 ulp of a)."""
+    v = a.astype(np.float64) + b.astype(np.float64)
+    f = v.astype(np.float32)
+    away = np.abs(f.astype(np.float64)) > np.abs(v)
+    return np.where(away, np.nextafter(f, np.float32(0)), f)
+
+
 def renormalize_fp32(hi, lo):
     """The kernel's FP32 form, operation for operation."""
     f = np.float32
@@ -29,10 +38,9 @@ def renormalize_fp32(hi, lo):
     bp = t - hi
     ap = t - bp
     e = (hi - ap) + (lo - bp)
-    pow2 = (t.view(np.uint32) & np.uint32(0x7F800000)).view(np.float32)  # 2^floor(log2|t|)
-    P = pow2 * f(2.0**-29)  # 2^23 x the FP64 ulp of hi + lo in t's binade
-    down = (np.abs(t) == pow2) & (e != 0) & (np.signbit(e) != np.signbit(t))
-    P = np.where(down, P * f(0.5), P)  # hi + lo lies in the binade below t
+    # 2^floor(log2|hi + lo|): the binade of hi + lo rounded toward zero
+    pow2 = (add_rz(t, e).view(np.uint32) & np.uint32(0x7F800000)).view(np.float32)
+    P = pow2 * f(2.0**-29)  # 2^23 x the FP64 ulp of hi + lo
     C = np.copysign(P, e)
     r = (e + C) - C
     lo2 = np.where(np.abs(e) < P, r, e)
