@@ -522,6 +522,44 @@ class ModelSource:
                     lines.append(f"{name}[{i}] = T(0.0);")
         return lines
 
+    def _dev_split_column_lines(self) -> List[str]:
+        """Body of ``rhs_split_column``: for the forward-difference column
+        ``i``, only the rows where column i of the Jacobian is structurally
+        non-zero (the rows the column reads), each computed by the statements
+        of ``rhs_split`` it depends on -- the same expressions, a subset."""
+        folded = self._fold(self.rhs)
+        inter = {n: self.model.sym(n) for n in self.model.intermediates}
+        rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
+                            [self.model.sym(p) for p in self.fparams], inter, reverse=False)
+        prT, prD = self._dev_printers(split=True)
+        binds = {b.name: b for b in rp.forward}
+        outs = {o.index: o for o in rp.outputs if o.array == "values"}
+        n = len(self.states)
+        lines = ["switch (i) {"]
+        for i in range(n):
+            rows = [r for r in range(n) if self.lus.jac[r][i] and r in outs]
+            need, stack = set(), [sym.name for r in rows for sym in outs[r].expr.free_symbols]
+            while stack:
+                name = stack.pop()
+                if name in binds and name not in need:
+                    need.add(name)
+                    stack += [sym.name for sym in binds[name].expr.free_symbols]
+            lines.append(f"case {i}: {{")
+            for b in rp.forward:
+                if b.name not in need:
+                    continue
+                if b.cls == TIME_CLS:
+                    lines.append(f"  const double v_{b.name} = {prD(b.expr)};")
+                else:
+                    lines.append(f"  const T v_{b.name} = {prT(factor_common(b.expr))};")
+            for r in rows:
+                lines.append(f"  values[{r}] = {prT(factor_common(outs[r].expr))};")
+            lines.append("  break;")
+            lines.append("}")
+        lines.append("default: break;")
+        lines.append("}")
+        return lines
+
     def _derived_host_lines(self) -> List[str]:
         """Host code filling C[k] with the derived constants from P."""
         def sym(s):
@@ -622,6 +660,15 @@ class ModelSource:
         L.append("  {")
         L += ["    " + x for x in head + self._dev_split_lines(self.rhs, {"values": "values"})]
         L.append("    (void)time; (void)P; (void)PD; (void)F;")
+        L.append("  }")
+        L.append("")
+        L.append("  // the rows of rhs_split that column i of a forward-difference Jacobian reads (those")
+        L.append("  // where column i is structurally non-zero), by the statements they depend on")
+        L.append("  template <typename T>")
+        L.append(f"  __device__ static __forceinline__ void rhs_split_column(const int i, {sig}, T* __restrict__ values)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_split_column_lines()]
+        L.append("    (void)time; (void)P; (void)PD; (void)F; (void)values;")
         L.append("  }")
         L.append("")
         L.append("  // vector-Jacobian product of linearized (reverse mode, generated): after the forward")

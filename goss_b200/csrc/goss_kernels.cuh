@@ -459,6 +459,20 @@ struct PackedRows {
     __device__ __forceinline__ double& operator[](int k) const { return base[(uint64_t)k * ld]; }
 };
 
+// ... or in a tiled region: the 32 nodes of a tile keep their entries together
+// ([tile][k][32]), so a warp's lu_nnz entries are one contiguous block of
+// 256-byte rows instead of lu_nnz rows ld apart (each 2 MiB apart at 262,144
+// nodes, whose cost depended on how the allocation happened to be mapped)
+struct PackedTile {
+    double* base;
+    __device__ __forceinline__ double& operator[](int k) const { return base[(uint64_t)k * 32]; }
+};
+
+__device__ __forceinline__ PackedTile packed_tile(double* region, uint32_t node, int nnz)
+{
+    return PackedTile{region + (((uint64_t)(node >> 5) * (uint64_t)nnz) << 5) + (node & 31u)};
+}
+
 template <int n>
 __device__ __forceinline__ double l2norm(const double* v)
 {
@@ -489,6 +503,18 @@ __device__ __forceinline__ void rhs64(const double* y, double t, const double* P
         M::template rhs<double>(y, t, P, P, F, out);
 }
 
+// f(y, t) at the rows column i of a forward-difference Jacobian reads (the
+// other entries of out are left as they are)
+template <class M>
+__device__ __forceinline__ void rhs64_column(int i, const double* y, double t, const double* P, const double* F,
+                                             double* out)
+{
+    if constexpr (GOSS_IMPLICIT_SPLIT)
+        M::template rhs_split_column<double>(i, y, t, P, P, F, out);
+    else
+        M::template rhs<double>(y, t, P, P, F, out);
+}
+
 template <class M, class A>
 __device__ __forceinline__ void jacobian64(const double* y, double t, const double* P, const double* F, A J)
 {
@@ -503,10 +529,16 @@ __device__ __forceinline__ void jacobian64(const double* y, double t, const doub
 // the same arguments), stored at the column's structural rows (the other
 // rows are exactly 0 in the reference too).  The perturbed state is built by
 // selects over compile-time indices, so y stays in registers (the reference
-// perturbs y[i] in place and restores it: the same values).
-template <class M, class A>
-__device__ void compute_jacobian(const double* y, double t, const double* P, const double* F, A J,
-                                 const double* f1)
+// perturbs y[i] in place and restores it: the same values).  With Rows, each
+// f(y + delta_i e_i) evaluates only the rows column i stores (its structural
+// non-zeros), by the statements of the split right-hand side they depend on:
+// 33-44 % of the work of n full evaluations on TT04.  Measured on B200 (TT04,
+// 262,144 nodes): ThetaSolver 4.43 -> 3.59 ms per 0.1 ms interval; ESDIRK23a,
+// which computes its Jacobian at three inlined call sites, is faster with the
+// full evaluations (255 against 836 ms: the column switch triples its code).
+template <class M, bool Rows = true, class A>
+__device__ __forceinline__ void compute_jacobian(const double* y, double t, const double* P, const double* F, A J,
+                                                 const double* f1)
 {
     constexpr int n = M::num_states;
     if constexpr (M::has_jacobian) {
@@ -526,7 +558,10 @@ __device__ void compute_jacobian(const double* y, double t, const double* P, con
 #pragma unroll
             for (int k = 0; k < n; ++k)
                 yp[k] = (k == i) ? ysafe + delta : y[k];
-            rhs64<M>(yp, t, P, F, f2);
+            if constexpr (Rows)
+                rhs64_column<M>(i, yp, t, P, F, f2);
+            else
+                rhs64<M>(yp, t, P, F, f2);
             M::fd_column(i, f1, f2, delta, J);
         }
     }
@@ -639,7 +674,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
             newton_done = true;
         } else {
             if (recompute || always) {
-                compute_jacobian<M>(yz, tn, a.P, F, J, f1);
+                compute_jacobian<M, true>(yz, tn, a.P, F, J, f1);
                 M::lu_shift(J, -ldt * alpha);
                 M::lu_factorize(J);
                 jac_comp += 1;
@@ -749,7 +784,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
 // ---------------------------------------------------------------------------
 enum EsdirkRows {
     ES_PREV_DT = 0, ES_LOC_ERROR, ES_ETA, ES_NEWTON_IT, ES_FIRST, ES_NEWJAC, ES_JACCOMP, ES_REJECTS, ES_ACCEPTED,
-    ES_SCALARS  // the packed jac[lu_nnz] and jfac[lu_nnz] follow
+    ES_SCALARS  // then the packed jac and jfac, each lu_nnz x ld values tiled [ld/32][lu_nnz][32]
 };
 
 struct EsdirkCoef {
@@ -796,7 +831,7 @@ struct EsdirkNode {
     const double* F;
     const goss_solver_params* sp;
     EsdirkCoef c;
-    PackedRows jac, jfac;
+    PackedTile jac, jfac;
     double prev_dt, loc_error, eta, dt;
     int newton_iterations, first_step, new_jacobian;
     double jac_comp, rejects, accepted;
@@ -807,7 +842,7 @@ struct EsdirkNode {
     __device__ void ode_jacobian(double* y, double t)
     {
         rhs64<M>(y, t, P, F, g1);
-        compute_jacobian<M>(y, t, P, F, jac, g1);
+        compute_jacobian<M, false>(y, t, P, F, jac, g1);
         jac_comp += 1;
         new_jacobian = 1;
     }
@@ -941,8 +976,8 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
     s.F = F;
     s.sp = &a.sp;
     s.c = esdirk_coefficients();
-    s.jac = PackedRows{ss + (uint64_t)ES_SCALARS * ld, ld};
-    s.jfac = PackedRows{ss + (uint64_t)(ES_SCALARS + M::lu_nnz) * ld, ld};
+    s.jac = packed_tile(a.sstate + (uint64_t)ES_SCALARS * ld, node, M::lu_nnz);
+    s.jfac = packed_tile(a.sstate + (uint64_t)(ES_SCALARS + M::lu_nnz) * ld, node, M::lu_nnz);
     s.prev_dt = ss[ES_PREV_DT * ld];
     s.loc_error = ss[ES_LOC_ERROR * ld];
     s.eta = ss[ES_ETA * ld];

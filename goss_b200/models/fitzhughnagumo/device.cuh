@@ -156,6 +156,33 @@ struct M_fitzhughnagumo {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
+  // the rows of rhs_split that column i of a forward-difference Jacobian reads (those
+  // where column i is structurally non-zero), by the statements they depend on
+  template <typename T>
+  __device__ static __forceinline__ void rhs_split_column(const int i, const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  {
+    const T s_V = y[0];
+    const T s_s = y[1];
+    switch (i) {
+    case 0: {
+      const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
+      const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+      values[0] = (v_I + T(v_i_Stim));
+      values[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
+      break;
+    }
+    case 1: {
+      const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
+      const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+      values[0] = (v_I + T(v_i_Stim));
+      values[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
+      break;
+    }
+    default: break;
+    }
+    (void)time; (void)P; (void)PD; (void)F; (void)values;
+  }
+
   // vector-Jacobian product of linearized (reverse mode, generated): after the forward
   // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
   // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters

@@ -137,6 +137,27 @@ struct M_oscilator__5dc98ee0 {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
+  // the rows of rhs_split that column i of a forward-difference Jacobian reads (those
+  // where column i is structurally non-zero), by the statements they depend on
+  template <typename T>
+  __device__ static __forceinline__ void rhs_split_column(const int i, const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    switch (i) {
+    case 0: {
+      values[1] = (F[1]*s_x);
+      break;
+    }
+    case 1: {
+      values[0] = (-(F[0]*s_y));
+      break;
+    }
+    default: break;
+    }
+    (void)time; (void)P; (void)PD; (void)F; (void)values;
+  }
+
   // vector-Jacobian product of linearized (reverse mode, generated): after the forward
   // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
   // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters
