@@ -522,42 +522,69 @@ class ModelSource:
                     lines.append(f"{name}[{i}] = T(0.0);")
         return lines
 
-    def _dev_split_column_lines(self) -> List[str]:
-        """Body of ``rhs_split_column``: for the forward-difference column
-        ``i``, only the rows where column i of the Jacobian is structurally
-        non-zero (the rows the column reads), each computed by the statements
-        of ``rhs_split`` it depends on -- the same expressions, a subset."""
+    def _dev_fd_jacobian_lines(self) -> List[str]:
+        """Body of ``fd_jacobian``: the forward-difference Jacobian of the split
+        right-hand side into the packed Newton matrix.  The unperturbed
+        statements are evaluated once; column i then recomputes, for
+        y + delta_i e_i, only the statements of its structural rows that depend
+        on state i (the others keep their unperturbed values, which is what
+        re-evaluating them would give), and stores (f2 - f1) / delta_i at those
+        rows.  delta_i = sqrt(1e-15 max(1e-5, |y_i|)) as in ODE::compute_jacobian."""
+        import sympy
+
         folded = self._fold(self.rhs)
         inter = {n: self.model.sym(n) for n in self.model.intermediates}
         rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
                             [self.model.sym(p) for p in self.fparams], inter, reverse=False)
         prT, prD = self._dev_printers(split=True)
-        binds = {b.name: b for b in rp.forward}
+        binds = list(rp.forward)
+        bmap = {b.name: b for b in binds}
         outs = {o.index: o for o in rp.outputs if o.array == "values"}
         n = len(self.states)
-        lines = ["switch (i) {"]
+        syms = {}
+        for e in [b.expr for b in binds] + [o.expr for o in outs.values()]:
+            for sym in e.free_symbols:
+                syms.setdefault(sym.name, sym)
+        sidx = {self.model.sym(st).name: i for i, st in enumerate(self.states)}
+        deps = {}  # binding -> states it depends on, transitively
+        for b in binds:
+            d = set()
+            for sym in b.expr.free_symbols:
+                if sym.name in sidx:
+                    d.add(sidx[sym.name])
+                elif sym.name in deps:
+                    d |= deps[sym.name]
+            deps[b.name] = d
+        lines = []
+        for b in binds:
+            if b.cls == TIME_CLS:
+                lines.append(f"const double v_{b.name} = {prD(b.expr)};")
+            else:
+                lines.append(f"const T v_{b.name} = {prT(factor_common(b.expr))};")
         for i in range(n):
             rows = [r for r in range(n) if self.lus.jac[r][i] and r in outs]
+            if not rows:
+                continue
             need, stack = set(), [sym.name for r in rows for sym in outs[r].expr.free_symbols]
             while stack:
                 name = stack.pop()
-                if name in binds and name not in need:
+                if name in bmap and name not in need:
                     need.add(name)
-                    stack += [sym.name for sym in binds[name].expr.free_symbols]
-            lines.append(f"case {i}: {{")
-            for b in rp.forward:
-                if b.name not in need:
-                    continue
-                if b.cls == TIME_CLS:
-                    lines.append(f"  const double v_{b.name} = {prD(b.expr)};")
-                else:
-                    lines.append(f"  const T v_{b.name} = {prT(factor_common(b.expr))};")
+                    stack += [sym.name for sym in bmap[name].expr.free_symbols]
+            state_sym = syms.get(self.model.sym(self.states[i]).name, self.model.sym(self.states[i]))
+            sub = {state_sym: sympy.Symbol(f"__yp{i}")}
+            lines.append("{")
+            lines.append(f"  const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[{i}])) ? 1e-5 : fabs(double(y[{i}]))));")
+            lines.append(f"  const T v___yp{i} = T(double(y[{i}]) + d);")
+            for b in binds:
+                if b.name in need and i in deps[b.name]:
+                    new = sympy.Symbol(f"{b.name}__k{i}")
+                    lines.append(f"  const T v_{new.name} = {prT(factor_common(b.expr.xreplace(sub)))};")
+                    sub[syms.get(b.name, sympy.Symbol(b.name))] = new
             for r in rows:
-                lines.append(f"  values[{r}] = {prT(factor_common(outs[r].expr))};")
-            lines.append("  break;")
+                f2 = prT(factor_common(outs[r].expr.xreplace(sub)))
+                lines.append(f"  J[{self.lus.pos[(r, i)]}] = (({f2}) - f1[{r}]) / d;")
             lines.append("}")
-        lines.append("default: break;")
-        lines.append("}")
         return lines
 
     def _derived_host_lines(self) -> List[str]:
@@ -662,13 +689,14 @@ class ModelSource:
         L.append("    (void)time; (void)P; (void)PD; (void)F;")
         L.append("  }")
         L.append("")
-        L.append("  // the rows of rhs_split that column i of a forward-difference Jacobian reads (those")
-        L.append("  // where column i is structurally non-zero), by the statements they depend on")
-        L.append("  template <typename T>")
-        L.append(f"  __device__ static __forceinline__ void rhs_split_column(const int i, {sig}, T* __restrict__ values)")
+        L.append("  // forward-difference Jacobian of rhs_split at y into the packed Newton matrix (structural")
+        L.append("  // entries; fd_clear sets the others): f1 = f(y, time); column i recomputes only the")
+        L.append("  // statements of its rows that depend on state i")
+        L.append("  template <typename T, class A>")
+        L.append(f"  __device__ static __forceinline__ void fd_jacobian({sig}, const T* __restrict__ f1, A J)")
         L.append("  {")
-        L += ["    " + x for x in head + self._dev_split_column_lines()]
-        L.append("    (void)time; (void)P; (void)PD; (void)F; (void)values;")
+        L += ["    " + x for x in head + self._dev_fd_jacobian_lines()]
+        L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
         L.append("  }")
         L.append("")
         L.append("  // vector-Jacobian product of linearized (reverse mode, generated): after the forward")

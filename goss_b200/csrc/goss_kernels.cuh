@@ -503,18 +503,6 @@ __device__ __forceinline__ void rhs64(const double* y, double t, const double* P
         M::template rhs<double>(y, t, P, P, F, out);
 }
 
-// f(y, t) at the rows column i of a forward-difference Jacobian reads (the
-// other entries of out are left as they are)
-template <class M>
-__device__ __forceinline__ void rhs64_column(int i, const double* y, double t, const double* P, const double* F,
-                                             double* out)
-{
-    if constexpr (GOSS_IMPLICIT_SPLIT)
-        M::template rhs_split_column<double>(i, y, t, P, P, F, out);
-    else
-        M::template rhs<double>(y, t, P, P, F, out);
-}
-
 template <class M, class A>
 __device__ __forceinline__ void jacobian64(const double* y, double t, const double* P, const double* F, A J)
 {
@@ -529,14 +517,15 @@ __device__ __forceinline__ void jacobian64(const double* y, double t, const doub
 // the same arguments), stored at the column's structural rows (the other
 // rows are exactly 0 in the reference too).  The perturbed state is built by
 // selects over compile-time indices, so y stays in registers (the reference
-// perturbs y[i] in place and restores it: the same values).  With Rows, each
-// f(y + delta_i e_i) evaluates only the rows column i stores (its structural
-// non-zeros), by the statements of the split right-hand side they depend on:
-// 33-44 % of the work of n full evaluations on TT04.  Measured on B200 (TT04,
-// 262,144 nodes): ThetaSolver 4.43 -> 3.59 ms per 0.1 ms interval; ESDIRK23a,
-// which computes its Jacobian at three inlined call sites, is faster with the
-// full evaluations (255 against 836 ms: the column switch triples its code).
-template <class M, bool Rows = true, class A>
+// perturbs y[i] in place and restores it: the same values).  With the split
+// right-hand side, the generated fd_jacobian evaluates it once at y and, for
+// each column i, recomputes only the statements of the column's structural
+// rows that depend on state i (the others keep the values a full
+// re-evaluation would give).  Measured on B200 (TT04, 262,144 nodes, 0.1 ms
+// intervals): ThetaSolver 4.43 ms per interval with n full evaluations, 3.61
+// with the rows of each column's structure, 1.62 with the cones; ESDIRK23a
+// 258 -> 219 ms.
+template <class M, class A>
 __device__ __forceinline__ void compute_jacobian(const double* y, double t, const double* P, const double* F, A J,
                                                  const double* f1)
 {
@@ -544,6 +533,9 @@ __device__ __forceinline__ void compute_jacobian(const double* y, double t, cons
     if constexpr (M::has_jacobian) {
         (void)f1;
         jacobian64<M>(y, t, P, F, J);
+    } else if constexpr (GOSS_IMPLICIT_SPLIT) {
+        M::fd_clear(J);
+        M::template fd_jacobian<double>(y, t, P, P, F, f1, J);
     } else {
         M::fd_clear(J);
 #pragma unroll 1
@@ -558,10 +550,7 @@ __device__ __forceinline__ void compute_jacobian(const double* y, double t, cons
 #pragma unroll
             for (int k = 0; k < n; ++k)
                 yp[k] = (k == i) ? ysafe + delta : y[k];
-            if constexpr (Rows)
-                rhs64_column<M>(i, yp, t, P, F, f2);
-            else
-                rhs64<M>(yp, t, P, F, f2);
+            rhs64<M>(yp, t, P, F, f2);
             M::fd_column(i, f1, f2, delta, J);
         }
     }
@@ -674,7 +663,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
             newton_done = true;
         } else {
             if (recompute || always) {
-                compute_jacobian<M, true>(yz, tn, a.P, F, J, f1);
+                compute_jacobian<M>(yz, tn, a.P, F, J, f1);
                 M::lu_shift(J, -ldt * alpha);
                 M::lu_factorize(J);
                 jac_comp += 1;
@@ -842,7 +831,7 @@ struct EsdirkNode {
     __device__ void ode_jacobian(double* y, double t)
     {
         rhs64<M>(y, t, P, F, g1);
-        compute_jacobian<M, false>(y, t, P, F, jac, g1);
+        compute_jacobian<M>(y, t, P, F, jac, g1);
         jac_comp += 1;
         new_jacobian = 1;
     }

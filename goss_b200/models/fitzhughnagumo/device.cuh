@@ -156,31 +156,31 @@ struct M_fitzhughnagumo {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
-  // the rows of rhs_split that column i of a forward-difference Jacobian reads (those
-  // where column i is structurally non-zero), by the statements they depend on
-  template <typename T>
-  __device__ static __forceinline__ void rhs_split_column(const int i, const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  // forward-difference Jacobian of rhs_split at y into the packed Newton matrix (structural
+  // entries; fd_clear sets the others): f1 = f(y, time); column i recomputes only the
+  // statements of its rows that depend on state i
+  template <typename T, class A>
+  __device__ static __forceinline__ void fd_jacobian(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const T* __restrict__ f1, A J)
   {
     const T s_V = y[0];
     const T s_s = y[1];
-    switch (i) {
-    case 0: {
-      const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
-      const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-      values[0] = (v_I + T(v_i_Stim));
-      values[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
-      break;
+    const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
+    const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[0])) ? 1e-5 : fabs(double(y[0]))));
+      const T v___yp0 = T(double(y[0]) + d);
+      const T v_I__k0 = ((v___yp0 + P[11])*((P[12]*s_s) + (P[14]*(v___yp0 + P[13])*(P[0] - ((v___yp0))))));
+      J[0] = (((v_I__k0 + T(v_i_Stim))) - f1[0]) / d;
+      J[2] = (((P[3]*(v___yp0 + P[11] + (P[17]*s_s)))) - f1[1]) / d;
     }
-    case 1: {
-      const T v_I = ((s_V + P[11])*((P[12]*s_s) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
-      const double v_i_Stim = (PD[7]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
-      values[0] = (v_I + T(v_i_Stim));
-      values[1] = (P[3]*(s_V + P[11] + (P[17]*s_s)));
-      break;
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[1])) ? 1e-5 : fabs(double(y[1]))));
+      const T v___yp1 = T(double(y[1]) + d);
+      const T v_I__k1 = ((s_V + P[11])*((v___yp1*P[12]) + (P[14]*(s_V + P[13])*(P[0] - ((s_V))))));
+      J[1] = (((v_I__k1 + T(v_i_Stim))) - f1[0]) / d;
+      J[3] = (((P[3]*(s_V + P[11] + (v___yp1*P[17])))) - f1[1]) / d;
     }
-    default: break;
-    }
-    (void)time; (void)P; (void)PD; (void)F; (void)values;
+    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
   }
 
   // vector-Jacobian product of linearized (reverse mode, generated): after the forward

@@ -138,25 +138,25 @@ struct M_oscilator {
     (void)time; (void)P; (void)PD; (void)F;
   }
 
-  // the rows of rhs_split that column i of a forward-difference Jacobian reads (those
-  // where column i is structurally non-zero), by the statements they depend on
-  template <typename T>
-  __device__ static __forceinline__ void rhs_split_column(const int i, const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, T* __restrict__ values)
+  // forward-difference Jacobian of rhs_split at y into the packed Newton matrix (structural
+  // entries; fd_clear sets the others): f1 = f(y, time); column i recomputes only the
+  // statements of its rows that depend on state i
+  template <typename T, class A>
+  __device__ static __forceinline__ void fd_jacobian(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const T* __restrict__ f1, A J)
   {
     const T s_x = y[0];
     const T s_y = y[1];
-    switch (i) {
-    case 0: {
-      values[1] = (P[1]*s_x);
-      break;
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[0])) ? 1e-5 : fabs(double(y[0]))));
+      const T v___yp0 = T(double(y[0]) + d);
+      J[2] = (((v___yp0*P[1])) - f1[1]) / d;
     }
-    case 1: {
-      values[0] = (P[2]*s_y);
-      break;
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[1])) ? 1e-5 : fabs(double(y[1]))));
+      const T v___yp1 = T(double(y[1]) + d);
+      J[1] = (((v___yp1*P[2])) - f1[0]) / d;
     }
-    default: break;
-    }
-    (void)time; (void)P; (void)PD; (void)F; (void)values;
+    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
   }
 
   // vector-Jacobian product of linearized (reverse mode, generated): after the forward
