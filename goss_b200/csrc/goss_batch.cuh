@@ -56,10 +56,14 @@ struct BatchArgs : BatchParamsT<T> {
     }
 };
 
-// Resident 128-thread blocks per SM the batch kernel is compiled for: a launch
-// streams every population's states through HBM for a step or a few, so
-// warps in flight matter -- FP32 fits 4 blocks (128 registers), FP64 stays at
-// the compiler's choice (its models spill heavily below ~240 registers).
+// Resident 128-thread blocks per SM the batch kernel is compiled for.  FP32
+// fits 4 blocks (128 registers): with a launch per forward it streams every
+// population's states through HBM, and with all forwards in one launch it is
+// bound by instruction issue, and in both cases warps in flight matter --
+// measured on B200 (1.97M-node mix, 1000 fused one-step forwards): 2 blocks
+// 128 ms, 3 blocks 98 ms, 4 blocks 90 ms, 5 blocks 92 ms, 6 blocks 99 ms.  FP64
+// stays at the compiler's choice (its models spill heavily below ~240
+// registers).
 #ifndef GOSS_BATCH_MIN_BLOCKS_F32
 #define GOSS_BATCH_MIN_BLOCKS_F32 4
 #endif
