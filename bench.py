@@ -717,10 +717,18 @@ def roofline(md, value_fp32, ms_per_step, n_nodes):
     sfu_rate = sfu * value_fp32
     fp_rate = fp * value_fp32
     hbm_bytes = n_nodes * (2 * n * 8 + 4 * 8)  # states in+out, field params in, per launch
+    # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel
+    # (explicit_kernel<TP06, float, GRL1>, 1,048,576 nodes x 1000 steps) in an
+    # ncu --set full capture of `bench.py --profile single --steps 1 --warmup 1`
+    # on a B200: 196 MB read, 103 MB written (below the algorithmic bytes:
+    # part of the states stay in L2 from the previous launch)
+    ncu_dram_bytes = (196e6 + 103e6) * n_nodes / 1_048_576
     return dict(
         bound="sfu",
         achieved=sfu_rate / 1e9, peak=sfu_peak / 1e9, unit="Gop/s (MUFU)", frac=sfu_rate / sfu_peak,
-        traffic=None,
+        traffic=ncu_dram_bytes,
+        traffic_source="ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one capture of "
+                       "bench.py --profile single (scaled by nodes when --nodes differs)",
         per_cell_step={"sfu_ops": sfu, "fp32_ops": fp},
         fp32_pipe={"achieved": fp_rate / 1e12, "peak": fma_peak / 1e12, "unit": "Top/s",
                    "frac": fp_rate / fma_peak},
