@@ -41,7 +41,9 @@
 // (ten Tusscher-Panfilov, 65,536 nodes x 2,000 steps, backward pass):
 //   FP32: blocks of up to 128 threads, 2 per SM (255 registers), lockstep
 //         28.0 ms; 256 x 1: 29.3 ms; register caps of 168 or 128 (3 or 4
-//         blocks of 128) spill more than the extra warps gain: 37.5 ms;
+//         blocks of 128) spill more than the extra warps gain: 37.5 ms; with
+//         the record's tape (65,536 nodes x 40,000 steps, 368 of 400
+//         segments taped) 2, 3, 4 blocks: 445, 650, 716 ms;
 //   FP64: 256 x 1: 207 ms; 128 x 2: 215 ms.
 template <typename T>
 struct AdjointShape {
