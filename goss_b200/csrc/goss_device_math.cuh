@@ -4,7 +4,7 @@
 // call CUDA's correctly behaved double-precision functions (the FP64 path is
 // checked state for state against the FP64 CPU oracle).  The float overloads
 // map to the SFU approximations (ex2/lg2/rcp/rsqrt based intrinsics) that make
-// the FP32 path fast; its accuracy is judged against FP64 in the tests.
+// the FP32 path fast; its accuracy is checked against FP64 in the tests.
 #ifndef GOSS_DEVICE_MATH_CUH
 #define GOSS_DEVICE_MATH_CUH
 

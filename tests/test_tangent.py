@@ -1,7 +1,7 @@
 """The FP64 tangent-linear checker (oracle/tangent) against the oracle.
 
 The tangent-linear GRL1 trace is the reference against which the adjoint
-kernels' gradients are judged, so it is pinned here first: its primal trace
+kernels' gradients are checked, so it is pinned here first: its primal trace
 equals the oracle's GRL1 trace (the reference's GRL1::forward), and its
 Jacobian equals central finite differences of the oracle on a smooth model
 to 1e-6.  On ten Tusscher-Panfilov, whose sodium-gate rates switch branches
