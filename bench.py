@@ -696,7 +696,22 @@ def implicit_reference_sample(target_s=6.0):
     return out
 
 
-def roofline(md, value_fp32, ms_per_step, n_nodes):
+def measured_peaks(dev):
+    """XU-pipe and FP32-FMA peaks of this GPU (goss_measure_peaks), or None."""
+    import ctypes as C
+
+    from goss_b200 import _capi
+
+    xu, fp = C.c_double(0.0), C.c_double(0.0)
+    try:
+        if _capi.lib().goss_measure_peaks(int(dev), C.byref(xu), C.byref(fp)) != 0:
+            return None
+    except Exception:
+        return None
+    return {"xu_ops_per_s": xu.value, "fp32_ops_per_s": fp.value}
+
+
+def roofline(md, value_fp32, ms_per_step, n_nodes, peaks=None):
     """Operation census of one GRL1 step (generator) against the CUDA-core peaks.
 
     The census is the generator's count of the linearised evaluation as the
@@ -712,8 +727,11 @@ def roofline(md, value_fp32, ms_per_step, n_nodes):
     sfu = lin["exp"] + lin["log"] + lin["sqrt"] + 2 * lin["pow"] + lin["div"]
     fp = lin["add"] + lin["mul"] + lin["div"] + lin["exp"] + 10 * n
     sm_clock = 1.965e9
-    sfu_peak = 148 * 16 * sm_clock          # 16 MUFU results / clk / SM
-    fma_peak = 148 * 128 * sm_clock         # 128 FP32 lanes / clk / SM (ops, FMA = 1 op)
+    nominal_sfu = 148 * 16 * sm_clock       # 16 MUFU results / clk / SM
+    nominal_fma = 148 * 128 * sm_clock      # 128 FP32 lanes / clk / SM (ops, FMA = 1 op)
+    measured = bool(peaks and peaks["xu_ops_per_s"] > 0 and peaks["fp32_ops_per_s"] > 0)
+    sfu_peak = peaks["xu_ops_per_s"] if measured else nominal_sfu
+    fma_peak = peaks["fp32_ops_per_s"] if measured else nominal_fma
     sfu_rate = sfu * value_fp32
     fp_rate = fp * value_fp32
     hbm_bytes = n_nodes * (2 * n * 8 + 4 * 8)  # states in+out, field params in, per launch
@@ -733,8 +751,11 @@ def roofline(md, value_fp32, ms_per_step, n_nodes):
         fp32_pipe={"achieved": fp_rate / 1e12, "peak": fma_peak / 1e12, "unit": "Top/s",
                    "frac": fp_rate / fma_peak},
         hbm={"achieved_gbs": hbm_bytes / (ms_per_step / 1e3) / 1e9, "algorithmic_bytes_per_launch": hbm_bytes},
-        peak_source="nominal B200: 148 SMs x (16 MUFU | 128 FP32) per clk x 1.965 GHz (no CUDA-core peak "
-                    "in MEASURED_PEAKS.json)",
+        peak_source=("measured on this GPU after the timed region by goss_measure_peaks (independent ex2/lg2 "
+                     "chains for the XU pipe, FP32 FMA chains, 2048 threads per SM)") if measured else
+                    ("nominal B200: 148 SMs x (16 MUFU | 128 FP32) per clk x 1.965 GHz (no CUDA-core peak "
+                     "in MEASURED_PEAKS.json)"),
+        nominal_peaks={"xu_gops": nominal_sfu / 1e9, "fp32_tops": nominal_fma / 1e12},
     )
 
 
@@ -848,7 +869,8 @@ def main():
             except Exception as exc:
                 cpu["implicit"] = {"failed": str(exc)}
     if rank == 0:
-        rl = roofline(md, res["value"] / world, res["ms_per_step"], args.nodes)
+        rl = roofline(md, res["value"] / world, res["ms_per_step"], args.nodes,
+                      measured_peaks(int(os.environ.get("LOCAL_RANK", 0))))
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 states)",

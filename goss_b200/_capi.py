@@ -139,6 +139,7 @@ _desc = C.POINTER(ModelDesc)
 
 _PROTOS = {
     "goss_abi_version": (C.c_uint32, []),
+    "goss_measure_peaks": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "goss_last_error": (C.c_char_p, []),
     "goss_system_last_error": (C.c_char_p, [_sys]),
     "goss_solver_default_params": (C.c_int, [C.c_int32, C.POINTER(SolverParams)]),

@@ -267,6 +267,117 @@ int launch_forward(goss_system* s, double t, double interval)
 extern "C" {
 
 GOSS_API uint32_t goss_abi_version(void) { return GOSS_B200_ABI_VERSION; }
+
+// ---------------------------------------------------------------------------
+// CUDA-core peaks for the rooflines of the model kernels: independent chains
+// of ex2/lg2 (XU pipe, the exponentials and reciprocals of the models) and of
+// FP32 fused multiply-adds, enough warps to fill every SM
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kXuChains = 8, kFmaChains = 16;
+
+__global__ void peak_xu_kernel(float* sink, int iters)
+{
+    float x[kXuChains];
+#pragma unroll
+    for (int c = 0; c < kXuChains; ++c)
+        x[c] = 0.5f + 0.01f * (threadIdx.x & 7) + 0.05f * c;
+    for (int k = 0; k < iters; ++k) {
+#pragma unroll
+        for (int c = 0; c < kXuChains; ++c) {
+            float y;
+            asm volatile("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x[c]));
+            asm volatile("lg2.approx.ftz.f32 %0, %1;" : "=f"(x[c]) : "f"(y));
+        }
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int c = 0; c < kXuChains; ++c)
+        s += x[c];
+    if (s == 12345.0f)  // never true; keeps the chains live
+        sink[blockIdx.x] = s;
+}
+
+__global__ void peak_fma_kernel(float* sink, int iters)
+{
+    float x[kFmaChains];
+#pragma unroll
+    for (int c = 0; c < kFmaChains; ++c)
+        x[c] = 0.5f + 0.01f * (threadIdx.x & 7) + 0.05f * c;
+    const float a = 0.999f, b = 0.001f;
+    for (int k = 0; k < iters; ++k) {
+#pragma unroll
+        for (int c = 0; c < kFmaChains; ++c)
+            asm volatile("fma.rn.f32 %0, %0, %1, %2;" : "+f"(x[c]) : "f"(a), "f"(b));
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int c = 0; c < kFmaChains; ++c)
+        s += x[c];
+    if (s == 12345.0f)
+        sink[blockIdx.x] = s;
+}
+}  // namespace
+
+GOSS_API int goss_measure_peaks(int32_t device, double* xu_ops_per_s, double* fp32_ops_per_s)
+{
+    if (!xu_ops_per_s || !fp32_ops_per_s)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL output");
+    cudaError_t e = cudaSetDevice(device);
+    int sms = 0;
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "measure peaks: %s", cudaGetErrorString(e));
+    const int block = 256, grid = sms * 8;  // 2048 threads per SM
+    const int xu_iters = 2048, fma_iters = 8192;
+    float* sink = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double best_xu = 0.0, best_fma = 0.0;
+    e = cudaMalloc(&sink, sizeof(float) * grid);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e0);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e1);
+    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {  // the first of each is a warm-up
+        float ms = 0.0f;
+        cudaEventRecord(e0, st);
+        peak_xu_kernel<<<grid, block, 0, st>>>(sink, xu_iters);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && rep && ms > 0)
+            best_xu = std::max(best_xu, (double)grid * block * xu_iters * 2 * kXuChains / (ms * 1e-3));
+        if (e != cudaSuccess)
+            break;
+        cudaEventRecord(e0, st);
+        peak_fma_kernel<<<grid, block, 0, st>>>(sink, fma_iters);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && rep && ms > 0)
+            best_fma = std::max(best_fma, (double)grid * block * fma_iters * kFmaChains / (ms * 1e-3));
+    }
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
+    if (e0)
+        cudaEventDestroy(e0);
+    if (e1)
+        cudaEventDestroy(e1);
+    if (st)
+        cudaStreamDestroy(st);
+    cudaFree(sink);
+    if (e != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "measure peaks: %s", cudaGetErrorString(e));
+    *xu_ops_per_s = best_xu;
+    *fp32_ops_per_s = best_fma;
+    return 0;
+}
 GOSS_API const char* goss_last_error(void) { return g_last_error.c_str(); }
 GOSS_API const char* goss_system_last_error(const goss_system* s) { return s ? s->last_error.c_str() : ""; }
 

@@ -410,6 +410,13 @@ GOSS_API const char* goss_system_last_error(const goss_system* sys);
 GOSS_API const char* goss_last_error(void);
 GOSS_API uint32_t goss_abi_version(void);
 
+/* No counterpart in the reference: the CUDA-core peaks the model kernels'
+ * rooflines are measured against, on `device`: XU-pipe results per second
+ * (independent ex2/lg2 chains, the pipe of the models' exponentials and
+ * reciprocals) and FP32 fused multiply-adds per second (one op each), each the
+ * best of three timed launches filling every SM.  Takes a few milliseconds. */
+GOSS_API int goss_measure_peaks(int32_t device, double* xu_ops_per_s, double* fp32_ops_per_s);
+
 #ifdef __cplusplus
 }
 #endif
