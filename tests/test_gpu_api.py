@@ -252,3 +252,18 @@ def test_fp32_precision_runs():
     assert np.isfinite(system.states).all()
     with pytest.raises(GossError):
         goss.ODESystemSolver(4, goss.solvers.ThetaSolver(ode), ode, precision="single")
+
+
+def test_measure_peaks_through_the_c_abi():
+    """goss_measure_peaks (the roofline denominators of the model kernels):
+    XU-pipe results and FP32 fused multiply-adds per second on cuda:0, in the
+    range a B200-class GPU can give (nominal 4.65e12 and 3.72e13)."""
+    import ctypes as C
+
+    from goss_b200 import _capi
+
+    xu, fp = C.c_double(0.0), C.c_double(0.0)
+    assert _capi.lib().goss_measure_peaks(0, C.byref(xu), C.byref(fp)) == 0
+    assert 1e12 < xu.value < 1e13, xu.value
+    assert 1e13 < fp.value < 1e14, fp.value
+    assert _capi.lib().goss_measure_peaks(0, None, C.byref(fp)) != 0  # NULL output rejected
