@@ -655,7 +655,16 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
         bool newton_done = false;
         for (int i = 0; i < n; ++i)
             yz[i] = y[i] + z1[i];
-        rhs64<M>(yz, tn, a.P, F, f1);
+        // forward differences: when this iteration will refactorise (both
+        // conditions are known before f(yz) is evaluated), f(yz) and the
+        // Jacobian come from one evaluation of the unperturbed statements
+        constexpr bool fused = !M::has_jacobian && GOSS_IMPLICIT_SPLIT;
+        if (fused && !(relative_residual < sp.relative_tolerance) && (recompute || always)) {
+            M::fd_clear(J);
+            M::template rhs_fd_jacobian<double>(yz, tn, a.P, a.P, F, f1, J);
+        } else {
+            rhs64<M>(yz, tn, a.P, F, f1);
+        }
         for (int i = 0; i < n; ++i)
             b[i] = -z1[i] * 1.0 + ldt * (prev[i] + alpha * f1[i]);
         residual = l2norm<n>(b);
@@ -663,7 +672,8 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
             newton_done = true;
         } else {
             if (recompute || always) {
-                compute_jacobian<M>(yz, tn, a.P, F, J, f1);
+                if constexpr (!fused)
+                    compute_jacobian<M>(yz, tn, a.P, F, J, f1);
                 M::lu_shift(J, -ldt * alpha);
                 M::lu_factorize(J);
                 jac_comp += 1;
