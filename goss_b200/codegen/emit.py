@@ -522,6 +522,34 @@ class ModelSource:
                     lines.append(f"{name}[{i}] = T(0.0);")
         return lines
 
+    def _dev_rhs_jacobian_lines(self) -> List[str]:
+        """Body of ``rhs_jacobian``: f(y) (``rhs_split``'s outputs) and the
+        analytic Jacobian into the packed Newton matrix from one split program,
+        so their exponentials, reciprocals and intermediates are computed once."""
+        rhs, jac = self.rhs, self._packed_jacobian()
+        names = {b.name for b in rhs.body if isinstance(b, Assign)}
+        body = [b for b in rhs.body if isinstance(b, Assign)]
+        body += [b for b in jac.body if isinstance(b, Assign) and b.name not in names]
+        body += [b for b in rhs.body if isinstance(b, Output)] + [b for b in jac.body if isinstance(b, Output)]
+        folded = self._fold(Program("rhs_jacobian", body, None))
+        inter = {n: self.model.sym(n) for n in self.model.intermediates}
+        rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
+                            [self.model.sym(p) for p in self.fparams], inter, reverse=False)
+        prT, prD = self._dev_printers(split=True)
+        lines = []
+        for b in rp.forward:
+            if b.cls == TIME_CLS:
+                lines.append(f"const double v_{b.name} = {prD(b.expr)};")
+            else:
+                lines.append(f"const T v_{b.name} = {prT(factor_common(b.expr))};")
+        arrays, sizes = {"values": "f1", "jac": "J"}, {"values": len(self.states), "jac": self.lus.nnz}
+        for o in rp.outputs:
+            lines.append(f"{arrays[o.array]}[{o.index}] = {prT(factor_common(o.expr))};")
+        for arr, name in arrays.items():
+            done = {o.index for o in rp.outputs if o.array == arr}
+            lines += [f"{name}[{i}] = T(0.0);" for i in range(sizes[arr]) if i not in done]
+        return lines
+
     def _dev_fd_jacobian_lines(self, with_rhs: bool = False) -> List[str]:
         """Body of ``fd_jacobian``: the forward-difference Jacobian of the split
         right-hand side into the packed Newton matrix.  The unperturbed
@@ -702,6 +730,16 @@ class ModelSource:
         L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
         L.append("  }")
         L.append("")
+        if self.jac is not None:
+            L.append("  // f1 = f(y, time) (rhs_split) and the analytic Jacobian into the packed Newton matrix,")
+            L.append("  // sharing their exponentials, reciprocals and intermediates")
+            L.append("  template <typename T, class A>")
+            L.append(f"  __device__ static __forceinline__ void rhs_jacobian({sig}, T* __restrict__ f1, A J)")
+            L.append("  {")
+            L += ["    " + x for x in head + self._dev_rhs_jacobian_lines()]
+            L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
+            L.append("  }")
+            L.append("")
         L.append("  // the same, also writing f1 = f(y, time) (rhs_split) from its unperturbed statements")
         L.append("  template <typename T, class A>")
         L.append(f"  __device__ static __forceinline__ void rhs_fd_jacobian({sig}, T* __restrict__ f1, A J)")

@@ -655,13 +655,18 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
         bool newton_done = false;
         for (int i = 0; i < n; ++i)
             yz[i] = y[i] + z1[i];
-        // forward differences: when this iteration will refactorise (both
-        // conditions are known before f(yz) is evaluated), f(yz) and the
-        // Jacobian come from one evaluation of the unperturbed statements
-        constexpr bool fused = !M::has_jacobian && GOSS_IMPLICIT_SPLIT;
+        // when this iteration will refactorise (both conditions are known
+        // before f(yz) is evaluated), f(yz) and the Jacobian come from one
+        // evaluation: the unperturbed statements of the forward differences,
+        // or the statements the analytic Jacobian shares with f
+        constexpr bool fused = GOSS_IMPLICIT_SPLIT;
         if (fused && !(relative_residual < sp.relative_tolerance) && (recompute || always)) {
-            M::fd_clear(J);
-            M::template rhs_fd_jacobian<double>(yz, tn, a.P, a.P, F, f1, J);
+            if constexpr (M::has_jacobian) {
+                M::template rhs_jacobian<double>(yz, tn, a.P, a.P, F, f1, J);
+            } else {
+                M::fd_clear(J);
+                M::template rhs_fd_jacobian<double>(yz, tn, a.P, a.P, F, f1, J);
+            }
         } else {
             rhs64<M>(yz, tn, a.P, F, f1);
         }
@@ -840,7 +845,10 @@ struct EsdirkNode {
     // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
     __device__ void ode_jacobian(double* y, double t)
     {
-        if constexpr (!M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
+        if constexpr (M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
+            // f(y) and the analytic Jacobian sharing their statements
+            M::template rhs_jacobian<double>(y, t, P, P, F, g1, jac);
+        } else if constexpr (GOSS_IMPLICIT_SPLIT) {
             // f(y) and the forward differences from one evaluation of the
             // unperturbed statements (TT04, 262,144 nodes: 214 -> 199 ms per
             // interval against a separate f(y))
