@@ -522,7 +522,42 @@ class ModelSource:
                     lines.append(f"{name}[{i}] = T(0.0);")
         return lines
 
-    def _dev_rhs_jacobian_lines(self) -> List[str]:
+    def _t0_lines(self, binds, outs, prT, prD) -> List[str]:
+        """f0 = f(y, t0) next to f1 = f(y, time) written just before: only the
+        statements that depend on the time (the stimulus and what it feeds) are
+        evaluated again at t0; every other row of f0 is the row of f1."""
+        import sympy
+
+        n = len(self.states)
+        syms = {}
+        for e in [b.expr for b in binds] + [o.expr for o in outs.values()]:
+            for sym in e.free_symbols:
+                syms.setdefault(sym.name, sym)
+        t0 = sympy.Symbol("__tzero")
+        sub, cone = {TIME: t0}, set()
+        lines = ["const double v___tzero = t0;"]
+        for b in binds:
+            names = {x.name for x in b.expr.free_symbols}
+            if b.cls == TIME_CLS or TIME in b.expr.free_symbols or names & cone:
+                cone.add(b.name)
+                new = sympy.Symbol(f"{b.name}__tz")
+                e = b.expr.xreplace(sub)
+                if b.cls == TIME_CLS:
+                    lines.append(f"const double v_{new.name} = {prD(e)};")
+                else:
+                    lines.append(f"const T v_{new.name} = {prT(factor_common(e))};")
+                sub[syms.get(b.name, sympy.Symbol(b.name))] = new
+        for r in range(n):
+            o = outs.get(r)
+            if o is None:
+                lines.append(f"f0[{r}] = T(0.0);")
+            elif TIME in o.expr.free_symbols or {x.name for x in o.expr.free_symbols} & cone:
+                lines.append(f"f0[{r}] = {prT(factor_common(o.expr.xreplace(sub)))};")
+            else:
+                lines.append(f"f0[{r}] = f1[{r}];")
+        return lines
+
+    def _dev_rhs_jacobian_lines(self, with_t0: bool = False) -> List[str]:
         """Body of ``rhs_jacobian``: f(y) (``rhs_split``'s outputs) and the
         analytic Jacobian into the packed Newton matrix from one split program,
         so their exponentials, reciprocals and intermediates are computed once."""
@@ -548,9 +583,12 @@ class ModelSource:
         for arr, name in arrays.items():
             done = {o.index for o in rp.outputs if o.array == arr}
             lines += [f"{name}[{i}] = T(0.0);" for i in range(sizes[arr]) if i not in done]
+        if with_t0:
+            lines += self._t0_lines(list(rp.forward), {o.index: o for o in rp.outputs if o.array == "values"},
+                                    prT, prD)
         return lines
 
-    def _dev_fd_jacobian_lines(self, with_rhs: bool = False) -> List[str]:
+    def _dev_fd_jacobian_lines(self, with_rhs: bool = False, with_t0: bool = False) -> List[str]:
         """Body of ``fd_jacobian``: the forward-difference Jacobian of the split
         right-hand side into the packed Newton matrix.  The unperturbed
         statements are evaluated once; column i then recomputes, for
@@ -592,6 +630,8 @@ class ModelSource:
         if with_rhs:  # f1 = f(y): the outputs of rhs_split, from the same statements
             for r in range(n):
                 lines.append(f"f1[{r}] = {prT(factor_common(outs[r].expr)) if r in outs else 'T(0.0)'};")
+            if with_t0:
+                lines += self._t0_lines(binds, outs, prT, prD)
         for i in range(n):
             rows = [r for r in range(n) if self.lus.jac[r][i] and r in outs]
             if not rows:
@@ -740,12 +780,30 @@ class ModelSource:
             L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
             L.append("  }")
             L.append("")
+            L.append("  // the same, also writing f0 = f(y, t0) (only the time-dependent statements again)")
+            L.append("  template <typename T, class A>")
+            L.append(f"  __device__ static __forceinline__ void rhs2_jacobian({sig}, const double t0,")
+            L.append("      T* __restrict__ f0, T* __restrict__ f1, A J)")
+            L.append("  {")
+            L += ["    " + x for x in head + self._dev_rhs_jacobian_lines(with_t0=True)]
+            L.append("    (void)time; (void)t0; (void)P; (void)PD; (void)F; (void)f0; (void)f1; (void)J;")
+            L.append("  }")
+            L.append("")
         L.append("  // the same, also writing f1 = f(y, time) (rhs_split) from its unperturbed statements")
         L.append("  template <typename T, class A>")
         L.append(f"  __device__ static __forceinline__ void rhs_fd_jacobian({sig}, T* __restrict__ f1, A J)")
         L.append("  {")
         L += ["    " + x for x in head + self._dev_fd_jacobian_lines(with_rhs=True)]
         L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
+        L.append("  }")
+        L.append("")
+        L.append("  // the same, also writing f0 = f(y, t0) (only the time-dependent statements again)")
+        L.append("  template <typename T, class A>")
+        L.append(f"  __device__ static __forceinline__ void rhs2_fd_jacobian({sig}, const double t0,")
+        L.append("      T* __restrict__ f0, T* __restrict__ f1, A J)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_fd_jacobian_lines(with_rhs=True, with_t0=True)]
+        L.append("    (void)time; (void)t0; (void)P; (void)PD; (void)F; (void)f0; (void)f1; (void)J;")
         L.append("  }")
         L.append("")
         L.append("  // vector-Jacobian product of linearized (reverse mode, generated): after the forward")

@@ -28,7 +28,7 @@ from .emit import ModelSource, c_ident, model_class_name
 from .ir import ModelIR
 from .odeparse import ODEModel
 
-GENERATOR_VERSION = "7"
+GENERATOR_VERSION = "8"
 
 _CENSUS_KEYS = ("add", "mul", "div", "exp", "log", "sqrt", "pow", "cmp", "misc")
 

@@ -620,7 +620,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
         prev[i] = 0.0;
     uint64_t guard = 0;
     // the step in progress and its Newton iteration state
-    bool done = !active, in_step = false, step_ok = true;
+    bool done = !active, in_step = false, step_ok = true, prev_pending = false;
     double tn = 0.0, alpha = 1.0;
     int newton_iterations = 0;
     double relative_previous_residual = 1.0, relative_residual = 1.0, previous_residual = 1.0;
@@ -636,11 +636,6 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
             }
             for (int i = 0; i < n; ++i)
                 z1[i] = 0.0;
-            if (!IE && fabs(sp.theta - 1.0) > kGossEps) {
-                rhs64<M>(y, t, a.P, F, f1);
-                for (int i = 0; i < n; ++i)
-                    prev[i] = (1 - sp.theta) * f1[i];
-            }
             if (IE ? num_refinements > sp.num_refinements_without_always_recomputing_jacobian
                    : num_refinements <= sp.num_refinements_without_always_recomputing_jacobian)
                 always = 1;
@@ -649,6 +644,18 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
             step_ok = true;
             newton_iterations = 0;
             relative_previous_residual = relative_residual = previous_residual = initial_residual = 1.0;
+            // (1 - theta) f(y, t): when the step's first Newton iteration will
+            // refactorise, its f(y, tn) evaluation writes f(y, t) as well
+            prev_pending = false;
+            if (!IE && fabs(sp.theta - 1.0) > kGossEps) {
+                if (GOSS_IMPLICIT_SPLIT && !(relative_residual < sp.relative_tolerance) && (recompute || always)) {
+                    prev_pending = true;
+                } else {
+                    rhs64<M>(y, t, a.P, F, f1);
+                    for (int i = 0; i < n; ++i)
+                        prev[i] = (1 - sp.theta) * f1[i];
+                }
+            }
             in_step = true;
         }
         // one iteration of ImplicitODESolver::newton_solve (ImplicitODESolver.cpp:114-245)
@@ -661,7 +668,17 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
         // or the statements the analytic Jacobian shares with f
         constexpr bool fused = GOSS_IMPLICIT_SPLIT;
         if (fused && !(relative_residual < sp.relative_tolerance) && (recompute || always)) {
-            if constexpr (M::has_jacobian) {
+            if (!IE && prev_pending) {  // first iteration of the step: yz = y; f(y, t) into b
+                if constexpr (M::has_jacobian) {
+                    M::template rhs2_jacobian<double>(yz, tn, a.P, a.P, F, t, b, f1, J);
+                } else {
+                    M::fd_clear(J);
+                    M::template rhs2_fd_jacobian<double>(yz, tn, a.P, a.P, F, t, b, f1, J);
+                }
+                for (int i = 0; i < n; ++i)
+                    prev[i] = (1 - sp.theta) * b[i];
+                prev_pending = false;
+            } else if constexpr (M::has_jacobian) {
                 M::template rhs_jacobian<double>(yz, tn, a.P, a.P, F, f1, J);
             } else {
                 M::fd_clear(J);

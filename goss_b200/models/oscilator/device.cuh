@@ -180,6 +180,31 @@ struct M_oscilator {
     (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
   }
 
+  // the same, also writing f0 = f(y, t0) (only the time-dependent statements again)
+  template <typename T, class A>
+  __device__ static __forceinline__ void rhs2_fd_jacobian(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const double t0,
+      T* __restrict__ f0, T* __restrict__ f1, A J)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    f1[0] = (P[2]*s_y);
+    f1[1] = (P[1]*s_x);
+    const double v___tzero = t0;
+    f0[0] = f1[0];
+    f0[1] = f1[1];
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[0])) ? 1e-5 : fabs(double(y[0]))));
+      const T v___yp0 = T(double(y[0]) + d);
+      J[2] = (((v___yp0*P[1])) - f1[1]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[1])) ? 1e-5 : fabs(double(y[1]))));
+      const T v___yp1 = T(double(y[1]) + d);
+      J[1] = (((v___yp1*P[2])) - f1[0]) / d;
+    }
+    (void)time; (void)t0; (void)P; (void)PD; (void)F; (void)f0; (void)f1; (void)J;
+  }
+
   // vector-Jacobian product of linearized (reverse mode, generated): after the forward
   // sweep seed(linear, rhs, abar, bbar) supplies the cotangents of the outputs, then
   // ybar = abar^T d(linear)/dy + bbar^T d(rhs)/dy and Fbar likewise for the field parameters
