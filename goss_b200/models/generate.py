@@ -1,6 +1,6 @@
 """Regenerate the shipped model variants from the reference ``.ode`` files.
 
-Usage (needs the reference sources, default ``/root/reference``)::
+Usage (needs the reference sources; there is no default location)::
 
     GOSS_REFERENCE=/path/to/goss python -m goss_b200.models.generate
 """
@@ -16,9 +16,14 @@ from . import HERE, SHIPPED
 
 
 def main() -> int:
-    ref = Path(os.environ.get("GOSS_REFERENCE", "/root/reference"))
+    env = os.environ.get("GOSS_REFERENCE")
+    if not env:
+        print("GOSS_REFERENCE is not set: point it at a goss checkout (the .ode files are read from it)",
+              file=sys.stderr)
+        return 1
+    ref = Path(env)
     if not ref.is_dir():
-        print(f"reference sources not found at {ref}", file=sys.stderr)
+        print(f"reference sources not found at {ref} (GOSS_REFERENCE)", file=sys.stderr)
         return 1
     for entry in SHIPPED:
         model = load_ode(ref / entry["ode"])

@@ -278,7 +278,24 @@ class TangentTrace:
         return tr, jac
 
 
-REF_SOURCES = Path(os.environ.get("GOSS_REFERENCE", "/root/reference"))
+def reference_dir() -> Optional[Path]:
+    """The reference source tree the oracle recipe reads: ``$GOSS_REFERENCE``
+    when set, else the Makefile's ``REF`` (the recipe is the one place that
+    names it); None when that directory does not exist (GPU machines carry
+    only the prebuilt ``oracle/_ref``)."""
+    env = os.environ.get("GOSS_REFERENCE")
+    if env:
+        ref = Path(env)
+    else:
+        try:
+            out = subprocess.run(["make", "-s", "--no-print-directory", "-C", str(HERE), "print-ref"],
+                                 capture_output=True, text=True, check=True).stdout.strip()
+        except (OSError, subprocess.CalledProcessError):
+            return None
+        if not out:
+            return None
+        ref = Path(out)
+    return ref if (ref / "cpp" / "goss").is_dir() else None
 
 
 def _cc(name: str) -> str:
@@ -292,9 +309,10 @@ def ref_available() -> bool:
 
 def build_ref_core() -> bool:
     """Build oracle/_ref with the Makefile when the reference sources exist."""
-    if not REF_SOURCES.is_dir():
+    ref = reference_dir()
+    if ref is None:
         return ref_available()
-    subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REF_SOURCES}"], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
     return ref_available()
 
 
@@ -305,12 +323,13 @@ def build_ref_plugin(variant_dir: Path, force: bool = False) -> Optional[Path]:
     hdr = variant_dir / "goss_plugin.h"
     if not force and out.exists() and out.stat().st_mtime >= hdr.stat().st_mtime:
         return out
-    if not REF_SOURCES.is_dir() or not ref_available():
+    ref = reference_dir()
+    if ref is None or not ref_available():
         return out if out.exists() else None
     out.parent.mkdir(parents=True, exist_ok=True)
     src = out.parent / "plugin.cpp"
     src.write_text(f'#include "{hdr}"\n')
-    subprocess.run([_cc("g++"), "-O3", "-DNDEBUG", "-std=c++17", "-fPIC", "-shared", f"-I{REF_SOURCES / 'cpp'}",
+    subprocess.run([_cc("g++"), "-O3", "-DNDEBUG", "-std=c++17", "-fPIC", "-shared", f"-I{ref / 'cpp'}",
                     str(src), f"-L{REFDIR}", "-lgoss_ref", f"-Wl,-rpath,{REFDIR}", "-o", str(out)], check=True)
     return out
 
@@ -339,6 +358,7 @@ class RefSystem:
             L.ref_last_error.argtypes = [C.c_void_p]
             L.ref_last_error.restype = C.c_char_p
             L.ref_num_jac_comp.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+            L.ref_num_rejected.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
             L.ref_compute_jacobian.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
             L.ref_lu_factorize.argtypes = [C.c_void_p, _dp]
             L.ref_forward_backward_subst.argtypes = [C.c_void_p, _dp, _dp, _dp]
@@ -396,6 +416,13 @@ class RefSystem:
     def num_jac_comp(self) -> np.ndarray:
         out = np.zeros(self.N, dtype=np.int64)
         self.lib().ref_num_jac_comp(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)))
+        return out
+
+    def num_rejected(self) -> np.ndarray:
+        """Rejected steps per node (ESDIRK23a only)."""
+        out = np.zeros(self.N, dtype=np.int64)
+        if self.lib().ref_num_rejected(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))):
+            raise ValueError("num_rejected: the solver keeps no rejection counter")
         return out
 
     def __del__(self):

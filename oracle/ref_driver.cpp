@@ -296,6 +296,20 @@ __attribute__((visibility("default"))) int ref_num_jac_comp(void* h, int64_t* ou
     return 0;
 }
 
+// AdaptiveImplicitSolver::get_num_rejected (AdaptiveImplicitSolver.h:63-66)
+// of every node's ESDIRK23a solver (the other solvers have no such counter).
+__attribute__((visibility("default"))) int ref_num_rejected(void* h, int64_t* out)
+{
+    auto* r = static_cast<RefSystem*>(h);
+    if (r->kind != 5)
+        return 1;
+    for (uint32_t i = 0; i < r->N; ++i) {
+        auto s = std::dynamic_pointer_cast<goss::AdaptiveImplicitSolver>(r->nodes[i]->solver());
+        out[i] = s ? s->get_num_rejected() : -1;
+    }
+    return 0;
+}
+
 // ODE::compute_jacobian (ODE.h:71) of the plugin model with its default
 // parameters: the generated analytic override when the plugin has one, else
 // the reference's forward differences (ODE.cpp:47-67); jac is row-major n x n.

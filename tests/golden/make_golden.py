@@ -1,9 +1,10 @@
 """Generate the golden vectors that pin the model code generator.
 
 Run from the repository root in a checkout that has the reference sources
-at ``$GOSS_REFERENCE`` (default ``/root/reference``)::
+at ``$GOSS_REFERENCE`` (or where the oracle recipe ``oracle/Makefile`` reads
+them, ``make -s -C oracle print-ref``)::
 
-    python tests/golden/make_golden.py
+    GOSS_REFERENCE=/path/to/goss python tests/golden/make_golden.py
 
 Sources of truth (all from the reference repository, used read-only):
 
@@ -24,7 +25,6 @@ from __future__ import annotations
 
 import ast
 import math
-import os
 import subprocess
 import sys
 import tempfile
@@ -33,7 +33,13 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("GOSS_REFERENCE", "/root/reference"))
+sys.path.insert(0, str(HERE.parents[1] / "oracle"))
+import pyoracle  # noqa: E402
+
+_ref = pyoracle.reference_dir()
+if _ref is None:
+    sys.exit("make_golden.py: the reference sources were not found; set GOSS_REFERENCE to a goss checkout")
+REF = _ref
 
 CPP_FIXTURES = [
     # (model name, header relative to REF, class name, .ode relative to REF)

@@ -14,7 +14,6 @@ through the fixtures in ``tests/golden`` (``make_golden.py``).
 from __future__ import annotations
 
 import json
-import os
 from pathlib import Path
 
 import numpy as np
@@ -26,7 +25,11 @@ from goss_b200.codegen.odeparse import ODEParseError, parse_ode_text
 from goss_b200.codegen.variant import write_variant
 from helpers import GOLDEN, meta, oracle_model, variant_dir
 
-REF = Path(os.environ.get("GOSS_REFERENCE", "/root/reference"))
+import pyoracle
+
+# the reference source tree (GOSS_REFERENCE or the oracle recipe's REF); the
+# tests that regenerate from its .ode files skip where it is absent
+REF = pyoracle.reference_dir() or Path("/nonexistent-reference")
 
 
 def test_state_order_follows_derivatives_and_parameters_sorted():

@@ -93,6 +93,55 @@ def test_tt04_implicit_fp64(solver, steps, dt, ldt):
     assert parity(gpu, cpu, rtol=TOL64) <= 1.0
 
 
+# ESDIRK23a on its accepting path: the stage loop and the state update
+# (ESDIRK23a.cpp:134-198), the step-size growth and Jacobian reuse of
+# ESDIRK23a::forward (:280-316).  TT04 accepts steps only with min_dt below
+# the default 0.001 ms (at the default the first attempt fails at min_dt and
+# no step is ever accepted, in the reference too).
+@pytest.mark.parametrize("model,N,steps,dt,sp", [
+    ("fitzhughnagumo", 33, 40, 1.0, {}),
+    ("oscilator", 33, 40, 0.1, {}),
+    ("beeler_reuter_1977", 33, 40, 1.0, {}),
+    ("tentusscher_2004_mcell", 16, 40, 0.1, {"min_dt": 1e-4}),
+])
+def test_esdirk_accepting_steps_fp64(model, N, steps, dt, sp):
+    rng = np.random.default_rng(21)
+    ode = goss.ParameterizedODE(model)
+    solver = goss.solvers.ESDIRK23a(ode)
+    solver.internal_time_step = -1.0
+    for k, v in sp.items():
+        solver.set_parameter(k, v)
+    system = goss.ODESystemSolver(N, solver, ode)
+    om = oracle_model(model)
+    y0 = perturbed_states(om.ic, N, rng, 0.02)
+    system.set_states(y0)
+    o = pyoracle.OracleSystem(om, "ESDIRK23a", N, ldt=-1.0, **sp)
+    o.states[:] = y0
+    for k in range(steps):
+        system.forward(k * dt, dt)
+        assert o.forward(k * dt, dt) == 0
+    gpu, cpu = system.states, o.states.copy()
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+    jc, rj, ac = system.counters()
+    ojc, orj, oac = o.counters()
+    assert np.array_equal(jc, ojc) and np.array_equal(rj, orj) and np.array_equal(ac, oac)
+    assert ac.min() > 0 and np.abs(gpu - y0).max() > 0
+
+
+def test_esdirk_accepting_steps_analytic_jacobian_fp64():
+    fps = ("g_Kr", "g_CaL")
+    md = meta(variant_dir("tentusscher_2004_mcell", fps, True))
+    rng = np.random.default_rng(23)
+    N = 16
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * (1 + rng.uniform(-0.05, 0.05, (N, 2)))
+    gpu, cpu, system = run_pair("tentusscher_2004_mcell", "ESDIRK23a", N, 40, 0.1, -1.0, fps, fp, jacobian=True,
+                                solver_params={"min_dt": 1e-4})
+    assert parity(gpu, cpu, rtol=TOL64) <= 1.0
+    _, _, ac = system.counters()
+    assert ac.min() > 0
+
+
 def test_tt04_implicit_with_field_parameters():
     fps = ("g_Kr", "g_CaL")
     md = meta(variant_dir("tentusscher_2004_mcell", fps))

@@ -56,6 +56,70 @@ def test_restatement_bit_identical_to_reference(model, solver, N, steps, dt, ldt
         assert np.array_equal(jc, r.num_jac_comp())
 
 
+# ESDIRK23a where it accepts steps (ESDIRK23a.cpp:134-198 state update,
+# :280-316 step-size growth and Jacobian reuse).  TT04 at the default
+# min_dt = 0.001 ms never accepts a step (the first attempt at min_dt fails the
+# error test and the step size cannot shrink below it), so its accepting case
+# lowers min_dt to 1e-4 ms, where the controller starts small and grows.
+ESDIRK_ACCEPTING = [
+    # model, nodes, intervals, interval, solver parameter overrides
+    ("fitzhughnagumo", 8, 40, 1.0, {}),
+    ("oscilator", 8, 40, 0.1, {}),
+    ("beeler_reuter_1977", 8, 40, 1.0, {}),
+    ("tentusscher_2004_mcell", 4, 40, 0.1, {"min_dt": 1e-4}),
+]
+
+
+@pytest.mark.parametrize("model,N,steps,dt,sp", ESDIRK_ACCEPTING)
+def test_esdirk_accepting_steps_bit_identical_to_reference(model, N, steps, dt, sp):
+    rng = np.random.default_rng(21)
+    om = oracle_model(model)
+    y0 = perturbed_states(om.ic, N, rng, spread=0.02)
+    o = pyoracle.OracleSystem(om, "ESDIRK23a", N, ldt=-1.0, **sp)
+    o.states[:] = y0
+    r = ref_system(model, "ESDIRK23a", N, ldt=-1.0, **sp)
+    if r is None:
+        pytest.skip("reference plugin not built")
+    r.set_states(y0)
+    for k in range(steps):
+        assert o.forward(k * dt, dt, threads=4) == 0
+        assert r.forward(k * dt, dt) == 0
+    a, b = o.states.copy(), r.get_states()
+    assert np.array_equal(a, b), float(np.max(np.abs(a - b)))
+    jc, rj, ac = o.counters()
+    assert np.array_equal(jc, r.num_jac_comp())
+    assert np.array_equal(rj, r.num_rejected())
+    # the states moved: accepted steps updated y (ESDIRK23a.cpp:194-195)
+    assert ac.min() > 0 and np.abs(a - y0).max() > 0
+
+
+def test_esdirk_accepting_analytic_jacobian_bit_identical_to_reference():
+    """TT04 with the generated analytic Jacobian and two field parameters,
+    ESDIRK23a accepting steps (min_dt 1e-4 ms)."""
+    name, fps = "tentusscher_2004_mcell", ("g_Kr", "g_CaL")
+    rng = np.random.default_rng(5)
+    om = oracle_model(name, fps, True)
+    N = 4
+    defaults = om.default_params[[meta(variant_dir(name, fps, True))["parameter_names"].index(p) for p in fps]]
+    fp = defaults[None, :] * (1 + rng.uniform(-0.05, 0.05, (N, len(fps))))
+    y0 = perturbed_states(om.ic, N, rng, spread=0.02)
+    o = pyoracle.OracleSystem(om, "ESDIRK23a", N, ldt=-1.0, min_dt=1e-4)
+    o.states[:] = y0
+    o.field_params[:] = fp
+    r = ref_system(name, "ESDIRK23a", N, field_parameters=fps, jacobian=True, ldt=-1.0, min_dt=1e-4)
+    if r is None:
+        pytest.skip("reference plugin not built")
+    r.set_states(y0)
+    r.set_field_parameters(fp)
+    for k in range(40):
+        assert o.forward(k * 0.1, 0.1, threads=4) == 0
+        assert r.forward(k * 0.1, 0.1) == 0
+    assert np.array_equal(o.states, r.get_states())
+    jc, rj, ac = o.counters()
+    assert np.array_equal(jc, r.num_jac_comp()) and np.array_equal(rj, r.num_rejected())
+    assert ac.min() > 0
+
+
 def test_restatement_field_parameters_match_reference():
     name, fps = "tentusscher_panfilov_2006_M_cell", ("g_Kr", "g_Ks", "g_CaL", "g_to")
     rng = np.random.default_rng(3)
