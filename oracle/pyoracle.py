@@ -334,6 +334,61 @@ def build_ref_plugin(variant_dir: Path, force: bool = False) -> Optional[Path]:
     return out
 
 
+def build_ref_plugin_field_states(variant_dir: Path, ode_path: str, field_states) -> Optional[Path]:
+    """A variant's plugin generated again with field states (the reference
+    fixes them in the plugin class: ParameterizedODE.h:147-150), so that the
+    reference's ODESystemSolver::solve returns them.  Generated from the
+    reference's .ode file where the sources exist; elsewhere the prebuilt
+    library is returned, or None."""
+    variant_dir = Path(variant_dir).resolve()
+    tag = "_".join(field_states)
+    out = REFDIR / f"{variant_dir.name}__fs_{tag}" / "libplugin.so"
+    ref = reference_dir()
+    if out.exists() and (ref is None or out.stat().st_mtime >= (variant_dir / "model.json").stat().st_mtime):
+        return out
+    if ref is None or not ref_available():
+        return out if out.exists() else None
+    import json
+    import sys
+
+    sys.path.insert(0, str(HERE.parent))
+    from goss_b200.codegen.emit import ModelSource
+    from goss_b200.codegen.ir import ModelIR
+    from goss_b200.codegen.odeparse import load_ode
+
+    md = json.loads((variant_dir / "model.json").read_text())
+    model = load_ode(ref / ode_path)
+    ir = ModelIR(model, field_parameters=md["field_parameter_names"], field_states=list(field_states),
+                 monitored=md["monitored_names"], linearization=md.get("linearization", "gotran"))
+    out.parent.mkdir(parents=True, exist_ok=True)
+    hdr = out.parent / "goss_plugin.h"
+    hdr.write_text(ModelSource(ir, jacobian=bool(md.get("jacobian"))).emit_goss_plugin())
+    src = out.parent / "plugin.cpp"
+    src.write_text(f'#include "{hdr}"\n')
+    subprocess.run([_cc("g++"), "-O3", "-DNDEBUG", "-std=c++17", "-fPIC", "-shared", f"-I{ref / 'cpp'}",
+                    str(src), f"-L{REFDIR}", "-lgoss_ref", f"-Wl,-rpath,{REFDIR}", "-o", str(out)], check=True)
+    return out
+
+
+# plugins built again with field states for the reference's solve():
+# (model, .ode path in the reference repository, field states)
+FIELD_STATE_PLUGINS = [("tentusscher_panfilov_2006_M_cell", "demo/tentusscher_panfilov_2006_M_cell.ode", ("V", "Ca_i"))]
+
+
+def field_state_plugin(name: str, field_states) -> Optional[Path]:
+    """The prebuilt (or, where the reference sources exist, built now) plugin
+    of a FIELD_STATE_PLUGINS entry."""
+    import sys
+
+    sys.path.insert(0, str(HERE.parent))
+    from goss_b200 import models
+
+    for nm, ode_path, fs in FIELD_STATE_PLUGINS:
+        if nm == name and tuple(fs) == tuple(field_states):
+            return build_ref_plugin_field_states(models.find_variant(nm), ode_path, fs)
+    return None
+
+
 class RefSystem:
     """The reference's ODESystemSolver over N nodes (implicit: one per node)."""
 
@@ -359,6 +414,10 @@ class RefSystem:
             L.ref_last_error.restype = C.c_char_p
             L.ref_num_jac_comp.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
             L.ref_num_rejected.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+            L.ref_solve.argtypes = [C.c_void_p, _dp, _dp, C.c_uint64, C.c_int]
+            L.ref_solve.restype = C.c_int
+            L.ref_num_field_states.argtypes = [C.c_void_p]
+            L.ref_num_field_states.restype = C.c_uint32
             L.ref_compute_jacobian.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
             L.ref_lu_factorize.argtypes = [C.c_void_p, _dp]
             L.ref_forward_backward_subst.argtypes = [C.c_void_p, _dp, _dp, _dp]
@@ -416,6 +475,16 @@ class RefSystem:
     def num_jac_comp(self) -> np.ndarray:
         out = np.zeros(self.N, dtype=np.int64)
         self.lib().ref_num_jac_comp(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)))
+        return out
+
+    def solve(self, t: np.ndarray, tangled: bool = True) -> np.ndarray:
+        """ODESystemSolver::solve over the times t: [nt][N][nfs] (tangled) or
+        [nt][nfs][N]; row 0 is left zero as the reference leaves it."""
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        nfs = int(self.lib().ref_num_field_states(self.h))
+        out = np.zeros((t.size, self.N, nfs) if tangled else (t.size, nfs, self.N))
+        if self.lib().ref_solve(self.h, _ptr(out), _ptr(t), t.size, int(tangled)):
+            raise RuntimeError(self.lib().ref_last_error(self.h).decode())
         return out
 
     def num_rejected(self) -> np.ndarray:

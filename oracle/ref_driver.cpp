@@ -279,6 +279,29 @@ __attribute__((visibility("default"))) int ref_forward(void* h, double t, double
     return failures;
 }
 
+// ODESystemSolver::solve (ODESystemSolver.cpp:81-99) of an explicit solver
+// over all nodes: field states of the plugin model at the times t[1..nt-1]
+// ([nt][N][nfs] tangled, [nt][nfs][N] untangled; row 0 is not written).
+__attribute__((visibility("default"))) int ref_solve(void* h, double* field_states, double* t, uint64_t nt,
+                                                    int tangled)
+{
+    auto* r = static_cast<RefSystem*>(h);
+    if (!r->system)
+        return 1;
+    try {
+        r->system->solve(field_states, t, nt, tangled != 0);
+    } catch (const std::exception& e) {
+        r->error = e.what();
+        return 1;
+    }
+    return 0;
+}
+
+__attribute__((visibility("default"))) uint32_t ref_num_field_states(void* h)
+{
+    return static_cast<RefSystem*>(h)->ode->num_field_states();
+}
+
 __attribute__((visibility("default"))) const char* ref_last_error(void* h)
 {
     return static_cast<RefSystem*>(h)->error.c_str();

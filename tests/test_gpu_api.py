@@ -267,3 +267,77 @@ def test_measure_peaks_through_the_c_abi():
     assert 1e12 < xu.value < 1e13, xu.value
     assert 1e13 < fp.value < 1e14, fp.value
     assert _capi.lib().goss_measure_peaks(0, None, C.byref(fp)) != 0  # NULL output rejected
+
+
+def test_measure_fp64_peak_through_the_c_abi():
+    """goss_measure_fp64_peak: FP64 fused multiply-adds per second on cuda:0
+    (B200 nominal ~37 TFLOP/s FP64 vector, i.e. ~1.9e13 FMA/s)."""
+    import ctypes as C
+
+    from goss_b200 import _capi
+
+    f = C.c_double(0.0)
+    assert _capi.lib().goss_measure_fp64_peak(0, C.byref(f)) == 0
+    assert 1e12 < f.value < 1e14, f.value
+    assert _capi.lib().goss_measure_fp64_peak(0, None) != 0
+
+
+def test_printed_fp64_grl1_matches_oracle():
+    """GOSS_FP64_PRINTED: GRL1 with the model in its printed operation order
+    (the plain FP64 path); within 1e-10 of the oracle like the split FP64."""
+    import pyoracle
+    from helpers import oracle_model, parity, perturbed_states
+
+    N = 40
+    ode = goss.ParameterizedODE("tentusscher_panfilov_2006_M_cell")
+    om = oracle_model("tentusscher_panfilov_2006_M_cell")
+    y0 = perturbed_states(om.ic, N, np.random.default_rng(4), 0.05)
+    solver = goss.solvers.GRL1(ode)
+    solver.internal_time_step = 0.01
+    printed = goss.ODESystemSolver(N, solver, ode, precision="double_printed")
+    assert printed.precision == "double_printed"
+    printed.set_states(y0)
+    o = pyoracle.OracleSystem(om, "GRL1", N, ldt=0.01)
+    o.states[:] = y0
+    for k in range(30):
+        printed.forward(float(k), 1.0)
+        o.forward(float(k), 1.0)
+    assert parity(printed.states, o.states, rtol=1e-10) <= 1.0
+    with pytest.raises(GossError):
+        goss.ODESystemSolver(4, goss.solvers.RK4(ode), ode, precision="double_printed")
+
+
+@pytest.mark.parametrize("tangled", [True, False])
+def test_solve_matches_reference_solve(tangled):
+    """goss_system_solve against the reference's own ODESystemSolver::solve
+    (ODESystemSolver.cpp:81-99, oracle/_ref with a plugin whose field states
+    are V and Ca_i): TP06 GRL1, 9 nodes, 21 output times over 20 ms,
+    tangled and untangled storage, within 1e-10."""
+    import ctypes as C
+
+    import pyoracle
+    from goss_b200 import _capi
+    from helpers import meta, parity, perturbed_states, variant_dir
+
+    name, fs = "tentusscher_panfilov_2006_M_cell", ("V", "Ca_i")
+    plugin = pyoracle.field_state_plugin(name, fs) if pyoracle.ref_available() else None
+    if plugin is None or not plugin.exists():
+        pytest.skip("reference solvers (oracle/_ref) not built")
+    om = oracle_model(name)
+    N = 9
+    y0 = perturbed_states(om.ic, N, np.random.default_rng(12), 0.05)
+    t = np.linspace(0.0, 20.0, 21)
+    r = pyoracle.RefSystem(plugin, meta(variant_dir(name))["class_name"], "GRL1", N, om.solver_params("GRL1", ldt=0.01))
+    r.set_states(y0)
+    ref = r.solve(t, tangled)
+    ode = goss.ParameterizedODE(name, field_states=list(fs))
+    system = goss.ODESystemSolver(N, goss.solvers.GRL1(ode), ode)
+    system.solver.internal_time_step = 0.01
+    system.set_states(y0)
+    out = np.zeros_like(ref)
+    system._sync_params()
+    _capi.check(_capi.lib().goss_system_solve(system._h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                              t.ctypes.data_as(C.POINTER(C.c_double)), t.size, int(tangled)),
+                system._h)
+    assert np.all(out[0] == 0.0) and np.all(ref[0] == 0.0)
+    assert parity(out[1:], ref[1:], rtol=1e-10) <= 1.0

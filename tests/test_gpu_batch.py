@@ -150,3 +150,49 @@ def test_batch_rejects_implicit_solvers():
     s = goss.ODESystemSolver(4, goss.solvers.ThetaSolver(ode), ode)
     with pytest.raises(ValueError):
         goss.BatchSolver([s])
+
+
+def _oracle_pops(pops):
+    """One oracle system (the C restatement of the reference solvers) per
+    population, with the population's current states and field parameters."""
+    import pyoracle
+    from helpers import oracle_model
+
+    out = []
+    for (model, fps, solver, n), p in zip(POPS, pops):
+        om = oracle_model(model, tuple(fps))
+        o = pyoracle.OracleSystem(om, solver, n, ldt=0.01)
+        o.states[:] = p.states
+        o.field_params[:] = p.field_parameters
+        out.append(o)
+    return out
+
+
+def test_batch_fp64_matches_oracle():
+    """Every population of one persistent batch launch against the oracle
+    directly: FP64 within 1e-10 (RK4 for FitzHugh-Nagumo and the oscillator,
+    GRL1 for TT04 and TP06, per-node field parameters)."""
+    pops = make_pops("double")
+    oracles = _oracle_pops(pops)
+    batch = goss.BatchSolver(pops)
+    for k in range(15):
+        batch.forward(k * 0.5, 0.5)
+        for o in oracles:
+            assert o.forward(k * 0.5, 0.5) == 0
+    for p, o in zip(pops, oracles):
+        assert parity(p.states, o.states, rtol=1e-10) <= 1.0
+
+
+def test_batch_graph_fused_forwards_fp64_matches_oracle():
+    """A captured graph of 40 forwards of 0.05 ms run in one launch (states on
+    chip between forwards) against the oracle's 40 forward calls."""
+    pops = make_pops("double", seed=6)
+    oracles = _oracle_pops(pops)
+    batch = goss.BatchSolver(pops)
+    batch.capture(1.0, 0.05, 40)
+    batch.replay()
+    for k in range(40):
+        for o in oracles:
+            assert o.forward(1.0 + k * 0.05, 0.05) == 0
+    for p, o in zip(pops, oracles):
+        assert parity(p.states, o.states, rtol=1e-10) <= 1.0

@@ -110,3 +110,52 @@ def test_views_save_restore_and_errors():
         cpl.to_field_states(torch.zeros(NUM_DOFS, dtype=torch.float32, device="cuda"))
     with pytest.raises(ValueError):
         cpl.to_field_states(torch.zeros(NUM_DOFS + 1, dtype=torch.float64, device="cuda"))
+
+
+def test_device_coupling_matches_reference_solvers():
+    """The same cable with the reference's own solvers on the host arm: each
+    population is the reference's compiled ODESystemSolver (oracle/_ref; the
+    C restatement where it is not built) and V goes into and out of its field
+    states every step, as DOLFINODESystemSolver.step does
+    (python/goss/dolfinutils.py:750-780).  V within 1e-10 (of max(|V|, 1 mV))."""
+    import torch
+
+    import pyoracle
+    from helpers import oracle_model, ref_system
+
+    host = {}
+    for label, model, n in (("tp06", "tentusscher_panfilov_2006_M_cell", 900),
+                            ("tt04", "tentusscher_2004_mcell", NUM_DOFS - 900)):
+        r = ref_system(model, "GRL1", n, ldt=0.01)
+        if r is None:
+            o = pyoracle.OracleSystem(oracle_model(model), "GRL1", n, ldt=0.01)
+            r = (lambda o=o: o.states.copy(), lambda y, o=o: o.states.__setitem__(slice(None), y),
+                 lambda t, dt, o=o: o.forward(t, dt))
+        else:
+            r = (r.get_states, r.set_states, r.forward)
+        om = oracle_model(model)
+        r[1](np.tile(om.ic, (n, 1)))
+        host[label] = r
+    sys_d, dofs = populations()
+    iv = {lab: s.ode.state_names.index("V") for lab, s in sys_d.items()}
+    v = initial_v(sys_d, dofs)
+    v0 = v.copy()
+    for k in range(STEPS):
+        for lab, (get, put, fwd) in host.items():
+            y = get()
+            y[:, iv[lab]] = v[dofs[lab]]          # to_field_states
+            put(y)
+            assert fwd(k * DT, DT) == 0
+            v[dofs[lab]] = get()[:, iv[lab]]       # from_field_states
+        v = diffuse_np(v)
+
+    cpl = FieldStateCoupling(sys_d, dofs, NUM_DOFS)
+    vd = torch.tensor(v0, device="cuda")
+    for k in range(STEPS):
+        cpl.step((k * DT, (k + 1) * DT), vd)
+        diffuse_torch(vd)
+    cpl.synchronize()
+    torch.cuda.synchronize()
+    got = vd.cpu().numpy()
+    assert got.max() > 0
+    assert np.max(np.abs(got - v) / np.maximum(np.abs(v), 1.0)) < 1e-10
