@@ -74,13 +74,15 @@ def profile_run(args):
 
     if args.profile in _IMPLICIT_PROFILES:
         label = _IMPLICIT_PROFILES[args.profile]
-        _, name, ldt, _, jac = next(c for c in IMPLICIT_SOLVERS if c[0] == label)
+        _, name, ldt, _, jac, sp = next(c for c in IMPLICIT_SOLVERS if c[0] == label)
         nodes = 65_536
         md, y0, fp = implicit_inputs(nodes)
         ode = goss.ParameterizedODE(IMPLICIT_MODEL, field_parameters=IMPLICIT_FIELDS,
                                     code_params={"generate_jacobian": jac})
         solver = goss.solvers.solver_mapper[name](ode)
         solver.internal_time_step = ldt
+        for k, v in sp.items():
+            solver.set_parameter(k, v)
         system = goss.ODESystemSolver(nodes, solver, ode)
         system.set_states(y0)
         system.field_parameters = fp
@@ -286,10 +288,12 @@ def run_gpu(args, rank, world, dist):
         s64 = make("double")
         fp64_ms, _ = timed(s64, args.steps, args.warmup)
     # --- plain FP64 GPU path: one launch per internal step (states through HBM
-    #     every step, as goss's PyCUDA path launches one kernel per substep) ---
+    #     every step, as goss's PyCUDA path launches one kernel per substep),
+    #     the model evaluated in its printed operation order (the arithmetic of
+    #     the reference's generated model code) ---
     plain64 = None
     if not args.skip_fp64:
-        sp = make("double")
+        sp = make("double_printed")
         t = 0.0
         for _ in range(50):
             sp.forward_async(t, LDT)
@@ -340,6 +344,8 @@ def run_gpu(args, rank, world, dist):
     e2e_s = time.perf_counter() - w0
     del e2e
 
+    out["grl2"] = run_grl2(dev, y0, fp) if not args.skip_fp64 else None
+    out["accuracy"] = run_accuracy(dev) if not args.skip_fp64 and rank == 0 else None
     out["batched"] = run_batched(args, dev) if not args.skip_fp64 else None
     out["adjoint"] = run_adjoint(dev) if not args.skip_fp64 else None
     out["implicit"] = run_implicit(dev) if not args.skip_fp64 else None
@@ -358,6 +364,174 @@ def run_gpu(args, rank, world, dist):
         model_time_ms=t_end,
     ))
     return out, md
+
+
+def run_grl2(dev, y0, fp, warmup=1, steps=3):
+    """GRL2 (GRL2.cpp:63-86) on the headline workload (1,048,576 TP06 nodes,
+    the same states and lognormal fields, forward(t, 10 ms) at 0.01 ms):
+    cell-steps/s in FP32 and FP64, CUDA events on the launch stream."""
+    import torch
+
+    import goss_b200 as goss
+
+    ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS)
+    stream = torch.cuda.Stream(device=dev)
+    out = {"workload": f"{MODEL} GRL2 dt=0.01ms, {y0.shape[0]} nodes, 4 lognormal field parameters, "
+                       f"10 ms per step, {warmup} warm-up + {steps} timed steps", "unit": "cell-steps/s"}
+    for precision in ("single", "double"):
+        solver = goss.solvers.GRL2(ode)
+        solver.internal_time_step = LDT
+        system = goss.ODESystemSolver(y0.shape[0], solver, ode, precision=precision, device=dev)
+        system.set_stream(stream.cuda_stream)
+        system.set_states(y0)
+        system.field_parameters = fp
+        t = 0.0
+        for _ in range(warmup):
+            system.forward_async(t, INTERVAL)
+            t += INTERVAL
+        system.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            system.forward_async(t, INTERVAL)
+            t += INTERVAL
+        e1.record(stream)
+        system.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out["fp32" if precision == "single" else "fp64"] = {
+            "value": y0.shape[0] * round(INTERVAL / LDT) * steps / (ms / 1e3), "ms_per_step": ms / steps}
+        del system
+    out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
+
+
+ACCURACY_NODES, ACCURACY_MS = 4096, 500
+
+
+def accuracy_subset(fp, num=ACCURACY_NODES, seed=SEED + 7):
+    """Node subset of the accuracy check: for each field parameter the two
+    nodes with the largest and the two with the smallest value (16 extreme
+    nodes for 4 fields), then seeded random nodes up to `num`, sorted."""
+    ext = []
+    for k in range(fp.shape[1]):
+        order = np.argsort(fp[:, k], kind="stable")
+        ext += [int(i) for i in (*order[:2], *order[-2:])]
+    ext = list(dict.fromkeys(ext))
+    rng = np.random.default_rng(seed)
+    rest = rng.choice(np.setdiff1d(np.arange(fp.shape[0]), ext), num - len(ext), replace=False)
+    return np.sort(np.concatenate([np.array(ext, dtype=np.int64), rest])), ext
+
+
+def _device_rows(system, n):
+    """Zero-copy torch view [n, ld] of a system's FP64 device state array."""
+    import torch
+
+    ptr, ld = system.device_states()
+
+    class _A:
+        __cuda_array_interface__ = {"shape": (n, ld), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                    "strides": None, "stream": None}
+    return torch.as_tensor(_A(), device=torch.device("cuda", torch.cuda.current_device()))
+
+
+def run_accuracy(dev, ms_total=ACCURACY_MS):
+    """The 1,048,576-node lognormal workload (the headline inputs) for the full
+    500 ms with GRL1 and GRL2, FP64 and FP32, against the reference's own
+    compiled solvers (oracle/_ref, FP64, all host cores) on a node subset.
+
+    Both sides make the same calls, forward(k * 1 ms, 1 ms) for k < 500
+    (100 internal steps of 0.01 ms each); the GPU runs all nodes and its
+    subset is gathered on the device after every call.  Reported per state:
+    the worst relative error |gpu - ref| / max(|ref|, 1e-12) over the subset
+    at every 1 ms sample, and at the end; for FP64 also the parity ratio
+    |gpu - ref| / (1e-12 + 1e-10 |ref|) (<= 1: within 1e-10)."""
+    import threading
+
+    import torch
+
+    import goss_b200 as goss
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from goss_b200 import models
+
+    md, y0, fp = inputs(N_NODES)
+    names = md["state_names"]
+    n = len(names)
+    idx, ext = accuracy_subset(fp)
+    vdir = models.find_variant(MODEL, FIELDS)
+    om = pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
+    plugin = pyoracle.REFDIR / vdir.name / "libplugin.so"
+    kind = "reference" if pyoracle.ref_available() and plugin.exists() else "port"
+    threads = cpu_threads()
+    ref = {}
+
+    def cpu_run(solver):
+        if kind == "reference":
+            r = pyoracle.RefSystem(plugin, md["class_name"], solver, idx.size, om.solver_params(solver, ldt=LDT))
+            r.set_states(y0[idx])
+            r.set_field_parameters(fp[idx])
+            r.set_num_threads(threads)
+            fwd, get = (lambda t: r.forward(t, 1.0)), r.get_states
+        else:
+            o = pyoracle.OracleSystem(om, solver, idx.size, ldt=LDT)
+            o.states[:] = y0[idx]
+            o.field_params[:] = fp[idx]
+            fwd, get = (lambda t: o.forward(t, 1.0, threads=threads)), (lambda: o.states.copy())
+        out = np.empty((ms_total, idx.size, n))
+        for k in range(ms_total):
+            fwd(float(k))
+            out[k] = get()
+        ref[solver] = out
+
+    cpu = threading.Thread(target=lambda: [cpu_run(s) for s in ("GRL1", "GRL2")])
+    w0 = time.perf_counter()
+    cpu.start()
+    ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS)
+    gidx = torch.tensor(idx, device=torch.device("cuda", dev))
+    gpu = {}
+    for solver in ("GRL1", "GRL2"):
+        for precision in ("double", "single"):
+            s = goss.solvers.solver_mapper[solver](ode)
+            s.internal_time_step = LDT
+            system = goss.ODESystemSolver(N_NODES, s, ode, precision=precision, device=dev)
+            system.set_states(y0)
+            system.field_parameters = fp
+            rows = _device_rows(system, n)
+            out = np.empty((ms_total, idx.size, n))
+            for k in range(ms_total):
+                system.forward(float(k), 1.0)
+                out[k] = rows.index_select(1, gidx).T.cpu().numpy()
+            gpu[(solver, precision)] = out
+            del rows, system
+    cpu.join()
+    wall = time.perf_counter() - w0
+
+    def rel(a, b):
+        return np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
+
+    res = {"workload": f"{MODEL}, {N_NODES} nodes, 4 lognormal field parameters (the headline inputs), "
+                       f"forward(k*1ms, 1ms) for k < {ms_total} (dt 0.01 ms)",
+           "subset": f"{idx.size} nodes: the {len(ext)} nodes with the 2 largest and 2 smallest value of each "
+                     f"field, then seeded random nodes",
+           "reference": {"kind": kind, "cores": threads, "solver": "goss ODESystemSolver, FP64"},
+           "samples": f"every 1 ms ({ms_total} samples) and the end", "wall_s": wall}
+    for solver in ("GRL1", "GRL2"):
+        r = ref[solver]
+        entry = {}
+        for precision, key in (("double", "fp64"), ("single", "fp32")):
+            g = gpu[(solver, precision)]
+            e_all = rel(g, r).max(axis=(0, 1))
+            e_end = rel(g[-1], r[-1]).max(axis=0)
+            d = {"max_rel_err": float(e_all.max()), "v_max_rel_err": float(e_all[names.index("V")]),
+                 "max_rel_err_end": float(e_end.max()),
+                 "per_state": {nm: float(e) for nm, e in zip(names, e_all)}}
+            if key == "fp64":
+                d["parity"] = float((np.abs(g - r) / (1e-12 + 1e-10 * np.abs(r))).max())
+            entry[key] = d
+        res[solver] = entry
+    return res
 
 
 BATCH_POPS = [  # heterogeneous workload: model, field parameters, solver, nodes
@@ -588,10 +762,19 @@ def run_coupled(dev, steps=200, pde_dt=0.1):
 
 IMPLICIT_MODEL, IMPLICIT_FIELDS, IMPLICIT_NODES, IMPLICIT_DT = "tentusscher_2004_mcell", ["g_Kr", "g_CaL"], 262_144, 0.1
 # label, solver, internal step, timed intervals, analytic Jacobian (code_params generate_jacobian)
-IMPLICIT_SOLVERS = [("ThetaSolver", "ThetaSolver", 0.1, 10, False), ("ESDIRK23a", "ESDIRK23a", -1.0, 2, False),
-                    ("ThetaSolver+jacobian", "ThetaSolver", 0.1, 20, True),
-                    ("ImplicitEuler+jacobian", "ImplicitEuler", 0.1, 20, True),
-                    ("ESDIRK23a+jacobian", "ESDIRK23a", -1.0, 4, True)]
+# label, solver, internal step, timed intervals, analytic Jacobian, solver parameters.
+# ESDIRK23a runs with min_dt = 1e-4 ms: at the default 1e-3 ms it never accepts a
+# TT04 step (its first attempt at min_dt fails the error test and the step size
+# cannot shrink further -- the reference behaves the same), so the default
+# configuration times rejected attempts only ("min_dt 1e-3" rows).
+ESDIRK_MIN_DT = 1e-4
+IMPLICIT_SOLVERS = [("ThetaSolver", "ThetaSolver", 0.1, 10, False, {}),
+                    ("ESDIRK23a", "ESDIRK23a", -1.0, 10, False, {"min_dt": ESDIRK_MIN_DT}),
+                    ("ThetaSolver+jacobian", "ThetaSolver", 0.1, 20, True, {}),
+                    ("ImplicitEuler+jacobian", "ImplicitEuler", 0.1, 20, True, {}),
+                    ("ESDIRK23a+jacobian", "ESDIRK23a", -1.0, 10, True, {"min_dt": ESDIRK_MIN_DT}),
+                    ("ESDIRK23a min_dt 1e-3", "ESDIRK23a", -1.0, 2, False, {}),
+                    ("ESDIRK23a+jacobian min_dt 1e-3", "ESDIRK23a", -1.0, 2, True, {})]
 
 
 def implicit_inputs(nodes):
@@ -611,10 +794,10 @@ def run_implicit(dev):
     """ThetaSolver (theta 0.5, one 0.1 ms step per interval) and ESDIRK23a
     (adaptive) on TT04 M-cell, 262,144 nodes, FP64 Newton and LU, forward
     (t, 0.1 ms) per step; one untimed interval first.  Unit: node-intervals/s.
-    With the reference's default tolerances ESDIRK23a rejects every TT04 step
-    down to min_dt (0.001 ms) and the states do not advance -- the reference's
-    own behaviour, reproduced -- so its cost is 100 rejected attempts per
-    interval."""
+    ESDIRK23a is timed with min_dt = 1e-4 ms, where it accepts steps; with the
+    reference's default min_dt (0.001 ms) it rejects every TT04 step and the
+    states do not advance -- the reference's own behaviour, reproduced -- so
+    those rows time 100 rejected attempts per interval."""
     import torch
 
     import goss_b200 as goss
@@ -624,10 +807,12 @@ def run_implicit(dev):
                                        code_params={"generate_jacobian": jac}) for jac in (False, True)}
     stream = torch.cuda.current_stream(dev)
     out = {}
-    for label, name, ldt, intervals, jac in IMPLICIT_SOLVERS:
+    for label, name, ldt, intervals, jac, sp in IMPLICIT_SOLVERS:
         ode = odes[jac]
         solver = goss.solvers.solver_mapper[name](ode)
         solver.internal_time_step = ldt
+        for k, v in sp.items():
+            solver.set_parameter(k, v)
         system = goss.ODESystemSolver(IMPLICIT_NODES, solver, ode, device=dev)
         system.set_stream(stream.cuda_stream)
         system.set_states(y0)
@@ -647,6 +832,7 @@ def run_implicit(dev):
         jac, rej, acc = system.counters()
         out[label] = {"value": IMPLICIT_NODES * intervals / (ms / 1e3), "unit": "node-intervals/s",
                      "ms_per_interval": ms / intervals, "intervals": intervals, "internal_time_step": ldt,
+                     "solver_parameters": sp,
                      "jacobians_per_node_interval": float(np.mean(jac)) / (intervals + 1),
                      "rejected_per_node_interval": float(np.mean(rej)) / (intervals + 1),
                      "accepted_per_node_interval": float(np.mean(acc)) / (intervals + 1)}
@@ -655,7 +841,7 @@ def run_implicit(dev):
             **out}
 
 
-def implicit_reference_sample(target_s=6.0):
+def implicit_reference_sample(target_s=3.0):
     """The reference's ThetaSolver / ESDIRK23a (one solver per node, OpenMP)
     on a node subset of the implicit workload: node-intervals/s."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -664,7 +850,7 @@ def implicit_reference_sample(target_s=6.0):
 
     threads = cpu_threads()
     out = {}
-    for label, name, ldt, _, jac in IMPLICIT_SOLVERS:
+    for label, name, ldt, _, jac, sp in IMPLICIT_SOLVERS:
         vdir = models.find_variant(IMPLICIT_MODEL, IMPLICIT_FIELDS, jacobian=jac)
         md = json.loads((vdir / "model.json").read_text())
         om = pyoracle.OracleModel(pyoracle.build_oracle(vdir, md["ident"]), md["ident"])
@@ -674,13 +860,13 @@ def implicit_reference_sample(target_s=6.0):
         for attempt in range(2):
             _, y0, fp = implicit_inputs(nodes)
             if kind == "reference":
-                r = pyoracle.RefSystem(plugin, md["class_name"], name, nodes, om.solver_params(name, ldt=ldt))
+                r = pyoracle.RefSystem(plugin, md["class_name"], name, nodes, om.solver_params(name, ldt=ldt, **sp))
                 r.set_states(y0)
                 r.set_field_parameters(fp)
                 r.set_num_threads(threads)
                 fwd = lambda t: r.forward(t, IMPLICIT_DT)
             else:
-                o = pyoracle.OracleSystem(om, name, nodes, ldt=ldt)
+                o = pyoracle.OracleSystem(om, name, nodes, ldt=ldt, **sp)
                 o.states[:] = y0
                 o.field_params[:] = fp
                 fwd = lambda t: o.forward(t, IMPLICIT_DT, threads=threads)
@@ -697,18 +883,46 @@ def implicit_reference_sample(target_s=6.0):
 
 
 def measured_peaks(dev):
-    """XU-pipe and FP32-FMA peaks of this GPU (goss_measure_peaks), or None."""
+    """XU-pipe, FP32-FMA and FP64-FMA peaks of this GPU (goss_measure_peaks,
+    goss_measure_fp64_peak), or None."""
     import ctypes as C
 
     from goss_b200 import _capi
 
-    xu, fp = C.c_double(0.0), C.c_double(0.0)
+    xu, fp, f64 = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
     try:
         if _capi.lib().goss_measure_peaks(int(dev), C.byref(xu), C.byref(fp)) != 0:
             return None
+        if _capi.lib().goss_measure_fp64_peak(int(dev), C.byref(f64)) != 0:
+            f64.value = 0.0
     except Exception:
         return None
-    return {"xu_ops_per_s": xu.value, "fp32_ops_per_s": fp.value}
+    return {"xu_ops_per_s": xu.value, "fp32_ops_per_s": fp.value, "fp64_fma_per_s": f64.value}
+
+
+# FP64-pipe instructions per TP06 GRL1 cell-step of explicit_kernel<TP06, double,
+# GRL1> (split program): the thread-level dadd + dmul + dfma counts of one ncu
+# capture of `bench.py --profile double --steps 1 --warmup 1 --nodes 262144`
+# divided by the cell-steps of the launch (None: not captured yet)
+FP64_PIPE_OPS_PER_CELL_STEP = None
+
+
+def roofline_fp64(value_fp64, peaks):
+    """FP64 GRL1 against the measured FP64 FMA peak: FP64-pipe instructions
+    per cell-step (ncu) x cell-steps/s over FP64 FMAs/s of independent chains
+    (one instruction each, like a dadd or dmul)."""
+    peak = (peaks or {}).get("fp64_fma_per_s") or None
+    ops = FP64_PIPE_OPS_PER_CELL_STEP
+    out = {"bound": "fp64 pipe", "unit": "Gop/s (FP64 pipe)", "peak": peak / 1e9 if peak else None,
+           "ops_per_cell_step": ops,
+           "peak_source": "measured on this GPU by goss_measure_fp64_peak (independent fma.rn.f64 chains, "
+                          "2048 threads per SM)",
+           "ops_source": "ncu smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum of one "
+                         "explicit_kernel<TP06, double, GRL1> launch / its cell-steps"}
+    if ops and peak and value_fp64:
+        out["achieved"] = ops * value_fp64 / 1e9
+        out["frac"] = ops * value_fp64 / peak
+    return out
 
 
 def roofline(md, value_fp32, ms_per_step, n_nodes, peaks=None):
@@ -769,9 +983,11 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def reference_sample(target_s=15.0):
+def reference_sample(target_s=5.0, warmup=3):
     """Time the reference ODESystemSolver (GRL1, OpenMP over nodes) on a
-    seeded node subset for one 10 ms interval; returns cell-steps/s."""
+    seeded node subset for one 10 ms interval, the one the GPU arm's first
+    timed step covers ([10 W, 10 W + 10) ms after W untimed intervals, so both
+    arms time the same phase of the model); returns cell-steps/s."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
     from goss_b200 import models
@@ -811,11 +1027,18 @@ def reference_sample(target_s=15.0):
     nodes = int(min(max(rate * target_s / steps, nodes), N_NODES))
     nodes = max(threads, nodes // threads * threads)
     obj, fwd = make(nodes)
+    if warmup:  # untimed: [0, 10 W) ms in one call
+        if kind == "reference":
+            obj.forward(0.0, warmup * INTERVAL)
+        else:
+            obj.forward(0.0, warmup * INTERVAL, threads=threads)
+    t_start = warmup * INTERVAL
     t0 = time.perf_counter()
-    fwd(0.0)
+    fwd(t_start)
     dt = time.perf_counter() - t0
     return dict(value=nodes * steps / dt, unit="cell-steps/s", cores=threads, kind=kind,
-                sample=f"{nodes} seeded nodes of the workload x one 10 ms interval (1000 GRL1 steps), "
+                sample=f"{nodes} seeded nodes of the workload x the 10 ms interval [{t_start:g}, "
+                       f"{t_start + INTERVAL:g}) ms (1000 GRL1 steps) after {warmup} untimed intervals, "
                        f"FP64, {threads} OpenMP threads, {dt:.1f} s")
 
 
@@ -835,7 +1058,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        res = reference_sample()
+        res = reference_sample(warmup=args.warmup)
         steps_done = 0
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
@@ -859,7 +1082,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1:
         try:
-            cpu = reference_sample()
+            cpu = reference_sample(warmup=args.warmup)
         except Exception as exc:  # the baseline is reported, never the target
             cpu = {"value": None, "unit": "cell-steps/s", "cores": cpu_threads(), "kind": "reference",
                    "sample": f"failed: {exc}"}
@@ -869,8 +1092,19 @@ def main():
             except Exception as exc:
                 cpu["implicit"] = {"failed": str(exc)}
     if rank == 0:
-        rl = roofline(md, res["value"] / world, res["ms_per_step"], args.nodes,
-                      measured_peaks(int(os.environ.get("LOCAL_RANK", 0))))
+        peaks = measured_peaks(int(os.environ.get("LOCAL_RANK", 0)))
+        rl = roofline(md, res["value"] / world, res["ms_per_step"], args.nodes, peaks)
+        acc = res.get("accuracy")
+        if acc:
+            # the worst cases of the accuracy check, in the config block that
+            # summaries of the line keep
+            config["accuracy_vs_cpu_reference"] = {
+                "fp64_max_rel_err": max(acc[s]["fp64"]["max_rel_err"] for s in ("GRL1", "GRL2")),
+                "fp64_parity_1e-10": max(acc[s]["fp64"]["parity"] for s in ("GRL1", "GRL2")),
+                "fp32_v_max_rel_err": max(acc[s]["fp32"]["v_max_rel_err"] for s in ("GRL1", "GRL2")),
+                "fp32_any_state_max_rel_err": max(acc[s]["fp32"]["max_rel_err"] for s in ("GRL1", "GRL2")),
+                "how": "GRL1 and GRL2, 1,048,576 nodes x 500 ms on the GPU; 4096-node subset incl. the 16 "
+                       "extreme-field nodes vs the reference's compiled solvers, every 1 ms"}
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 states)",
@@ -880,10 +1114,17 @@ def main():
                          "plain_value": res["fp64_plain_value"],
                          "fp32_over_plain_fp64": (res["value"] / world / res["fp64_plain_value"])
                          if res["fp64_plain_value"] else None,
-                         "v_max_rel_err_fp32_vs_fp64": res["v_max_rel_err_fp32_vs_fp64"]},
+                         "plain_path": "one launch per 0.01 ms step, the model in its printed operation "
+                                       "order (GOSS_FP64_PRINTED)",
+                         "v_max_rel_err_fp32_vs_fp64": res["v_max_rel_err_fp32_vs_fp64"],
+                         "roofline": roofline_fp64(res["fp64_value"] / world if res["fp64_value"] else None,
+                                                   peaks)},
+                "grl2": res.get("grl2"),
                 "state_max_rel_err_fp32_vs_fp64": res.get("state_max_rel_err_fp32_vs_fp64"),
                 "batched_heterogeneous": res.get("batched"), "adjoint": res.get("adjoint"),
-                "implicit": res.get("implicit"), "coupled": res.get("coupled")}
+                "implicit": res.get("implicit"), "coupled": res.get("coupled"),
+                # last, so that the end of the line shows it in full
+                "accuracy_vs_cpu_reference": res.get("accuracy")}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

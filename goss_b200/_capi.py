@@ -16,7 +16,7 @@ ABI_VERSION = 3
 
 (GOSS_EXPLICIT_EULER, GOSS_RK4, GOSS_GRL1, GOSS_GRL2, GOSS_THETA, GOSS_ESDIRK23A, GOSS_RL1, GOSS_RL2, GOSS_RK2,
  GOSS_IMPLICIT_EULER) = range(10)
-GOSS_FP64, GOSS_FP32 = 0, 1
+GOSS_FP64, GOSS_FP32, GOSS_FP64_PRINTED = 0, 1, 2
 GOSS_OK, GOSS_ERR_ARGUMENT, GOSS_ERR_CUDA, GOSS_ERR_NEWTON, GOSS_ERR_UNSUPPORTED, GOSS_ERR_TIMEOUT = range(6)
 GOSS_FLAG_NONFINITE, GOSS_FLAG_NEWTON_FAILED, GOSS_FLAG_ITERATION_CAP = 1, 2, 4
 
@@ -140,6 +140,7 @@ _desc = C.POINTER(ModelDesc)
 _PROTOS = {
     "goss_abi_version": (C.c_uint32, []),
     "goss_measure_peaks": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "goss_measure_fp64_peak": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
     "goss_last_error": (C.c_char_p, []),
     "goss_system_last_error": (C.c_char_p, [_sys]),
     "goss_solver_default_params": (C.c_int, [C.c_int32, C.POINTER(SolverParams)]),

@@ -107,7 +107,9 @@ struct EvalArgs {
 // ---------------------------------------------------------------------------
 // explicit solvers
 // ---------------------------------------------------------------------------
-enum class Explicit { Euler, RK4, GRL1, GRL2, RL1, RL2, RK2 };
+// GRL1Printed: GRL1 with the model evaluated in its printed operation order
+// (the arithmetic of the reference's generated model code), FP64 only.
+enum class Explicit { Euler, RK4, GRL1, GRL2, RL1, RL2, RK2, GRL1Printed };
 
 template <class M, typename T>
 __device__ __forceinline__ void load_field(const double* __restrict__ fp, uint64_t ld, uint32_t node,
@@ -237,29 +239,26 @@ struct NodeIO {
     double interval = 0.0;
 };
 
-// The model evaluations the explicit steps use.  FP32 kernels take the split
-// forms (every distinct transcendental and reciprocal evaluated once; they
-// are XU-pipe bound); FP64 kernels take the programs with the reference's
-// operation order (FP64 parity with the reference at 1e-10).
-#ifndef GOSS_FP32_SPLIT
-#define GOSS_FP32_SPLIT 1
-#endif
-template <class M, typename T>
+// The model evaluations the explicit steps use: the split forms (every
+// distinct transcendental and reciprocal of a state-dependent operand
+// evaluated once), in FP32 and in FP64.  The split FP64 programs change the
+// reference's results by re-association only; they stay within 1e-10 of the
+// reference over 10^5 TP06 GRL1 steps.  Printed = true takes the programs in
+// the printed operation order of the model (one exp per occurrence, divisions
+// as written), the arithmetic of the reference's own generated code.
+template <class M, typename T, bool Printed = false>
 __device__ __forceinline__ void model_linearized(const T* y, double t, const T* P, const double* PD, const T* F,
                                                  T* lin, T* rhs)
 {
-    if constexpr (GOSS_FP32_SPLIT && sizeof(T) == 4)
-        M::template linearized_split<T>(y, t, P, PD, F, lin, rhs);
-    else
+    if constexpr (Printed)
         M::template linearized<T>(y, t, P, PD, F, lin, rhs);
+    else
+        M::template linearized_split<T>(y, t, P, PD, F, lin, rhs);
 }
 template <class M, typename T>
 __device__ __forceinline__ void model_rhs(const T* y, double t, const T* P, const double* PD, const T* F, T* f)
 {
-    if constexpr (GOSS_FP32_SPLIT && sizeof(T) == 4)
-        M::template rhs_split<T>(y, t, P, PD, F, f);
-    else
-        M::template rhs<T>(y, t, P, PD, F, f);
+    M::template rhs_split<T>(y, t, P, PD, F, f);
 }
 
 // One internal step of an explicit solver at time lt with step ldt, in place
@@ -315,6 +314,13 @@ __device__ __forceinline__ void explicit_step(Acc<T>* y, const double lt, const 
         // GRL1.h:72-84
         T lin[n], rhs[n];
         model_linearized<M, T>(yt, lt, P, PD, F, lin, rhs);
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+            y[i].add(grl_increment(lin[i], rhs[i], h, delta));
+    } else if constexpr (S == Explicit::GRL1Printed) {
+        // GRL1.h:72-84 over the printed model program
+        T lin[n], rhs[n];
+        model_linearized<M, T, true>(yt, lt, P, PD, F, lin, rhs);
 #pragma unroll
         for (int i = 0; i < n; ++i)
             y[i].add(grl_increment(lin[i], rhs[i], h, delta));
@@ -468,6 +474,15 @@ struct PackedTile {
     __device__ __forceinline__ double& operator[](int k) const { return base[(uint64_t)k * 32]; }
 };
 
+// ... or in shared memory: entry k of the block's thread t at base[k * stride]
+// with base = smem + t and stride = blockDim.x, so a warp's accesses to one
+// entry are 32 consecutive words (no bank conflicts)
+struct PackedShared {
+    double* base;
+    uint32_t stride;
+    __device__ __forceinline__ double& operator[](int k) const { return base[(uint32_t)k * stride]; }
+};
+
 __device__ __forceinline__ PackedTile packed_tile(double* region, uint32_t node, int nnz)
 {
     return PackedTile{region + (((uint64_t)(node >> 5) * (uint64_t)nnz) << 5) + (node & 31u)};
@@ -477,6 +492,7 @@ template <int n>
 __device__ __forceinline__ double l2norm(const double* v)
 {
     double s = 0;
+#pragma unroll
     for (int i = 0; i < n; ++i)
         s += v[i] * v[i];
     return sqrt(s);
@@ -579,16 +595,68 @@ enum ThetaRows { TH_ETA = 0, TH_RECOMPUTE, TH_ALWAYS, TH_JUSTREFINED, TH_JACCOMP
 // it 1.24 -> 1.16 ms, with forward differences unchanged (4.41 ms).  Blocks of
 // up to 256 threads; __launch_bounds__(256, 1) keeps the 255-register budget
 // (without the minimum of one block ptxas capped it at 128 and spilled more).
+//
+// The packed Newton matrix (TT04: 71 values, TP06: 82), the Newton update z1
+// and the explicit part prev live in dynamic shared memory, theta_smem_rows
+// * blockDim.x doubles (210 KB for TT04 in blocks of 256): in registers they
+// pushed the kernel past 255 registers and the spills reached DRAM (5.8x the
+// algorithmic write bytes of an interval).  Models whose rows do not fit for
+// 32 threads keep them in thread-local arrays.
+#ifndef GOSS_THETA_SMEM_VECTORS
+#define GOSS_THETA_SMEM_VECTORS 1
+#endif
+constexpr uint32_t kThetaSmemBytes = 232448;  // 227 KB, the opt-in maximum per block
+template <class M>
+__host__ __device__ constexpr uint32_t theta_smem_rows()
+{
+    return M::lu_nnz + (GOSS_THETA_SMEM_VECTORS ? 2 * M::num_states : 0);
+}
+template <class M>
+__host__ __device__ constexpr bool theta_matrix_in_smem()
+{
+    return (uint64_t)theta_smem_rows<M>() * sizeof(double) * 32 <= kThetaSmemBytes;
+}
+
+// Launch shape: at most GOSS_THETA_THREADS threads per block, compiled for
+// GOSS_THETA_MIN_BLOCKS resident blocks per SM (register cap 65536 / product).
+#ifndef GOSS_THETA_THREADS
+#define GOSS_THETA_THREADS 256
+#endif
+#ifndef GOSS_THETA_MIN_BLOCKS
+#define GOSS_THETA_MIN_BLOCKS 1
+#endif
 template <class M, bool IE>
-__global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ ImplicitArgs<M> a)
+__global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
+    theta_kernel(const __grid_constant__ ImplicitArgs<M> a)
 {
     constexpr int n = M::num_states;
     const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = node < a.N;
     const uint32_t src = active ? node : a.N - 1;  // threads past the end only take part in the barriers
     const goss_solver_params& sp = a.sp;
-    double y[n], z1[n], prev[n], yz[n], f1[n], b[n];
-    double J[M::lu_nnz];
+    double y[n], yz[n], f1[n], b[n];
+    extern __shared__ double theta_smem[];
+    constexpr bool in_smem = theta_matrix_in_smem<M>();
+    constexpr bool vec_smem = in_smem && GOSS_THETA_SMEM_VECTORS;
+    double Jlocal[in_smem ? 1 : M::lu_nnz], z1_local[vec_smem ? 1 : n], prev_local[vec_smem ? 1 : n];
+    const auto J = [&]() {
+        if constexpr (in_smem)
+            return PackedShared{theta_smem + threadIdx.x, blockDim.x};
+        else
+            return static_cast<double*>(Jlocal);
+    }();
+    const auto z1 = [&]() {
+        if constexpr (vec_smem)
+            return PackedShared{theta_smem + (uint32_t)M::lu_nnz * blockDim.x + threadIdx.x, blockDim.x};
+        else
+            return static_cast<double*>(z1_local);
+    }();
+    const auto prev = [&]() {
+        if constexpr (vec_smem)
+            return PackedShared{theta_smem + (uint32_t)(M::lu_nnz + n) * blockDim.x + threadIdx.x, blockDim.x};
+        else
+            return static_cast<double*>(prev_local);
+    }();
 #pragma unroll
     for (int i = 0; i < n; ++i)
         y[i] = a.states[i * a.ld + src];
@@ -616,6 +684,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
     int num_refinements = 0;
     const double eps = kGossEps * 1000;
     uint8_t status = 0;
+#pragma unroll
     for (int i = 0; i < n; ++i)
         prev[i] = 0.0;
     uint64_t guard = 0;
@@ -634,6 +703,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
                 done = true;
                 continue;
             }
+#pragma unroll
             for (int i = 0; i < n; ++i)
                 z1[i] = 0.0;
             if (IE ? num_refinements > sp.num_refinements_without_always_recomputing_jacobian
@@ -652,6 +722,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
                     prev_pending = true;
                 } else {
                     rhs64<M>(y, t, a.P, F, f1);
+#pragma unroll
                     for (int i = 0; i < n; ++i)
                         prev[i] = (1 - sp.theta) * f1[i];
                 }
@@ -660,6 +731,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
         }
         // one iteration of ImplicitODESolver::newton_solve (ImplicitODESolver.cpp:114-245)
         bool newton_done = false;
+#pragma unroll
         for (int i = 0; i < n; ++i)
             yz[i] = y[i] + z1[i];
         // when this iteration will refactorise (both conditions are known
@@ -675,6 +747,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
                     M::fd_clear(J);
                     M::template rhs2_fd_jacobian<double>(yz, tn, a.P, a.P, F, t, b, f1, J);
                 }
+#pragma unroll
                 for (int i = 0; i < n; ++i)
                     prev[i] = (1 - sp.theta) * b[i];
                 prev_pending = false;
@@ -687,6 +760,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
         } else {
             rhs64<M>(yz, tn, a.P, F, f1);
         }
+#pragma unroll
         for (int i = 0; i < n; ++i)
             b[i] = -z1[i] * 1.0 + ldt * (prev[i] + alpha * f1[i]);
         residual = l2norm<n>(b);
@@ -729,6 +803,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
                 newton_done = true;
             }
             if (!newton_done) {
+#pragma unroll
                 for (int i = 0; i < n; ++i)
                     z1[i] += b[i];
                 relative_residual = residual / initial_residual;
@@ -741,6 +816,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
             continue;
         in_step = false;
         if (step_ok) {
+#pragma unroll
             for (int i = 0; i < n; ++i)
                 y[i] += z1[i];
             t += ldt;
@@ -776,6 +852,7 @@ __global__ void __launch_bounds__(256, 1) theta_kernel(const __grid_constant__ I
     if (!active)
         return;
     bool finite = true;
+#pragma unroll
     for (int i = 0; i < n; ++i) {
         a.states[i * a.ld + node] = y[i];
         finite = finite && isfinite(y[i]);
@@ -845,7 +922,22 @@ __device__ __forceinline__ EsdirkCoef esdirk_coefficients()
     return c;
 }
 
-template <class M>
+// a node's vector of n values in thread-local storage
+template <int n>
+struct LocalVec {
+    double v[n];
+    __device__ __forceinline__ double& operator[](int i) { return v[i]; }
+};
+
+// ESDIRK23a's stage derivatives z1..z4 and the explicit part prev of a stage
+// (5 n values per node) are thread-local, or with GOSS_ESDIRK_SMEM in dynamic
+// shared memory (vector k of the block's thread t at rows [k n, (k+1) n),
+// PackedShared layout).
+#ifndef GOSS_ESDIRK_SMEM
+#define GOSS_ESDIRK_SMEM 0
+#endif
+
+template <class M, class V>
 struct EsdirkNode {
     static constexpr int n = M::num_states;
     const double* P;
@@ -856,12 +948,12 @@ struct EsdirkNode {
     double prev_dt, loc_error, eta, dt;
     int newton_iterations, first_step, new_jacobian;
     double jac_comp, rejects, accepted;
-    double z1[n], z2[n], z3[n], z4[n], prev[n], yh[n];
-    double y_int[n], z_int[n], b[n], dz[n], prev_dz[n], g1[n];
+    V z1, z2, z3, z4, prev;
 
     // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
     __device__ void ode_jacobian(double* y, double t)
     {
+        double g1[n];  // f(y), a by-product of the fused evaluations
         if constexpr (M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
             // f(y) and the analytic Jacobian sharing their statements
             M::template rhs_jacobian<double>(y, t, P, P, F, g1, jac);
@@ -884,26 +976,32 @@ struct EsdirkNode {
         M::lu_copy_shift(jac, jfac, -h * c.a22);
         M::lu_factorize(jfac);
     }
-    // ESDIRK23a::compute_stage_val (ESDIRK23a.cpp:201-258)
-    __device__ bool stage(double* z, const double* y, double t_s, double h)
+    // ESDIRK23a::compute_stage_val (ESDIRK23a.cpp:201-258).  The reference keeps
+    // the previous Newton update (prev_dz) only for its norm; the norm is kept
+    // here (the same value: l2norm of the same vector), and the residual b is
+    // formed in place of f(y_int).
+    template <class Z>
+    __device__ bool stage(Z& z, const double* y, double t_s, double h)
     {
         newton_iterations = 0;
         bool conv_ok = true;
-        for (int i = 0; i < n; ++i)
-            dz[i] = 0.0, prev_dz[i] = 0.0;
+        double dz[n], dz_norm = 0.0;
         eta = pow(std_max(eta, c.etamin), 0.8);
         int guard = 0;
         do {
+            double y_int[n], b[n];
+#pragma unroll
             for (int i = 0; i < n; i++)
                 y_int[i] = y[i] + h * prev[i] + c.gamma * h * z[i];
-            rhs64<M>(y_int, t_s, P, F, z_int);
+            rhs64<M>(y_int, t_s, P, F, b);
+#pragma unroll
             for (int i = 0; i < n; i++)
-                b[i] = -z[i] + z_int[i];
-            for (int i = 0; i < n; i++)
-                prev_dz[i] = dz[i];
+                b[i] = -z[i] + b[i];
+            const double prev_dz_norm = dz_norm;
             M::lu_solve(jfac, b, dz);
+            dz_norm = l2norm<n>(dz);
             if (newton_iterations >= 1) {
-                const double theta = l2norm<n>(dz) / l2norm<n>(prev_dz);
+                const double theta = dz_norm / prev_dz_norm;
                 if (!(theta <= 1)) {
                     rejects += 1;
                     conv_ok = false;
@@ -916,19 +1014,25 @@ struct EsdirkNode {
                 conv_ok = false;
                 break;
             }
+#pragma unroll
             for (int i = 0; i < n; i++)
                 z[i] += dz[i];
             newton_iterations++;
-        } while (eta * l2norm<n>(dz) > c.kappa * c.tol);
+        } while (eta * dz_norm > c.kappa * c.tol);
         return conv_ok;
     }
     // ESDIRK23a::do_step (ESDIRK23a.cpp:134-199)
     __device__ bool do_step(double* y, double t0, double h)
     {
-        rhs64<M>(y, t0, P, F, z1);
-        for (int i = 0; i < n; i++) {
-            z2[i] = z1[i];
-            prev[i] = z1[i] * c.a21;
+        {
+            double f0[n];
+            rhs64<M>(y, t0, P, F, f0);
+#pragma unroll
+            for (int i = 0; i < n; i++) {
+                z1[i] = f0[i];
+                z2[i] = f0[i];
+                prev[i] = f0[i] * c.a21;
+            }
         }
         bool step_ok = stage(z2, y, t0 + c.c2 * h, h);
         if (step_ok) {
@@ -946,6 +1050,8 @@ struct EsdirkNode {
             step_ok = stage(z4, y, t0 + c.c4 * h, h);
         }
         if (step_ok) {
+            double yh[n];
+#pragma unroll
             for (int i = 0; i < n; i++)
                 yh[i] = h * ((c.b1 - c.bh1) * z1[i] + (c.b2 - c.bh2) * z2[i] + (c.b3 - c.gamma) * z3[i] +
                              c.gamma * z4[i]);
@@ -1003,7 +1109,21 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
     double F[Dims<M>::nfp];
     load_field<M, double>(a.fparams, ld, node, F);
     double* ss = a.sstate + node;
-    EsdirkNode<M> s;
+#if GOSS_ESDIRK_SMEM
+    extern __shared__ double esdirk_smem[];
+    EsdirkNode<M, PackedShared> s;
+    {
+        double* base = esdirk_smem + threadIdx.x;
+        const uint32_t rows = (uint32_t)n * blockDim.x;
+        s.z1 = PackedShared{base, blockDim.x};
+        s.z2 = PackedShared{base + rows, blockDim.x};
+        s.z3 = PackedShared{base + 2 * rows, blockDim.x};
+        s.z4 = PackedShared{base + 3 * rows, blockDim.x};
+        s.prev = PackedShared{base + 4 * rows, blockDim.x};
+    }
+#else
+    EsdirkNode<M, LocalVec<n>> s;
+#endif
     s.P = a.P;
     s.F = F;
     s.sp = &a.sp;
@@ -1178,18 +1298,32 @@ inline int launch_implicit(const goss_launch* L)
     // ThetaSolver / ImplicitEuler: lockstep blocks of 256 (kernel limit 256);
     // ESDIRK23a: 64 (limit 128)
     const bool theta = L->solver == GOSS_THETA || L->solver == GOSS_IMPLICIT_EULER;
-    const unsigned block = L->block ? L->block : (theta ? 256 : 64);
-    if (block > (theta ? 256u : 128u))
+    unsigned block = L->block ? L->block : (theta ? GOSS_THETA_THREADS : 64);
+    if (block > (theta ? (unsigned)GOSS_THETA_THREADS : 128u))
         return GOSS_ERR_ARGUMENT;
+    if (theta && theta_matrix_in_smem<M>()) {
+        // as many threads as the block's shared rows leave room for
+        const unsigned fit = kThetaSmemBytes / (unsigned)(sizeof(double) * theta_smem_rows<M>()) / 32u * 32u;
+        block = block < fit ? block : fit;
+    }
     const unsigned grid = (L->num_nodes + block - 1) / block;
     if (grid == 0)
         return 0;
-    if (L->solver == GOSS_THETA)
-        theta_kernel<M, false><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
-    else if (L->solver == GOSS_IMPLICIT_EULER)
-        theta_kernel<M, true><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
-    else
-        esdirk_kernel<M><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    if (theta) {
+        // the block's shared rows in dynamic shared memory
+        const size_t smem = theta_matrix_in_smem<M>() ? sizeof(double) * (size_t)theta_smem_rows<M>() * block : 0;
+        auto kernel = L->solver == GOSS_THETA ? theta_kernel<M, false> : theta_kernel<M, true>;
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return GOSS_ERR_CUDA;
+        kernel<<<grid, block, smem, (cudaStream_t)L->stream>>>(a);
+    } else {
+        const size_t smem = GOSS_ESDIRK_SMEM ? sizeof(double) * 5 * (size_t)M::num_states * block : 0;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(esdirk_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess)
+            return GOSS_ERR_CUDA;
+        esdirk_kernel<M><<<grid, block, smem, (cudaStream_t)L->stream>>>(a);
+    }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
 }
 
@@ -1197,6 +1331,8 @@ template <class M>
 inline int launch_solver(const goss_launch* L)
 {
     const bool f32 = L->precision == GOSS_FP32;
+    if (L->precision == GOSS_FP64_PRINTED)
+        return L->solver == GOSS_GRL1 ? launch_explicit<M, double, Explicit::GRL1Printed>(L) : GOSS_ERR_UNSUPPORTED;
     switch (L->solver) {
     case GOSS_EXPLICIT_EULER:
         return f32 ? launch_explicit<M, float, Explicit::Euler>(L) : launch_explicit<M, double, Explicit::Euler>(L);

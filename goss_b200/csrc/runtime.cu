@@ -5,6 +5,7 @@
 // component-major state and field-parameter arrays, the per-node solver state
 // of the implicit solvers, a stream and a status word, and it drives the
 // model module's solver kernels through goss_model_desc::launch.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -254,7 +255,8 @@ int launch_forward(goss_system* s, double t, double interval)
     int rc = s->m->launch(&L);
     if (rc == GOSS_ERR_UNSUPPORTED)
         return fail(&s->last_error, rc, "solver %d is not available in %s precision for model %s", s->solver,
-                    s->precision == GOSS_FP32 ? "FP32" : "FP64", s->m->name);
+                    s->precision == GOSS_FP32 ? "FP32" : s->precision == GOSS_FP64_PRINTED ? "printed FP64" : "FP64",
+                    s->m->name);
     if (rc) {
         cudaError_t e = cudaGetLastError();
         return fail(&s->last_error, rc, "kernel launch failed: %s", cudaGetErrorString(e));
@@ -378,6 +380,80 @@ GOSS_API int goss_measure_peaks(int32_t device, double* xu_ops_per_s, double* fp
     *fp32_ops_per_s = best_fma;
     return 0;
 }
+
+namespace {
+constexpr int kDfmaChains = 8;
+
+__global__ void peak_dfma_kernel(double* sink, int iters)
+{
+    double x[kDfmaChains];
+#pragma unroll
+    for (int c = 0; c < kDfmaChains; ++c)
+        x[c] = 0.5 + 0.01 * (threadIdx.x & 7) + 0.05 * c;
+    const double a = 0.999, b = 0.001;
+    for (int k = 0; k < iters; ++k) {
+#pragma unroll
+        for (int c = 0; c < kDfmaChains; ++c)
+            asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(x[c]) : "d"(a), "d"(b));
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < kDfmaChains; ++c)
+        s += x[c];
+    if (s == 12345.0)
+        sink[blockIdx.x] = s;
+}
+}  // namespace
+
+GOSS_API int goss_measure_fp64_peak(int32_t device, double* fp64_fma_per_s)
+{
+    if (!fp64_fma_per_s)
+        return fail(nullptr, GOSS_ERR_ARGUMENT, "NULL output");
+    cudaError_t e = cudaSetDevice(device);
+    int sms = 0;
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "measure FP64 peak: %s", cudaGetErrorString(e));
+    const int block = 256, grid = sms * 8;  // 2048 threads per SM
+    const int iters = 2048;
+    double* sink = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double best = 0.0;
+    e = cudaMalloc(&sink, sizeof(double) * grid);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e0);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e1);
+    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {  // the first is a warm-up
+        float ms = 0.0f;
+        cudaEventRecord(e0, st);
+        peak_dfma_kernel<<<grid, block, 0, st>>>(sink, iters);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && rep && ms > 0)
+            best = std::max(best, (double)grid * block * iters * kDfmaChains / (ms * 1e-3));
+    }
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
+    if (e0)
+        cudaEventDestroy(e0);
+    if (e1)
+        cudaEventDestroy(e1);
+    if (st)
+        cudaStreamDestroy(st);
+    cudaFree(sink);
+    if (e != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "measure FP64 peak: %s", cudaGetErrorString(e));
+    *fp64_fma_per_s = best;
+    return 0;
+}
+
 GOSS_API const char* goss_last_error(void) { return g_last_error.c_str(); }
 GOSS_API const char* goss_system_last_error(const goss_system* s) { return s ? s->last_error.c_str() : ""; }
 
@@ -410,11 +486,13 @@ GOSS_API int goss_system_create(const goss_model_desc* m, int32_t solver, const 
         return fail(nullptr, GOSS_ERR_ARGUMENT, "model descriptor missing or built for another ABI version");
     if (solver < 0 || solver >= GOSS_NUM_SOLVERS || !(m->supported_solvers & (1u << solver)))
         return fail(nullptr, GOSS_ERR_UNSUPPORTED, "solver kind %d is not available for model %s", solver, m->name);
-    if (precision != GOSS_FP64 && precision != GOSS_FP32)
+    if (precision != GOSS_FP64 && precision != GOSS_FP32 && precision != GOSS_FP64_PRINTED)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "invalid precision %d", precision);
     if ((solver == GOSS_THETA || solver == GOSS_ESDIRK23A || solver == GOSS_IMPLICIT_EULER) && precision == GOSS_FP32)
         return fail(nullptr, GOSS_ERR_UNSUPPORTED,
                     "implicit solvers run their Newton iteration in FP64; use GOSS_FP64 precision");
+    if (precision == GOSS_FP64_PRINTED && solver != GOSS_GRL1)
+        return fail(nullptr, GOSS_ERR_UNSUPPORTED, "GOSS_FP64_PRINTED is available for GRL1 only");
     auto* s = new goss_system();
     s->m = m;
     s->solver = solver;
@@ -1258,29 +1336,71 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
-double* g_scratch_ptr[kMaxDevices] = {};
+struct ScratchAddress {
+    unsigned long long context = 0;  // the context the address belongs to
+    double* ptr = nullptr;
+};
+ScratchAddress g_scratch[kMaxDevices];
+
+// Identifier of the calling thread's current CUDA context, 0 if it cannot be
+// read.  The driver functions are reached through the runtime's entry-point
+// query, so the library does not link the driver library itself.
+unsigned long long current_context_id()
+{
+    typedef CUresult (*get_current_fn)(CUcontext*);
+    typedef CUresult (*get_id_fn)(CUcontext, unsigned long long*);
+    static get_current_fn get_current = nullptr;
+    static get_id_fn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<get_current_fn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<get_id_fn>(f);
+    });
+    CUcontext ctx = nullptr;
+    if (!get_current || get_current(&ctx) != CUDA_SUCCESS || !ctx)
+        return 0;
+    unsigned long long id = 0;
+    if (get_id && get_id(ctx, &id) == CUDA_SUCCESS)
+        return id;
+    return (unsigned long long)(uintptr_t)ctx;
+}
 
 // Device address of g_eval_scratch on the current device.  In host code the
-// symbol is only a host-side stand-in, so the address is looked up once per
-// device with that device current and cached.
+// symbol is only a host-side stand-in, so the address is looked up with the
+// device current: once per device, and again when the device's context is
+// no longer the one the cached address belongs to (after cudaDeviceReset the
+// array lives in a new context at a new address).
 int noalloc_scratch(double** out)
 {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaSetDevice(dev);  // makes the device's primary context current
     if (e != cudaSuccess)
-        return fail(nullptr, GOSS_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+        return fail(nullptr, GOSS_ERR_CUDA, "cannot make the current device's context current: %s",
+                    cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "device ordinal %d out of range", dev);
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
+    ScratchAddress& a = g_scratch[dev];
+    if (!a.ptr || ctx == 0 || a.context != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_eval_scratch);
         if (e != cudaSuccess || !p)
             return fail(nullptr, GOSS_ERR_CUDA, "cudaGetSymbolAddress of the evaluation scratch failed: %s",
                         cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<double*>(p);
+        a.ptr = static_cast<double*>(p);
+        a.context = ctx;
     }
-    *out = g_scratch_ptr[dev];
+    *out = a.ptr;
     return 0;
 }
 
@@ -1351,6 +1471,12 @@ GOSS_API int goss_model_eval_noalloc(const goss_model_desc* m, int32_t what, int
                     "scratch holds %u (at most %llu states of this model)",
                     (unsigned long long)count, m->name, (unsigned long long)need, GOSS_NOALLOC_SCRATCH_DOUBLES,
                     (unsigned long long)(GOSS_NOALLOC_SCRATCH_DOUBLES / (n + nfp + width) / 32 * 32));
+    // an error left by the caller's own earlier work is reported as such (and
+    // left pending), not blamed on this call's kernels
+    cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+        return fail(nullptr, GOSS_ERR_CUDA, "goss_model_eval_noalloc: a CUDA error from earlier work is pending: %s",
+                    cudaGetErrorName(pending));
     double* scratch = nullptr;
     int rc = noalloc_scratch(&scratch);
     if (rc)
@@ -1374,7 +1500,8 @@ GOSS_API int goss_model_eval_noalloc(const goss_model_desc* m, int32_t what, int
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
-        return fail(nullptr, GOSS_ERR_CUDA, "layout kernel launch failed: %s", cudaGetErrorString(e));
+        return fail(nullptr, GOSS_ERR_CUDA, "goss_model_eval_noalloc: layout kernel launch failed: %s (%s)",
+                    cudaGetErrorName(e), cudaGetErrorString(e));
     goss_eval_launch L{};
     L.what = what;
     L.precision = precision;

@@ -12,8 +12,10 @@ reference reads the shared solver and ODE objects), so changing
 takes effect on the next step.
 
 Extra keyword arguments beyond the reference API: ``precision`` ("double" —
-FP64 everywhere — or "single": FP32 model arithmetic with FP64 state
-accumulation) and ``device`` (CUDA ordinal).
+FP64 everywhere —, "single": FP32 model arithmetic with FP64 state
+accumulation, or "double_printed": FP64 with the model evaluated in the
+printed operation order of the reference's generated code, GRL1 only) and
+``device`` (CUDA ordinal).
 """
 from __future__ import annotations
 
@@ -40,6 +42,8 @@ def _precision(p) -> int:
         return _capi.GOSS_FP64
     if p in ("single", "float", "float32", "fp32", _capi.GOSS_FP32):
         return _capi.GOSS_FP32
+    if p in ("double_printed", _capi.GOSS_FP64_PRINTED):
+        return _capi.GOSS_FP64_PRINTED
     raise ValueError(f"unknown precision {p!r}")
 
 
@@ -112,7 +116,7 @@ class ODESystemSolver:
 
     @property
     def precision(self) -> str:
-        return "single" if self._precision == _capi.GOSS_FP32 else "double"
+        return {_capi.GOSS_FP32: "single", _capi.GOSS_FP64_PRINTED: "double_printed"}.get(self._precision, "double")
 
     @property
     def num_threads(self) -> int:

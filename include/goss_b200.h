@@ -54,8 +54,12 @@ enum goss_solver_kind {
 
 /* Arithmetic of the right-hand side.  States are always stored and
  * accumulated in FP64; GOSS_FP32 evaluates the model and the explicit
- * update in FP32 (implicit solvers keep Newton and LU in FP64). */
-enum goss_precision { GOSS_FP64 = 0, GOSS_FP32 = 1 };
+ * update in FP32 (implicit solvers keep Newton and LU in FP64).  GOSS_FP64
+ * evaluates the model's split program (every distinct exponential and
+ * reciprocal once); GOSS_FP64_PRINTED evaluates it in the printed operation
+ * order of the reference's generated model code (GRL1 only: the plain FP64
+ * path the FP32 kernels are compared with). */
+enum goss_precision { GOSS_FP64 = 0, GOSS_FP32 = 1, GOSS_FP64_PRINTED = 2 };
 
 enum goss_status {
     GOSS_OK = 0,
@@ -390,10 +394,13 @@ GOSS_API const char* goss_batch_last_error(const goss_batch* batch);
  * goss_model_eval_noalloc_capacity() doubles (16 MiB) that every GPU using
  * this library keeps until the process exits; (n + nfp + width) * count,
  * with count rounded up to 32, must fit or the call fails with
- * GOSS_ERR_ARGUMENT.  The first call on a device looks up that array's
- * device address (make the first call before any stream capture).  All calls
- * share the array, so calls that overlap on the GPU (other streams, other
- * threads) race; the call synchronises `stream` before it returns. */
+ * GOSS_ERR_ARGUMENT.  The first call on a device, and the first after the
+ * device's context was reset, looks up that array's device address; make
+ * that first call before any stream capture begins.  All calls share the
+ * array and it keeps the last call's contents, so calls that overlap on the
+ * GPU (other streams, other threads) race; the call synchronises `stream`
+ * before it returns.  A CUDA error left pending by earlier work is reported
+ * (GOSS_ERR_CUDA) and left pending. */
 GOSS_API int goss_model_eval_noalloc(const goss_model_desc* model, int32_t what, int32_t precision,
                                      const double* params, const double* states, const double* field_params,
                                      const double* times, uint64_t count, double* out, void* stream);
@@ -416,6 +423,10 @@ GOSS_API uint32_t goss_abi_version(void);
  * reciprocals) and FP32 fused multiply-adds per second (one op each), each the
  * best of three timed launches filling every SM.  Takes a few milliseconds. */
 GOSS_API int goss_measure_peaks(int32_t device, double* xu_ops_per_s, double* fp32_ops_per_s);
+/* No counterpart in the reference: FP64 fused multiply-adds per second on
+ * `device` (independent fma.rn.f64 chains, 2048 threads per SM, best of three
+ * timed launches), the FP64-pipe peak of the FP64 model kernels' roofline. */
+GOSS_API int goss_measure_fp64_peak(int32_t device, double* fp64_fma_per_s);
 
 #ifdef __cplusplus
 }

@@ -284,3 +284,38 @@ def test_analytic_jacobian_eval_matches_oracle():
         assert np.max(np.abs(a - b) / scale) < 1e-12
     plain = goss.ParameterizedODE("tentusscher_2004_mcell", field_parameters=list(fps))
     assert not plain.has_jacobian
+
+
+@pytest.mark.parametrize("solver", ["GRL1", "GRL2"])
+def test_lognormal_fields_2048_nodes_100ms(solver):
+    """The headline workload's inputs at 2,048 nodes for 100 ms (stimulus and
+    upstroke included), four lognormal (sigma 0.2) conductance fields: FP64
+    within 1e-10 of the oracle for every state, FP32 V within 1e-3."""
+    fps = ("g_Kr", "g_Ks", "g_CaL", "g_to")
+    name = "tentusscher_panfilov_2006_M_cell"
+    md = meta(variant_dir(name, fps))
+    rng = np.random.default_rng(1234)
+    N = 2048
+    om = oracle_model(name, fps)
+    y0 = perturbed_states(om.ic, N, rng, 0.05)
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * np.exp(0.2 * rng.standard_normal((N, 4)))
+    ode = goss.ParameterizedODE(name, field_parameters=list(fps))
+    systems = {}
+    for precision in ("double", "single"):
+        s = goss.solvers.solver_mapper[solver](ode)
+        s.internal_time_step = 0.01
+        systems[precision] = goss.ODESystemSolver(N, s, ode, precision=precision)
+        systems[precision].set_states(y0)
+        systems[precision].field_parameters = fp
+    o = pyoracle.OracleSystem(om, solver, N, ldt=0.01)
+    o.states[:] = y0
+    o.field_params[:] = fp
+    for k in range(10):
+        for s in systems.values():
+            s.forward(10.0 * k, 10.0)
+        o.forward(10.0 * k, 10.0)
+    assert parity(systems["double"].states, o.states, rtol=TOL64) <= 1.0
+    iv = md["state_names"].index("V")
+    v32, v = systems["single"].states[:, iv], o.states[:, iv]
+    assert np.max(np.abs(v32 - v) / np.abs(v)) < 1e-3
