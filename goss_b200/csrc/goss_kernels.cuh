@@ -596,29 +596,14 @@ enum ThetaRows { TH_ETA = 0, TH_RECOMPUTE, TH_ALWAYS, TH_JUSTREFINED, TH_JACCOMP
 // up to 256 threads; __launch_bounds__(256, 1) keeps the 255-register budget
 // (without the minimum of one block ptxas capped it at 128 and spilled more).
 //
-// The packed Newton matrix (TT04: 71 values, TP06: 82), the Newton update z1
-// and the explicit part prev live in dynamic shared memory, theta_smem_rows
-// * blockDim.x doubles (210 KB for TT04 in blocks of 256): in registers they
-// pushed the kernel past 255 registers and the spills reached DRAM (5.8x the
-// algorithmic write bytes of an interval).  Models whose rows do not fit for
-// 32 threads keep them in thread-local arrays.
-#ifndef GOSS_THETA_SMEM_VECTORS
-#define GOSS_THETA_SMEM_VECTORS 1
-#endif
-constexpr uint32_t kThetaSmemBytes = 232448;  // 227 KB, the opt-in maximum per block
-template <class M>
-__host__ __device__ constexpr uint32_t theta_smem_rows()
-{
-    return M::lu_nnz + (GOSS_THETA_SMEM_VECTORS ? 2 * M::num_states : 0);
-}
-template <class M>
-__host__ __device__ constexpr bool theta_matrix_in_smem()
-{
-    return (uint64_t)theta_smem_rows<M>() * sizeof(double) * 32 <= kThetaSmemBytes;
-}
-
 // Launch shape: at most GOSS_THETA_THREADS threads per block, compiled for
 // GOSS_THETA_MIN_BLOCKS resident blocks per SM (register cap 65536 / product).
+// Measured on B200 (TT04 with the analytic Jacobian, 262,144 nodes, 0.1 ms
+// intervals): 256 x 1 with the Newton matrix, z1 and prev in registers and
+// local memory 0.61 ms per interval; the same with them in dynamic shared
+// memory 0.77 ms (the DRAM spill traffic disappears, but the shared memory
+// takes the L1 capacity the remaining spills hit in); the matrix alone in
+// shared memory 0.79 ms, and in blocks of 128 x 3 (168 registers) 0.92 ms.
 #ifndef GOSS_THETA_THREADS
 #define GOSS_THETA_THREADS 256
 #endif
@@ -634,30 +619,8 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
     const bool active = node < a.N;
     const uint32_t src = active ? node : a.N - 1;  // threads past the end only take part in the barriers
     const goss_solver_params& sp = a.sp;
-    double y[n], yz[n], f1[n], b[n];
-    extern __shared__ double theta_smem[];
-    constexpr bool in_smem = theta_matrix_in_smem<M>();
-    constexpr bool vec_smem = in_smem && GOSS_THETA_SMEM_VECTORS;
-    double Jlocal[in_smem ? 1 : M::lu_nnz], z1_local[vec_smem ? 1 : n], prev_local[vec_smem ? 1 : n];
-    const auto J = [&]() {
-        if constexpr (in_smem)
-            return PackedShared{theta_smem + threadIdx.x, blockDim.x};
-        else
-            return static_cast<double*>(Jlocal);
-    }();
-    const auto z1 = [&]() {
-        if constexpr (vec_smem)
-            return PackedShared{theta_smem + (uint32_t)M::lu_nnz * blockDim.x + threadIdx.x, blockDim.x};
-        else
-            return static_cast<double*>(z1_local);
-    }();
-    const auto prev = [&]() {
-        if constexpr (vec_smem)
-            return PackedShared{theta_smem + (uint32_t)(M::lu_nnz + n) * blockDim.x + threadIdx.x, blockDim.x};
-        else
-            return static_cast<double*>(prev_local);
-    }();
-#pragma unroll
+    double y[n], z1[n], prev[n], yz[n], f1[n], b[n];
+    double J[M::lu_nnz];
     for (int i = 0; i < n; ++i)
         y[i] = a.states[i * a.ld + src];
     double F[Dims<M>::nfp];
@@ -684,7 +647,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
     int num_refinements = 0;
     const double eps = kGossEps * 1000;
     uint8_t status = 0;
-#pragma unroll
     for (int i = 0; i < n; ++i)
         prev[i] = 0.0;
     uint64_t guard = 0;
@@ -703,7 +665,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
                 done = true;
                 continue;
             }
-#pragma unroll
             for (int i = 0; i < n; ++i)
                 z1[i] = 0.0;
             if (IE ? num_refinements > sp.num_refinements_without_always_recomputing_jacobian
@@ -722,7 +683,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
                     prev_pending = true;
                 } else {
                     rhs64<M>(y, t, a.P, F, f1);
-#pragma unroll
                     for (int i = 0; i < n; ++i)
                         prev[i] = (1 - sp.theta) * f1[i];
                 }
@@ -731,7 +691,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
         }
         // one iteration of ImplicitODESolver::newton_solve (ImplicitODESolver.cpp:114-245)
         bool newton_done = false;
-#pragma unroll
         for (int i = 0; i < n; ++i)
             yz[i] = y[i] + z1[i];
         // when this iteration will refactorise (both conditions are known
@@ -747,7 +706,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
                     M::fd_clear(J);
                     M::template rhs2_fd_jacobian<double>(yz, tn, a.P, a.P, F, t, b, f1, J);
                 }
-#pragma unroll
                 for (int i = 0; i < n; ++i)
                     prev[i] = (1 - sp.theta) * b[i];
                 prev_pending = false;
@@ -760,7 +718,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
         } else {
             rhs64<M>(yz, tn, a.P, F, f1);
         }
-#pragma unroll
         for (int i = 0; i < n; ++i)
             b[i] = -z1[i] * 1.0 + ldt * (prev[i] + alpha * f1[i]);
         residual = l2norm<n>(b);
@@ -803,7 +760,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
                 newton_done = true;
             }
             if (!newton_done) {
-#pragma unroll
                 for (int i = 0; i < n; ++i)
                     z1[i] += b[i];
                 relative_residual = residual / initial_residual;
@@ -816,7 +772,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
             continue;
         in_step = false;
         if (step_ok) {
-#pragma unroll
             for (int i = 0; i < n; ++i)
                 y[i] += z1[i];
             t += ldt;
@@ -852,7 +807,6 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
     if (!active)
         return;
     bool finite = true;
-#pragma unroll
     for (int i = 0; i < n; ++i) {
         a.states[i * a.ld + node] = y[i];
         finite = finite && isfinite(y[i]);
@@ -1298,24 +1252,16 @@ inline int launch_implicit(const goss_launch* L)
     // ThetaSolver / ImplicitEuler: lockstep blocks of 256 (kernel limit 256);
     // ESDIRK23a: 64 (limit 128)
     const bool theta = L->solver == GOSS_THETA || L->solver == GOSS_IMPLICIT_EULER;
-    unsigned block = L->block ? L->block : (theta ? GOSS_THETA_THREADS : 64);
+    const unsigned block = L->block ? L->block : (theta ? GOSS_THETA_THREADS : 64);
     if (block > (theta ? (unsigned)GOSS_THETA_THREADS : 128u))
         return GOSS_ERR_ARGUMENT;
-    if (theta && theta_matrix_in_smem<M>()) {
-        // as many threads as the block's shared rows leave room for
-        const unsigned fit = kThetaSmemBytes / (unsigned)(sizeof(double) * theta_smem_rows<M>()) / 32u * 32u;
-        block = block < fit ? block : fit;
-    }
     const unsigned grid = (L->num_nodes + block - 1) / block;
     if (grid == 0)
         return 0;
-    if (theta) {
-        // the block's shared rows in dynamic shared memory
-        const size_t smem = theta_matrix_in_smem<M>() ? sizeof(double) * (size_t)theta_smem_rows<M>() * block : 0;
-        auto kernel = L->solver == GOSS_THETA ? theta_kernel<M, false> : theta_kernel<M, true>;
-        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return GOSS_ERR_CUDA;
-        kernel<<<grid, block, smem, (cudaStream_t)L->stream>>>(a);
+    if (L->solver == GOSS_THETA) {
+        theta_kernel<M, false><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
+    } else if (L->solver == GOSS_IMPLICIT_EULER) {
+        theta_kernel<M, true><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
     } else {
         const size_t smem = GOSS_ESDIRK_SMEM ? sizeof(double) * 5 * (size_t)M::num_states * block : 0;
         if (smem > 48 * 1024 &&

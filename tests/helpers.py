@@ -72,6 +72,24 @@ def parity(a, b, rtol=1e-10, atol=1e-12):
     return float(np.max(np.abs(a[m] - b[m]) / (atol + rtol * np.abs(b[m])))) if m.any() else 0.0
 
 
+def parity_scaled(a, b, rtol=1e-10, atol=1e-12, floor=0.01):
+    """parity() with each state's magnitude floored at `floor` times that
+    state's largest magnitude over the compared rows: |a-b| / (atol + rtol *
+    max(|b|, floor * max|b[:, i]|)).  For states that pass through zero (the
+    membrane potential during an upstroke), where a relative error compares
+    rounding with a value that happens to be near 0."""
+    a = np.atleast_2d(np.asarray(a))
+    b = np.atleast_2d(np.asarray(b))
+    if not a.size:
+        return 0.0
+    if not (np.isfinite(a) == np.isfinite(b)).all():
+        return float("inf")
+    scale = floor * np.nanmax(np.abs(np.where(np.isfinite(b), b, np.nan)), axis=0, keepdims=True)
+    den = atol + rtol * np.maximum(np.abs(b), scale)
+    m = np.isfinite(b)
+    return float(np.max(np.abs(a[m] - b[m]) / den[m])) if m.any() else 0.0
+
+
 def oracle_state_traces(name, field_parameters, fp, y0, interval, steps_per_interval, num_intervals, state_index,
                         t0=0.0, solver="GRL1"):
     """Oracle (reference semantics) traces [J, nodes] of one state: the loop
