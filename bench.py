@@ -652,6 +652,13 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
     tape32 = (tr32.taped_segments, tape_bytes(tr32))
     del tr32
     torch.cuda.empty_cache()
+    # the FP32 trajectory differentiated with FP64 step VJPs: splits the FP32
+    # gradient's error into the trajectory's share and the reverse arithmetic's
+    tr32m = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="single",
+                      tape_bytes="auto", reverse_precision="double")
+    g32m, _, bwd32m, _ = grad(tr32m)
+    del tr32m
+    torch.cuda.empty_cache()
     # every segment recomputed from its checkpoint (no tape)
     tr32r = GRL1Trace(ode, nodes, interval, steps_per_interval, num_intervals, checkpoint_every, precision="single")
     g32r, fwd32r, bwd32r, _ = grad(tr32r)
@@ -680,6 +687,8 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
 
     den = np.maximum(np.abs(g64).max(axis=0), 1e-300)
     col_err = np.abs(g32 - g64).max(axis=0) / den
+    traj_err = np.abs(g32m - g64).max(axis=0) / den    # FP32 trajectory, FP64 VJPs vs all FP64
+    rev_err = np.abs(g32 - g32m).max(axis=0) / den     # FP32 VJPs vs FP64 VJPs, same trajectory
     elem = np.abs(g32 - g64) / np.maximum(np.abs(g64), 1e-12 * den)
     return {
         "workload": f"TP06 GRL1 dt=0.01ms, {nodes} nodes, {num_intervals} ms ({num_intervals * steps_per_interval} "
@@ -700,7 +709,14 @@ def run_adjoint(dev, nodes=65_536, num_intervals=400, steps_per_interval=100, ch
         "checkpoint_bytes_fp32": int(cp_bytes),
         "grad_rel_err_fp32_vs_fp64": {"per_field_scaled_max": {f: float(e) for f, e in zip(FIELDS, col_err)},
                                       "elementwise_median": float(np.median(elem)),
-                                      "elementwise_p99": float(np.quantile(elem, 0.99))},
+                                      "elementwise_p99": float(np.quantile(elem, 0.99)),
+                                      "split": {
+                                          "trajectory_part": {f: float(e) for f, e in zip(FIELDS, traj_err)},
+                                          "reverse_arithmetic_part": {f: float(e) for f, e in zip(FIELDS, rev_err)},
+                                          "how": "trajectory part: FP32 record + FP64 step VJPs vs the FP64 "
+                                                 "adjoint; reverse part: FP32 adjoint vs FP32 record + FP64 "
+                                                 "step VJPs (field-scaled max)",
+                                          "fp64_vjp_backward_ms": bwd32m}},
     }
 
 

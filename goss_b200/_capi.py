@@ -12,7 +12,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 RUNTIME_SO = PKG / "_lib" / "libgoss_b200.so"
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 (GOSS_EXPLICIT_EULER, GOSS_RK4, GOSS_GRL1, GOSS_GRL2, GOSS_THETA, GOSS_ESDIRK23A, GOSS_RL1, GOSS_RL2, GOSS_RK2,
  GOSS_IMPLICIT_EULER) = range(10)
@@ -116,6 +116,7 @@ class AdjointLaunch(C.Structure):
         ("stream", C.c_void_p),
         ("tape", C.c_void_p),
         ("taped_segments", C.c_uint32),
+        ("reverse_precision", C.c_int32),
     ]
 
 

@@ -59,7 +59,7 @@ class SolverTrace:
     def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
                  num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
                  t0: float = 0.0, device: int = 0, solver: str = "GRL1", tape_bytes=0,
-                 tape_reserve: int = 2 << 30):
+                 tape_reserve: int = 2 << 30, reverse_precision: Optional[str] = None):
         import torch
 
         if solver not in self.SOLVERS:
@@ -80,6 +80,13 @@ class SolverTrace:
         self.t0 = float(t0)
         self.trace_index = ode.state_names.index(trace_state)
         self.precision = _capi.GOSS_FP32 if precision in ("single", "float32", "fp32") else _capi.GOSS_FP64
+        # arithmetic of the backward's step VJPs: the trajectory's, or "double"
+        # over an FP32 trajectory (GRL1)
+        self.reverse_precision = self.precision if reverse_precision is None else (
+            _capi.GOSS_FP32 if reverse_precision in ("single", "float32", "fp32") else _capi.GOSS_FP64)
+        if self.reverse_precision != self.precision and not (
+                self.precision == _capi.GOSS_FP32 and self.reverse_precision == _capi.GOSS_FP64 and solver == "GRL1"):
+            raise ValueError("reverse_precision differs from precision only as FP64 over an FP32 GRL1 trajectory")
         self.device = torch.device("cuda", device)
         self.ld = _ld(self.N)
         total = self.J * self.S
@@ -137,6 +144,7 @@ class SolverTrace:
         L.flags = self._flags.data_ptr()
         L.tape = self._tape.data_ptr() if self._tape is not None else None
         L.taped_segments = self.taped_segments
+        L.reverse_precision = self.reverse_precision
         L.stream = torch.cuda.current_stream(self.device).cuda_stream
         rc = self._fn(C.byref(L))
         _capi.check(rc)
@@ -175,14 +183,18 @@ class SolverTrace:
 
 
 class GRL1Trace(SolverTrace):
-    """:class:`SolverTrace` of the GRL1 solver."""
+    """:class:`SolverTrace` of the GRL1 solver.  ``reverse_precision="double"``
+    with ``precision="single"`` differentiates the FP32 trajectory with FP64
+    step VJPs (separates the FP32 trajectory's share of the gradient error
+    from the FP32 reverse arithmetic's)."""
 
     def __init__(self, ode: ParameterizedODE, num_nodes: int, interval: float, steps_per_interval: int,
                  num_intervals: int, checkpoint_every: int, trace_state: str = "V", precision: str = "single",
-                 t0: float = 0.0, device: int = 0, tape_bytes=0, tape_reserve: int = 2 << 30):
+                 t0: float = 0.0, device: int = 0, tape_bytes=0, tape_reserve: int = 2 << 30,
+                 reverse_precision: Optional[str] = None):
         super().__init__(ode, num_nodes, interval, steps_per_interval, num_intervals, checkpoint_every,
                          trace_state, precision, t0, device, solver="GRL1", tape_bytes=tape_bytes,
-                         tape_reserve=tape_reserve)
+                         tape_reserve=tape_reserve, reverse_precision=reverse_precision)
 
 
 class RK4Trace(SolverTrace):

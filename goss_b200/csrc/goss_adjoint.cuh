@@ -45,6 +45,7 @@
 //         the record's tape (65,536 nodes x 40,000 steps, 368 of 400
 //         segments taped) 2, 3, 4 blocks: 445, 650, 716 ms;
 //   FP64: 256 x 1: 207 ms; 128 x 2: 215 ms.
+// (the shape of the backward follows the arithmetic of its VJPs)
 template <typename T>
 struct AdjointShape {
     static constexpr unsigned block = sizeof(T) == 4 ? 128 : 256;
@@ -309,12 +310,16 @@ __device__ __forceinline__ void reverse_step_rk4(const T* yt, double lt, double 
         lam[i].add(ysum[i]);
 }
 
-template <class M, typename T, Explicit S>
-__global__ void __launch_bounds__(AdjointShape<T>::block, AdjointShape<T>::min_blocks)
+// R is the arithmetic of the step VJPs and of lambda: T, or double over an
+// FP32 trajectory (the recompute keeps T, so the same trajectory is
+// differentiated; only the VJP arithmetic changes).
+template <class M, typename T, Explicit S, typename R = T>
+__global__ void __launch_bounds__(AdjointShape<R>::block, AdjointShape<R>::min_blocks)
 adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
 {
     constexpr int n = M::num_states;
     constexpr int nfp = Dims<M>::nfp;
+    static_assert(sizeof(R) >= sizeof(T), "the VJP arithmetic is at least the trajectory's");
     // Every thread runs every loop (block-wide barriers below); threads past
     // the last node shadow it (reads only) and keep their own scratch column.
     const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
@@ -325,7 +330,14 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
     const double ldt = a.interval / S_;
     T F[nfp];
     load_field<M, T>(a.fparams, a.ld, src, F);
-    Acc<T> lam[n];
+    R FR[nfp];
+    load_field<M, R>(a.fparams, a.ld, src, FR);
+    const R* PR;
+    if constexpr (sizeof(R) == sizeof(T))
+        PR = reinterpret_cast<const R*>(a.P);
+    else
+        PR = a.PD;
+    Acc<R> lam[n];
     for (int i = 0; i < n; ++i)
         lam[i].load(0.0);
     double gF[nfp];
@@ -376,15 +388,15 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
             const uint64_t g = g0 + k;  // step g maps state g to state g+1
             if ((g + 1) % S_ == 0) {
                 const uint64_t j = (g + 1) / S_ - 1;
-                lam[a.trace_state].add(T(a.trace_bar[j * a.ld + src]));
+                lam[a.trace_state].add(R(a.trace_bar[j * a.ld + src]));
             }
-            T yt[n];
+            R yt[n];
             for (int i = 0; i < n; ++i)
-                yt[i] = seg[((uint64_t)k * n + i) * a.sld];
+                yt[i] = R(seg[((uint64_t)k * n + i) * a.sld]);
             if constexpr (S == Explicit::GRL1)
-                reverse_step_grl1<M, T>(yt, s_time[k], ldt, a.P, a.PD, F, lam, gF);
+                reverse_step_grl1<M, R>(yt, s_time[k], ldt, PR, a.PD, FR, lam, gF);
             else
-                reverse_step_rk4<M, T>(yt, s_time[k], ldt, a.P, a.PD, F, lam, gF);
+                reverse_step_rk4<M, R>(yt, s_time[k], ldt, PR, a.PD, FR, lam, gF);
 #if GOSS_ADJOINT_LOCKSTEP
             __syncthreads();
 #endif
@@ -405,18 +417,18 @@ adjoint_kernel(const __grid_constant__ AdjointArgs<M, T> a)
 // the larger block) -- e.g. for 65,536 nodes on 148 SMs with two blocks per
 // SM: 112 threads (two nearly full waves) instead of 128 (a second wave on
 // 108 of 148 SMs).
-template <class M, typename T, Explicit S>
+template <class M, typename T, Explicit S, typename R = T>
 inline unsigned adjoint_block(uint32_t num_nodes, size_t shm)
 {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
-        return AdjointShape<T>::block;
-    unsigned best = AdjointShape<T>::block;
+        return AdjointShape<R>::block;
+    unsigned best = AdjointShape<R>::block;
     uint64_t best_cost = ~0ull;
-    for (unsigned b = AdjointShape<T>::block; b >= 32; b -= 32) {
+    for (unsigned b = AdjointShape<R>::block; b >= 32; b -= 32) {
         int active = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&active, adjoint_kernel<M, T, S>, (int)b, shm) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&active, adjoint_kernel<M, T, S, R>, (int)b, shm) !=
                 cudaSuccess || active <= 0)
             continue;
         const uint64_t grid = (num_nodes + b - 1) / b;
@@ -431,7 +443,7 @@ inline unsigned adjoint_block(uint32_t num_nodes, size_t shm)
     return best;
 }
 
-template <class M, typename T, Explicit S>
+template <class M, typename T, Explicit S, typename R = T>
 inline int launch_adjoint_t(const goss_adjoint_launch* L)
 {
     AdjointArgs<M, T> a;
@@ -478,11 +490,11 @@ inline int launch_adjoint_t(const goss_adjoint_launch* L)
         const size_t shm = sizeof(double) * a.checkpoint_every;
         if (shm > 48 * 1024)
             return GOSS_ERR_ARGUMENT;
-        const unsigned block = L->block ? L->block : adjoint_block<M, T, S>(L->num_nodes, shm);
-        if (block == 0 || block > AdjointShape<T>::block || block % 32)
+        const unsigned block = L->block ? L->block : adjoint_block<M, T, S, R>(L->num_nodes, shm);
+        if (block == 0 || block > AdjointShape<R>::block || block % 32)
             return GOSS_ERR_ARGUMENT;
         const unsigned grid = (L->num_nodes + block - 1) / block;
-        adjoint_kernel<M, T, S><<<grid, block, shm, (cudaStream_t)L->stream>>>(a);
+        adjoint_kernel<M, T, S, R><<<grid, block, shm, (cudaStream_t)L->stream>>>(a);
     }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
 }
@@ -491,8 +503,13 @@ template <class M>
 inline int launch_adjoint(const goss_adjoint_launch* L)
 {
     const bool f32 = L->precision == GOSS_FP32;
+    const bool rev64 = L->reverse_precision == GOSS_FP64;
+    if (!(L->reverse_precision == L->precision || (f32 && rev64 && L->solver == GOSS_GRL1)))
+        return GOSS_ERR_UNSUPPORTED;
     switch (L->solver) {
     case GOSS_GRL1:
+        if (f32 && rev64)
+            return launch_adjoint_t<M, float, Explicit::GRL1, double>(L);
         return f32 ? launch_adjoint_t<M, float, Explicit::GRL1>(L) : launch_adjoint_t<M, double, Explicit::GRL1>(L);
     case GOSS_RK4:
         return f32 ? launch_adjoint_t<M, float, Explicit::RK4>(L) : launch_adjoint_t<M, double, Explicit::RK4>(L);

@@ -35,7 +35,7 @@ extern "C" {
 #define GOSS_API
 #endif
 
-#define GOSS_B200_ABI_VERSION 3u
+#define GOSS_B200_ABI_VERSION 4u
 
 /* Solver kinds: the reference solver classes on this path. */
 enum goss_solver_kind {
@@ -178,6 +178,11 @@ typedef struct goss_adjoint_launch {
     void* stream;
     void* tape;
     uint32_t taped_segments;  /* <= C */
+    int32_t reverse_precision; /* arithmetic of the backward's step VJPs: the
+                                  record's precision, or GOSS_FP64 with precision
+                                  GOSS_FP32 (GRL1): the FP32 trajectory (its
+                                  checkpoints, tape and recomputed steps)
+                                  differentiated in FP64 */
 } goss_adjoint_launch;
 
 /* A compiled model: produced by the code generator for one .ode model and one

@@ -233,3 +233,22 @@ def test_tape_size_arguments():
     assert SolverTrace(ode, 24, INTERVAL, S, J, 400, tape_bytes="auto").taped_segments == 4
     with pytest.raises(TypeError):
         SolverTrace(ode, 24, INTERVAL, S, J, 400, tape_bytes=1.5)
+
+
+def test_fp64_reverse_over_fp32_trajectory():
+    """reverse_precision="double" over an FP32 record: the FP32 trajectory
+    differentiated with FP64 step VJPs.  Its gradient sits between the FP32
+    and the FP64 adjoints: against the FP64 adjoint it carries only the FP32
+    trajectory's difference, against the FP32 adjoint only the FP32 reverse
+    arithmetic's; each is bounded like the FP32 gradient's total error."""
+    ode, tr64, fp, y0, target = setup("double")
+    _, g64, _ = loss_grad(tr64, fp, y0, target)
+    tr32 = GRL1Trace(ode, N, INTERVAL, S, J, 400, precision="single")
+    _, g32, _ = loss_grad(tr32, fp, y0, target)
+    trm = GRL1Trace(ode, N, INTERVAL, S, J, 400, precision="single", reverse_precision="double")
+    _, gm, _ = loss_grad(trm, fp, y0, target)
+    assert np.isfinite(gm).all()
+    total = column_rel_err(g32, g64)
+    assert column_rel_err(gm, g64) < 1e-3 and column_rel_err(g32, gm) < 1e-3, total
+    with pytest.raises(ValueError):
+        GRL1Trace(ode, N, INTERVAL, S, J, 400, precision="double", reverse_precision="single")
