@@ -89,6 +89,7 @@ struct ImplicitArgs {
     goss_solver_params sp;
     uint32_t N;
     double P[Dims<M>::np];
+    float P32[Dims<M>::np];  // the same block in FP32 (the FP32 Jacobian of GOSS_FP32)
 };
 
 template <class M, typename T>
@@ -525,6 +526,26 @@ __device__ __forceinline__ void jacobian64(const double* y, double t, const doub
     M::template jacobian<double>(y, t, P, P, F, J);
 }
 
+// The analytic Jacobian evaluated in FP32 at the FP64 point (y, t) and stored
+// into the FP64 packed Newton matrix: the implicit solvers' GOSS_FP32 mode.
+// The matrix only steers the simplified Newton iteration (the residual, the
+// right-hand sides, the LU and the updates stay FP64), so the iteration
+// converges to the same tolerance with an FP32-accurate matrix.
+template <class M, class A>
+__device__ __forceinline__ void jacobian32(const double* y, double t, const float* P32, const double* PD,
+                                           const double* F, A J)
+{
+    float yf[M::num_states];
+#pragma unroll
+    for (int i = 0; i < M::num_states; ++i)
+        yf[i] = float(y[i]);
+    float Ff[Dims<M>::nfp];
+#pragma unroll
+    for (int k = 0; k < Dims<M>::nfp; ++k)
+        Ff[k] = float(F[k]);
+    M::template jacobian<float>(yf, t, P32, PD, Ff, J);
+}
+
 // ODE::compute_jacobian (ODE.cpp:47-67) into the packed Newton matrix J:
 // the model's analytic Jacobian when it was generated with one (the
 // reference's generated override), else forward differences: column i is
@@ -610,7 +631,7 @@ enum ThetaRows { TH_ETA = 0, TH_RECOMPUTE, TH_ALWAYS, TH_JUSTREFINED, TH_JACCOMP
 #ifndef GOSS_THETA_MIN_BLOCKS
 #define GOSS_THETA_MIN_BLOCKS 1
 #endif
-template <class M, bool IE>
+template <class M, bool IE, bool J32 = false>
 __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
     theta_kernel(const __grid_constant__ ImplicitArgs<M> a)
 {
@@ -699,7 +720,17 @@ __global__ void __launch_bounds__(GOSS_THETA_THREADS, GOSS_THETA_MIN_BLOCKS)
         // or the statements the analytic Jacobian shares with f
         constexpr bool fused = GOSS_IMPLICIT_SPLIT;
         if (fused && !(relative_residual < sp.relative_tolerance) && (recompute || always)) {
-            if (!IE && prev_pending) {  // first iteration of the step: yz = y; f(y, t) into b
+            if constexpr (J32) {
+                // FP64 right-hand sides, the FP32 Jacobian
+                if (!IE && prev_pending) {
+                    rhs64<M>(yz, t, a.P, F, b);
+                    for (int i = 0; i < n; ++i)
+                        prev[i] = (1 - sp.theta) * b[i];
+                    prev_pending = false;
+                }
+                rhs64<M>(yz, tn, a.P, F, f1);
+                jacobian32<M>(yz, tn, a.P32, a.P, F, J);
+            } else if (!IE && prev_pending) {  // first iteration of the step: yz = y; f(y, t) into b
                 if constexpr (M::has_jacobian) {
                     M::template rhs2_jacobian<double>(yz, tn, a.P, a.P, F, t, b, f1, J);
                 } else {
@@ -891,7 +922,7 @@ struct LocalVec {
 #define GOSS_ESDIRK_SMEM 0
 #endif
 
-template <class M, class V>
+template <class M, class V, bool J32 = false>
 struct EsdirkNode {
     static constexpr int n = M::num_states;
     const double* P;
@@ -905,10 +936,14 @@ struct EsdirkNode {
     V z1, z2, z3, z4, prev;
 
     // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
+    const float* P32;
     __device__ void ode_jacobian(double* y, double t)
     {
         double g1[n];  // f(y), a by-product of the fused evaluations
-        if constexpr (M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
+        if constexpr (J32) {
+            (void)g1;
+            jacobian32<M>(y, t, P32, P, F, jac);
+        } else if constexpr (M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
             // f(y) and the analytic Jacobian sharing their statements
             M::template rhs_jacobian<double>(y, t, P, P, F, g1, jac);
         } else if constexpr (GOSS_IMPLICIT_SPLIT) {
@@ -1049,7 +1084,7 @@ struct EsdirkNode {
     }
 };
 
-template <class M>
+template <class M, bool J32 = false>
 __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ ImplicitArgs<M> a)
 {
     constexpr int n = M::num_states;
@@ -1065,7 +1100,7 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
     double* ss = a.sstate + node;
 #if GOSS_ESDIRK_SMEM
     extern __shared__ double esdirk_smem[];
-    EsdirkNode<M, PackedShared> s;
+    EsdirkNode<M, PackedShared, J32> s;
     {
         double* base = esdirk_smem + threadIdx.x;
         const uint32_t rows = (uint32_t)n * blockDim.x;
@@ -1076,9 +1111,10 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
         s.prev = PackedShared{base + 4 * rows, blockDim.x};
     }
 #else
-    EsdirkNode<M, LocalVec<n>> s;
+    EsdirkNode<M, LocalVec<n>, J32> s;
 #endif
     s.P = a.P;
+    s.P32 = a.P32;
     s.F = F;
     s.sp = &a.sp;
     s.c = esdirk_coefficients();
@@ -1249,6 +1285,12 @@ inline int launch_implicit(const goss_launch* L)
     a.sp = *L->solver_params;
     a.max_loop = L->max_loop ? L->max_loop : (1ull << 24);
     parameter_block<M>(L->params, a.P);
+    for (int i = 0; i < Dims<M>::np; ++i)
+        a.P32[i] = float(a.P[i]);
+    // GOSS_FP32: the analytic Jacobian in FP32 (models generated with it)
+    const bool j32 = L->precision == GOSS_FP32;
+    if (j32 && !M::has_jacobian)
+        return GOSS_ERR_UNSUPPORTED;
     // ThetaSolver / ImplicitEuler: lockstep blocks of 256 (kernel limit 256);
     // ESDIRK23a: 64 (limit 128)
     const bool theta = L->solver == GOSS_THETA || L->solver == GOSS_IMPLICIT_EULER;
@@ -1258,17 +1300,28 @@ inline int launch_implicit(const goss_launch* L)
     const unsigned grid = (L->num_nodes + block - 1) / block;
     if (grid == 0)
         return 0;
-    if (L->solver == GOSS_THETA) {
-        theta_kernel<M, false><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
-    } else if (L->solver == GOSS_IMPLICIT_EULER) {
-        theta_kernel<M, true><<<grid, block, 0, (cudaStream_t)L->stream>>>(a);
-    } else {
-        const size_t smem = GOSS_ESDIRK_SMEM ? sizeof(double) * 5 * (size_t)M::num_states * block : 0;
-        if (smem > 48 * 1024 &&
-            cudaFuncSetAttribute(esdirk_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                cudaSuccess)
+    const cudaStream_t st = (cudaStream_t)L->stream;
+    const size_t esmem = GOSS_ESDIRK_SMEM ? sizeof(double) * 5 * (size_t)M::num_states * block : 0;
+    if (L->solver == GOSS_ESDIRK23A && esmem > 48 * 1024) {
+        auto k = j32 ? esdirk_kernel<M, M::has_jacobian> : esdirk_kernel<M, false>;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem) != cudaSuccess)
             return GOSS_ERR_CUDA;
-        esdirk_kernel<M><<<grid, block, smem, (cudaStream_t)L->stream>>>(a);
+    }
+    if (j32) {
+        if constexpr (M::has_jacobian) {
+            if (L->solver == GOSS_THETA)
+                theta_kernel<M, false, true><<<grid, block, 0, st>>>(a);
+            else if (L->solver == GOSS_IMPLICIT_EULER)
+                theta_kernel<M, true, true><<<grid, block, 0, st>>>(a);
+            else
+                esdirk_kernel<M, true><<<grid, block, esmem, st>>>(a);
+        }
+    } else if (L->solver == GOSS_THETA) {
+        theta_kernel<M, false><<<grid, block, 0, st>>>(a);
+    } else if (L->solver == GOSS_IMPLICIT_EULER) {
+        theta_kernel<M, true><<<grid, block, 0, st>>>(a);
+    } else {
+        esdirk_kernel<M><<<grid, block, esmem, st>>>(a);
     }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
 }
@@ -1297,8 +1350,6 @@ inline int launch_solver(const goss_launch* L)
     case GOSS_THETA:
     case GOSS_ESDIRK23A:
     case GOSS_IMPLICIT_EULER:
-        if (f32)
-            return GOSS_ERR_UNSUPPORTED;
         return launch_implicit<M>(L);
     default:
         return GOSS_ERR_ARGUMENT;

@@ -488,9 +488,12 @@ GOSS_API int goss_system_create(const goss_model_desc* m, int32_t solver, const 
         return fail(nullptr, GOSS_ERR_UNSUPPORTED, "solver kind %d is not available for model %s", solver, m->name);
     if (precision != GOSS_FP64 && precision != GOSS_FP32 && precision != GOSS_FP64_PRINTED)
         return fail(nullptr, GOSS_ERR_ARGUMENT, "invalid precision %d", precision);
-    if ((solver == GOSS_THETA || solver == GOSS_ESDIRK23A || solver == GOSS_IMPLICIT_EULER) && precision == GOSS_FP32)
+    if ((solver == GOSS_THETA || solver == GOSS_ESDIRK23A || solver == GOSS_IMPLICIT_EULER) && precision == GOSS_FP32 &&
+        !m->has_jacobian)
         return fail(nullptr, GOSS_ERR_UNSUPPORTED,
-                    "implicit solvers run their Newton iteration in FP64; use GOSS_FP64 precision");
+                    "implicit solvers in GOSS_FP32 evaluate the analytic Jacobian in FP32 (the residuals, LU and "
+                    "updates stay FP64) and need a model generated with it (code_params generate_jacobian); "
+                    "use GOSS_FP64 for model %s", m->name);
     if (precision == GOSS_FP64_PRINTED && solver != GOSS_GRL1)
         return fail(nullptr, GOSS_ERR_UNSUPPORTED, "GOSS_FP64_PRINTED is available for GRL1 only");
     auto* s = new goss_system();

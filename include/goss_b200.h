@@ -54,7 +54,10 @@ enum goss_solver_kind {
 
 /* Arithmetic of the right-hand side.  States are always stored and
  * accumulated in FP64; GOSS_FP32 evaluates the model and the explicit
- * update in FP32 (implicit solvers keep Newton and LU in FP64).  GOSS_FP64
+ * update in FP32.  The implicit solvers (ThetaSolver, ImplicitEuler,
+ * ESDIRK23a) in GOSS_FP32 evaluate only the Newton matrix's Jacobian in FP32,
+ * from the model's analytic Jacobian (models generated with it); right-hand
+ * sides, residuals, LU and updates stay FP64.  GOSS_FP64
  * evaluates the model's split program (every distinct exponential and
  * reciprocal once); GOSS_FP64_PRINTED evaluates it in the printed operation
  * order of the reference's generated model code (GRL1 only: the plain FP64
