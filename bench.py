@@ -449,7 +449,9 @@ def run_accuracy(dev, ms_total=ACCURACY_MS):
     unfloored relative error divides rounding by ~0), and the plain relative
     error |gpu - ref| / max(|ref|, 1e-12) at the end; for FP64 also the parity
     ratio, the worst error over 1e-12 + 1e-10 max(|ref|, 0.01 s) (<= 1: within
-    1e-10)."""
+    1e-10), over the run and at the end (1e-12 + 1e-10 |ref|).  GRL1 also runs
+    in the printed operation order (GOSS_FP64_PRINTED, "fp64_printed"), to
+    show what the split FP64 program changes."""
     import threading
 
     import torch
@@ -495,20 +497,20 @@ def run_accuracy(dev, ms_total=ACCURACY_MS):
     ode = goss.ParameterizedODE(MODEL, field_parameters=FIELDS)
     gidx = torch.tensor(idx, device=torch.device("cuda", dev))
     gpu = {}
-    for solver in ("GRL1", "GRL2"):
-        for precision in ("double", "single"):
-            s = goss.solvers.solver_mapper[solver](ode)
-            s.internal_time_step = LDT
-            system = goss.ODESystemSolver(N_NODES, s, ode, precision=precision, device=dev)
-            system.set_states(y0)
-            system.field_parameters = fp
-            rows = _device_rows(system, n)
-            out = np.empty((ms_total, idx.size, n))
-            for k in range(ms_total):
-                system.forward(float(k), 1.0)
-                out[k] = rows.index_select(1, gidx).T.cpu().numpy()
-            gpu[(solver, precision)] = out
-            del rows, system
+    for solver, precision in (("GRL1", "double"), ("GRL1", "single"), ("GRL1", "double_printed"),
+                              ("GRL2", "double"), ("GRL2", "single")):
+        s = goss.solvers.solver_mapper[solver](ode)
+        s.internal_time_step = LDT
+        system = goss.ODESystemSolver(N_NODES, s, ode, precision=precision, device=dev)
+        system.set_states(y0)
+        system.field_parameters = fp
+        rows = _device_rows(system, n)
+        out = np.empty((ms_total, idx.size, n))
+        for k in range(ms_total):
+            system.forward(float(k), 1.0)
+            out[k] = rows.index_select(1, gidx).T.cpu().numpy()
+        gpu[(solver, precision)] = out
+        del rows, system
     cpu.join()
     wall = time.perf_counter() - w0
 
@@ -525,15 +527,18 @@ def run_accuracy(dev, ms_total=ACCURACY_MS):
         r = ref[solver]
         floor = 0.01 * np.abs(r).max(axis=(0, 1))  # per state
         entry = {}
-        for precision, key in (("double", "fp64"), ("single", "fp32")):
+        for precision, key in (("double", "fp64"), ("single", "fp32"), ("double_printed", "fp64_printed")):
+            if (solver, precision) not in gpu:
+                continue
             g = gpu[(solver, precision)]
             e_all = rel(g, r, floor).max(axis=(0, 1))
             e_end = rel(g[-1], r[-1]).max(axis=0)
             d = {"max_rel_err": float(e_all.max()), "v_max_rel_err": float(e_all[names.index("V")]),
                  "max_rel_err_end": float(e_end.max()), "v_max_rel_err_end": float(e_end[names.index("V")]),
                  "per_state": {nm: float(e) for nm, e in zip(names, e_all)}}
-            if key == "fp64":
+            if key != "fp32":
                 d["parity"] = float((np.abs(g - r) / (1e-12 + 1e-10 * np.maximum(np.abs(r), floor))).max())
+                d["parity_end"] = float((np.abs(g[-1] - r[-1]) / (1e-12 + 1e-10 * np.abs(r[-1]))).max())
             entry[key] = d
         res[solver] = entry
     return res

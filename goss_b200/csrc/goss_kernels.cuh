@@ -907,183 +907,18 @@ __device__ __forceinline__ EsdirkCoef esdirk_coefficients()
     return c;
 }
 
-// a node's vector of n values in thread-local storage
-template <int n>
-struct LocalVec {
-    double v[n];
-    __device__ __forceinline__ double& operator[](int i) { return v[i]; }
-};
-
-// ESDIRK23a's stage derivatives z1..z4 and the explicit part prev of a stage
-// (5 n values per node) are thread-local, or with GOSS_ESDIRK_SMEM in dynamic
-// shared memory (vector k of the block's thread t at rows [k n, (k+1) n),
-// PackedShared layout).
-#ifndef GOSS_ESDIRK_SMEM
-#define GOSS_ESDIRK_SMEM 0
-#endif
-
-template <class M, class V, bool J32 = false>
-struct EsdirkNode {
-    static constexpr int n = M::num_states;
-    const double* P;
-    const double* F;
-    const goss_solver_params* sp;
-    EsdirkCoef c;
-    PackedTile jac, jfac;
-    double prev_dt, loc_error, eta, dt;
-    int newton_iterations, first_step, new_jacobian;
-    double jac_comp, rejects, accepted;
-    V z1, z2, z3, z4, prev;
-
-    // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
-    const float* P32;
-    __device__ void ode_jacobian(double* y, double t)
-    {
-        double g1[n];  // f(y), a by-product of the fused evaluations
-        if constexpr (J32) {
-            (void)g1;
-            jacobian32<M>(y, t, P32, P, F, jac);
-        } else if constexpr (M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
-            // f(y) and the analytic Jacobian sharing their statements
-            M::template rhs_jacobian<double>(y, t, P, P, F, g1, jac);
-        } else if constexpr (GOSS_IMPLICIT_SPLIT) {
-            // f(y) and the forward differences from one evaluation of the
-            // unperturbed statements (TT04, 262,144 nodes: 214 -> 199 ms per
-            // interval against a separate f(y))
-            M::fd_clear(jac);
-            M::template rhs_fd_jacobian<double>(y, t, P, P, F, g1, jac);
-        } else {
-            rhs64<M>(y, t, P, F, g1);
-            compute_jacobian<M>(y, t, P, F, jac, g1);
-        }
-        jac_comp += 1;
-        new_jacobian = 1;
-    }
-    // ESDIRK23a::compute_factorized_jacobian(dt) (ESDIRK23a.cpp:101-115)
-    __device__ void factorize(double h)
-    {
-        M::lu_copy_shift(jac, jfac, -h * c.a22);
-        M::lu_factorize(jfac);
-    }
-    // ESDIRK23a::compute_stage_val (ESDIRK23a.cpp:201-258).  The reference keeps
-    // the previous Newton update (prev_dz) only for its norm; the norm is kept
-    // here (the same value: l2norm of the same vector), and the residual b is
-    // formed in place of f(y_int).
-    template <class Z>
-    __device__ bool stage(Z& z, const double* y, double t_s, double h)
-    {
-        newton_iterations = 0;
-        bool conv_ok = true;
-        double dz[n], dz_norm = 0.0;
-        eta = pow(std_max(eta, c.etamin), 0.8);
-        int guard = 0;
-        do {
-            double y_int[n], b[n];
-#pragma unroll
-            for (int i = 0; i < n; i++)
-                y_int[i] = y[i] + h * prev[i] + c.gamma * h * z[i];
-            rhs64<M>(y_int, t_s, P, F, b);
-#pragma unroll
-            for (int i = 0; i < n; i++)
-                b[i] = -z[i] + b[i];
-            const double prev_dz_norm = dz_norm;
-            M::lu_solve(jfac, b, dz);
-            dz_norm = l2norm<n>(dz);
-            if (newton_iterations >= 1) {
-                const double theta = dz_norm / prev_dz_norm;
-                if (!(theta <= 1)) {
-                    rejects += 1;
-                    conv_ok = false;
-                    break;
-                }
-                eta = theta / (1.0 - theta);
-            }
-            if (newton_iterations > sp->max_iterations || ++guard > 100000) {
-                rejects += 1;
-                conv_ok = false;
-                break;
-            }
-#pragma unroll
-            for (int i = 0; i < n; i++)
-                z[i] += dz[i];
-            newton_iterations++;
-        } while (eta * dz_norm > c.kappa * c.tol);
-        return conv_ok;
-    }
-    // ESDIRK23a::do_step (ESDIRK23a.cpp:134-199)
-    __device__ bool do_step(double* y, double t0, double h)
-    {
-        {
-            double f0[n];
-            rhs64<M>(y, t0, P, F, f0);
-#pragma unroll
-            for (int i = 0; i < n; i++) {
-                z1[i] = f0[i];
-                z2[i] = f0[i];
-                prev[i] = f0[i] * c.a21;
-            }
-        }
-        bool step_ok = stage(z2, y, t0 + c.c2 * h, h);
-        if (step_ok) {
-            for (int i = 0; i < n; i++) {
-                z3[i] = z2[i];
-                prev[i] = z1[i] * c.bh1 + z2[i] * c.bh2;
-            }
-            step_ok = stage(z3, y, t0 + c.c3 * h, h);
-        }
-        if (step_ok) {
-            for (int i = 0; i < n; i++) {
-                z4[i] = z3[i];
-                prev[i] = z1[i] * c.b1 + z2[i] * c.b2 + z3[i] * c.b3;
-            }
-            step_ok = stage(z4, y, t0 + c.c4 * h, h);
-        }
-        if (step_ok) {
-            double yh[n];
-#pragma unroll
-            for (int i = 0; i < n; i++)
-                yh[i] = h * ((c.b1 - c.bh1) * z1[i] + (c.b2 - c.bh2) * z2[i] + (c.b3 - c.gamma) * z3[i] +
-                             c.gamma * z4[i]);
-            M::lu_solve(jfac, yh, yh);
-            loc_error = l2norm<n>(yh);
-            if (loc_error > c.tol) {
-                rejects += 1;
-                step_ok = false;
-            } else {
-                for (int i = 0; i < n; i++)
-                    y[i] = y[i] + h * (c.b1 * z1[i] + c.b2 * z2[i] + c.b3 * z3[i] + c.gamma * z4[i]);
-                accepted += 1;
-            }
-        }
-        return step_ok;
-    }
-    // ESDIRK23a::reduce_time_step (ESDIRK23a.cpp:260-278)
-    __device__ void reduce(double& h)
-    {
-        double reduction_factor = 1.0, e = loc_error;
-        int guard = 0;
-        do {
-            reduction_factor *= 0.6;
-            e *= 0.1;
-        } while (e > c.tol && ++guard < 4096);
-        h = std_max(reduction_factor * h, sp->min_dt);
-    }
-    // ESDIRK23a::advance_one_step (ESDIRK23a.cpp:117-132)
-    __device__ void advance(double* y, double t0, double& h)
-    {
-        bool ok = do_step(y, t0, h);
-        int guard = 0;
-        while (!ok && h > sp->min_dt && ++guard < 4096) {
-            if (!new_jacobian)
-                ode_jacobian(y, t0);
-            reduce(h);
-            factorize(h);
-            ok = do_step(y, t0, h);
-        }
-        new_jacobian = 0;
-    }
-};
-
+// ESDIRK23a as one loop per node in which every pass evaluates the right-hand
+// side at most once and runs at most one substitution with the factorised
+// matrix, whatever phase of the method the node is in: the start of a step
+// attempt (f(y, t), the first stage), a Newton iteration of stage 2, 3 or 4,
+// or the error estimate.  The lanes of a warp drift apart in their Newton
+// iteration and step counts; in the nested form each lane then runs a
+// different inlined copy of the stage loop and the warp executes the copies
+// one after the other, here they share one copy of the model code.  The
+// Jacobian (at most once per pass) and the factorisation follow the same rule.
+// Per node the operations and their order are the nested form's
+// (ESDIRK23a::forward, advance_one_step, do_step, compute_stage_val,
+// reduce_time_step; ESDIRK23a.cpp:101-316).
 template <class M, bool J32 = false>
 __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ ImplicitArgs<M> a)
 {
@@ -1098,67 +933,221 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
     double F[Dims<M>::nfp];
     load_field<M, double>(a.fparams, ld, node, F);
     double* ss = a.sstate + node;
-#if GOSS_ESDIRK_SMEM
-    extern __shared__ double esdirk_smem[];
-    EsdirkNode<M, PackedShared, J32> s;
-    {
-        double* base = esdirk_smem + threadIdx.x;
-        const uint32_t rows = (uint32_t)n * blockDim.x;
-        s.z1 = PackedShared{base, blockDim.x};
-        s.z2 = PackedShared{base + rows, blockDim.x};
-        s.z3 = PackedShared{base + 2 * rows, blockDim.x};
-        s.z4 = PackedShared{base + 3 * rows, blockDim.x};
-        s.prev = PackedShared{base + 4 * rows, blockDim.x};
-    }
-#else
-    EsdirkNode<M, LocalVec<n>, J32> s;
-#endif
-    s.P = a.P;
-    s.P32 = a.P32;
-    s.F = F;
-    s.sp = &a.sp;
-    s.c = esdirk_coefficients();
-    s.jac = packed_tile(a.sstate + (uint64_t)ES_SCALARS * ld, node, M::lu_nnz);
-    s.jfac = packed_tile(a.sstate + (uint64_t)(ES_SCALARS + M::lu_nnz) * ld, node, M::lu_nnz);
-    s.prev_dt = ss[ES_PREV_DT * ld];
-    s.loc_error = ss[ES_LOC_ERROR * ld];
-    s.eta = ss[ES_ETA * ld];
-    s.newton_iterations = (int)ss[ES_NEWTON_IT * ld];
-    s.first_step = ss[ES_FIRST * ld] != 0.0;
-    s.new_jacobian = ss[ES_NEWJAC * ld] != 0.0;
-    s.jac_comp = ss[ES_JACCOMP * ld];
-    s.rejects = ss[ES_REJECTS * ld];
-    s.accepted = ss[ES_ACCEPTED * ld];
+    const EsdirkCoef c = esdirk_coefficients();
+    const goss_solver_params& sp = a.sp;
+    const PackedTile jac = packed_tile(a.sstate + (uint64_t)ES_SCALARS * ld, node, M::lu_nnz);
+    const PackedTile jfac = packed_tile(a.sstate + (uint64_t)(ES_SCALARS + M::lu_nnz) * ld, node, M::lu_nnz);
+    double prev_dt = ss[ES_PREV_DT * ld];
+    double loc_error = ss[ES_LOC_ERROR * ld];
+    double eta = ss[ES_ETA * ld];
+    int newton_iterations = (int)ss[ES_NEWTON_IT * ld];
+    int first_step = ss[ES_FIRST * ld] != 0.0;
+    int new_jacobian = ss[ES_NEWJAC * ld] != 0.0;
+    double jac_comp = ss[ES_JACCOMP * ld], rejects = ss[ES_REJECTS * ld], accepted = ss[ES_ACCEPTED * ld];
 
-    // ESDIRK23a::forward (ESDIRK23a.cpp:280-316)
+    // stage derivatives z1, z2, z3 and the current stage's z (z2, z3 or z4)
+    double z1[n], z2[n], z3[n], z[n], prev[n];
+    enum { PH_BEGIN = 0, PH_NEWTON = 1, PH_ERROR = 2 };
+    int phase = PH_BEGIN, stage = 2;
+    double t_step = 0.0, t_s = 0.0, dz_norm = 0.0;
+    int newton_guard = 0, advance_guard = 0;
+    int jac_pending = 0;  // Jacobians due at the top of the next pass (same y and t)
+    double t_jac = 0.0;
+    bool fact_pending = false;
+
     const double t0 = a.t, interval = a.interval;
-    const double min_dt = a.sp.min_dt;
+    const double min_dt = sp.min_dt;
     double local_t = 0;
     uint8_t status = 0;
-    double h = std_max(s.c.s_fac * s.prev_dt * pow((s.c.tol / s.loc_error), 0.25), min_dt);
-    h = std_min(h, interval);
-    if (s.first_step) {
-        s.prev_dt = h;
-        s.ode_jacobian(y, t0);
-    }
     uint64_t guard = 0;
-    while (local_t < interval) {
+    // ESDIRK23a::forward (ESDIRK23a.cpp:280-316)
+    double h = std_max(c.s_fac * prev_dt * pow((c.tol / loc_error), 0.25), min_dt);
+    h = std_min(h, interval);
+    if (first_step) {
+        prev_dt = h;
+        jac_pending = 1;
+        t_jac = t0;
+    }
+    // top of the while loop of forward: returns false when the interval is done
+    auto outer_begin = [&]() -> bool {
+        if (!(local_t < interval))
+            return false;
         if (++guard > a.max_loop) {
             status |= GOSS_FLAG_ITERATION_CAP;
-            break;
+            return false;
         }
         if (h * 1.1 >= interval - local_t)
             h = interval - local_t;
-        if (s.newton_iterations >= 2)
-            s.ode_jacobian(y, t0 + local_t);
-        if (fabs((h - s.prev_dt) / s.prev_dt) > 0.2 || s.new_jacobian)
-            s.factorize(h);
-        s.advance(y, t0 + local_t, h);
-        s.prev_dt = h;
+        if (newton_iterations >= 2) {
+            jac_pending += 1;
+            t_jac = t0 + local_t;
+        }
+        if (fabs((h - prev_dt) / prev_dt) > 0.2 || new_jacobian || jac_pending)
+            fact_pending = true;
+        t_step = t0 + local_t;
+        advance_guard = 0;
+        phase = PH_BEGIN;
+        return true;
+    };
+    // compute_stage_val's entry
+    auto start_stage = [&](int st, double t_stage) {
+        stage = st;
+        t_s = t_stage;
+        newton_iterations = 0;
+        dz_norm = 0.0;
+        newton_guard = 0;
+        eta = pow(std_max(eta, c.etamin), 0.8);
+        phase = PH_NEWTON;
+    };
+    // the end of advance_one_step and of the while loop's body
+    auto end_advance = [&]() -> bool {
+        new_jacobian = 0;
+        prev_dt = h;
         local_t += h;
-        h = std_max(s.c.s_fac * s.prev_dt * pow((s.c.tol / s.loc_error), 0.25), min_dt);
+        h = std_max(c.s_fac * prev_dt * pow((c.tol / loc_error), 0.25), min_dt);
+        return outer_begin();
+    };
+    // do_step returned false: advance_one_step's retry loop
+    auto step_failed = [&]() -> bool {
+        if (h > min_dt && ++advance_guard < 4096) {
+            if (!new_jacobian) {
+                jac_pending = 1;
+                t_jac = t_step;
+            }
+            // reduce_time_step (ESDIRK23a.cpp:260-278)
+            double reduction_factor = 1.0, e = loc_error;
+            int g = 0;
+            do {
+                reduction_factor *= 0.6;
+                e *= 0.1;
+            } while (e > c.tol && ++g < 4096);
+            h = std_max(reduction_factor * h, min_dt);
+            fact_pending = true;
+            phase = PH_BEGIN;
+            return true;
+        }
+        return end_advance();
+    };
+
+    bool running = outer_begin();
+    while (running) {
+        // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
+        if (jac_pending) {
+            double g1[n];  // f(y), a by-product of the fused evaluations
+            if constexpr (J32) {
+                (void)g1;
+                jacobian32<M>(y, t_jac, a.P32, a.P, F, jac);
+            } else if constexpr (M::has_jacobian && GOSS_IMPLICIT_SPLIT) {
+                M::template rhs_jacobian<double>(y, t_jac, a.P, a.P, F, g1, jac);
+            } else if constexpr (GOSS_IMPLICIT_SPLIT) {
+                M::fd_clear(jac);
+                M::template rhs_fd_jacobian<double>(y, t_jac, a.P, a.P, F, g1, jac);
+            } else {
+                rhs64<M>(y, t_jac, a.P, F, g1);
+                compute_jacobian<M>(y, t_jac, a.P, F, jac, g1);
+            }
+            jac_comp += jac_pending;
+            jac_pending = 0;
+            new_jacobian = 1;
+        }
+        // ESDIRK23a::compute_factorized_jacobian(dt) (ESDIRK23a.cpp:101-115)
+        if (fact_pending) {
+            M::lu_copy_shift(jac, jfac, -h * c.a22);
+            M::lu_factorize(jfac);
+            fact_pending = false;
+        }
+        // the pass's right-hand side: f(y, t) at an attempt's start, else
+        // f(y + h prev + gamma h z, t_s) of a Newton iteration
+        double f[n];
+        if (phase != PH_ERROR) {
+            double x[n];
+#pragma unroll
+            for (int i = 0; i < n; i++)
+                x[i] = phase == PH_BEGIN ? y[i] : y[i] + h * prev[i] + c.gamma * h * z[i];
+            rhs64<M>(x, phase == PH_BEGIN ? t_step : t_s, a.P, F, f);
+        }
+        // the pass's substitution: the Newton update, or the error estimate
+        double dz[n];
+        if (phase != PH_BEGIN) {
+            double v[n];
+#pragma unroll
+            for (int i = 0; i < n; i++)
+                v[i] = phase == PH_NEWTON
+                           ? -z[i] + f[i]
+                           : h * ((c.b1 - c.bh1) * z1[i] + (c.b2 - c.bh2) * z2[i] + (c.b3 - c.gamma) * z3[i] +
+                                  c.gamma * z[i]);
+            M::lu_solve(jfac, v, dz);
+        }
+        if (phase == PH_BEGIN) {
+            // do_step: z1 = f(y, t0), z2 = z1, prev = a21 z1
+#pragma unroll
+            for (int i = 0; i < n; i++) {
+                z1[i] = f[i];
+                z[i] = f[i];
+                prev[i] = f[i] * c.a21;
+            }
+            start_stage(2, t_step + c.c2 * h);
+        } else if (phase == PH_NEWTON) {
+            // one iteration of compute_stage_val (ESDIRK23a.cpp:201-258)
+            const double prev_dz_norm = dz_norm;
+            dz_norm = l2norm<n>(dz);
+            bool fail = false;
+            if (newton_iterations >= 1) {
+                const double theta = dz_norm / prev_dz_norm;
+                if (!(theta <= 1)) {
+                    rejects += 1;
+                    fail = true;
+                } else {
+                    eta = theta / (1.0 - theta);
+                }
+            }
+            if (!fail && (newton_iterations > sp.max_iterations || ++newton_guard > 100000)) {
+                rejects += 1;
+                fail = true;
+            }
+            if (fail) {
+                running = step_failed();
+                continue;
+            }
+#pragma unroll
+            for (int i = 0; i < n; i++)
+                z[i] += dz[i];
+            newton_iterations++;
+            if (!(eta * dz_norm > c.kappa * c.tol)) {
+                if (stage == 2) {
+#pragma unroll
+                    for (int i = 0; i < n; i++) {
+                        z2[i] = z[i];
+                        prev[i] = z1[i] * c.bh1 + z2[i] * c.bh2;
+                    }
+                    start_stage(3, t_step + c.c3 * h);
+                } else if (stage == 3) {
+#pragma unroll
+                    for (int i = 0; i < n; i++) {
+                        z3[i] = z[i];
+                        prev[i] = z1[i] * c.b1 + z2[i] * c.b2 + z3[i] * c.b3;
+                    }
+                    start_stage(4, t_step + c.c4 * h);
+                } else {
+                    phase = PH_ERROR;  // z holds z4
+                }
+            }
+        } else {
+            // do_step's error test (ESDIRK23a.cpp:180-196)
+            loc_error = l2norm<n>(dz);
+            if (loc_error > c.tol) {
+                rejects += 1;
+                running = step_failed();
+            } else {
+#pragma unroll
+                for (int i = 0; i < n; i++)
+                    y[i] = y[i] + h * (c.b1 * z1[i] + c.b2 * z2[i] + c.b3 * z3[i] + c.gamma * z[i]);
+                accepted += 1;
+                running = end_advance();
+            }
+        }
     }
-    s.first_step = 0;
+    first_step = 0;
     bool finite = true;
     for (int i = 0; i < n; ++i) {
         a.states[i * ld + node] = y[i];
@@ -1166,15 +1155,15 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
     }
     if (!finite)
         status |= GOSS_FLAG_NONFINITE;
-    ss[ES_PREV_DT * ld] = s.prev_dt;
-    ss[ES_LOC_ERROR * ld] = s.loc_error;
-    ss[ES_ETA * ld] = s.eta;
-    ss[ES_NEWTON_IT * ld] = s.newton_iterations;
-    ss[ES_FIRST * ld] = s.first_step;
-    ss[ES_NEWJAC * ld] = s.new_jacobian;
-    ss[ES_JACCOMP * ld] = s.jac_comp;
-    ss[ES_REJECTS * ld] = s.rejects;
-    ss[ES_ACCEPTED * ld] = s.accepted;
+    ss[ES_PREV_DT * ld] = prev_dt;
+    ss[ES_LOC_ERROR * ld] = loc_error;
+    ss[ES_ETA * ld] = eta;
+    ss[ES_NEWTON_IT * ld] = newton_iterations;
+    ss[ES_FIRST * ld] = first_step;
+    ss[ES_NEWJAC * ld] = new_jacobian;
+    ss[ES_JACCOMP * ld] = jac_comp;
+    ss[ES_REJECTS * ld] = rejects;
+    ss[ES_ACCEPTED * ld] = accepted;
     if (status) {
         a.node_status[node] |= status;
         atomicOr(a.flags, (uint32_t)status);
@@ -1301,12 +1290,6 @@ inline int launch_implicit(const goss_launch* L)
     if (grid == 0)
         return 0;
     const cudaStream_t st = (cudaStream_t)L->stream;
-    const size_t esmem = GOSS_ESDIRK_SMEM ? sizeof(double) * 5 * (size_t)M::num_states * block : 0;
-    if (L->solver == GOSS_ESDIRK23A && esmem > 48 * 1024) {
-        auto k = j32 ? esdirk_kernel<M, M::has_jacobian> : esdirk_kernel<M, false>;
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem) != cudaSuccess)
-            return GOSS_ERR_CUDA;
-    }
     if (j32) {
         if constexpr (M::has_jacobian) {
             if (L->solver == GOSS_THETA)
@@ -1314,14 +1297,14 @@ inline int launch_implicit(const goss_launch* L)
             else if (L->solver == GOSS_IMPLICIT_EULER)
                 theta_kernel<M, true, true><<<grid, block, 0, st>>>(a);
             else
-                esdirk_kernel<M, true><<<grid, block, esmem, st>>>(a);
+                esdirk_kernel<M, true><<<grid, block, 0, st>>>(a);
         }
     } else if (L->solver == GOSS_THETA) {
         theta_kernel<M, false><<<grid, block, 0, st>>>(a);
     } else if (L->solver == GOSS_IMPLICIT_EULER) {
         theta_kernel<M, true><<<grid, block, 0, st>>>(a);
     } else {
-        esdirk_kernel<M><<<grid, block, esmem, st>>>(a);
+        esdirk_kernel<M><<<grid, block, 0, st>>>(a);
     }
     return cudaPeekAtLastError() == cudaSuccess ? 0 : GOSS_ERR_CUDA;
 }

@@ -352,7 +352,10 @@ def test_tt04_implicit_fp32_jacobian(solver, steps, ldt, sp):
                                 precision="single", solver_params=sp)
     assert system.precision == "single"
     assert np.isfinite(g32).all()
-    assert parity_scaled(g32, cpu, rtol=1e-8) <= 1.0
+    # ThetaSolver/ImplicitEuler: the matrix only steers Newton; ESDIRK23a's
+    # error estimate solves with it too, ||(I - h gamma J)^-1 h sum (b - bh) z||
+    # (ESDIRK23a.cpp:180-188), so the step sizes follow the FP32 matrix
+    assert parity_scaled(g32, cpu, rtol=1e-8 if solver != "ESDIRK23a" else 1e-6) <= 1.0
     _, _, ac = system.counters()
     assert ac.min() > 0
 
