@@ -1031,6 +1031,15 @@ __global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ Imp
 
     bool running = outer_begin();
     while (running) {
+        if (jac_pending || fact_pending) {
+            // both are due only before an attempt's first stage, which
+            // rewrites z1, z and prev before reading them, and z2, z3 before
+            // reading them: their old values are dead here, and saying so
+            // keeps them out of the registers the Jacobian code needs
+#pragma unroll
+            for (int i = 0; i < n; i++)
+                z1[i] = z2[i] = z3[i] = z[i] = prev[i] = 0.0;
+        }
         // ESDIRK23a::compute_ode_jacobian (ESDIRK23a.h:58-63)
         if (jac_pending) {
             double g1[n];  // f(y), a by-product of the fused evaluations
