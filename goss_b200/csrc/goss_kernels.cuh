@@ -919,8 +919,15 @@ __device__ __forceinline__ EsdirkCoef esdirk_coefficients()
 // Per node the operations and their order are the nested form's
 // (ESDIRK23a::forward, advance_one_step, do_step, compute_stage_val,
 // reduce_time_step; ESDIRK23a.cpp:101-316).
+#ifndef GOSS_ESDIRK_THREADS
+#define GOSS_ESDIRK_THREADS 128
+#endif
+#ifndef GOSS_ESDIRK_MIN_BLOCKS
+#define GOSS_ESDIRK_MIN_BLOCKS 1
+#endif
 template <class M, bool J32 = false>
-__global__ void __launch_bounds__(128) esdirk_kernel(const __grid_constant__ ImplicitArgs<M> a)
+__global__ void __launch_bounds__(GOSS_ESDIRK_THREADS, GOSS_ESDIRK_MIN_BLOCKS)
+    esdirk_kernel(const __grid_constant__ ImplicitArgs<M> a)
 {
     constexpr int n = M::num_states;
     const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1293,7 +1300,7 @@ inline int launch_implicit(const goss_launch* L)
     // ESDIRK23a: 64 (limit 128)
     const bool theta = L->solver == GOSS_THETA || L->solver == GOSS_IMPLICIT_EULER;
     const unsigned block = L->block ? L->block : (theta ? GOSS_THETA_THREADS : 64);
-    if (block > (theta ? (unsigned)GOSS_THETA_THREADS : 128u))
+    if (block > (theta ? (unsigned)GOSS_THETA_THREADS : (unsigned)GOSS_ESDIRK_THREADS))
         return GOSS_ERR_ARGUMENT;
     const unsigned grid = (L->num_nodes + block - 1) / block;
     if (grid == 0)
