@@ -441,8 +441,26 @@ __device__ __forceinline__ void explicit_node_from(const NodeIO& a, uint32_t nod
     explicit_node_core<M, T, S>(a, node, P, PD, y, F);
 }
 
+// Resident blocks of 128 threads per SM the explicit kernels are compiled for
+// (register cap 65536 / (128 * blocks)).  FP64: 3 for the one-evaluation
+// steps (170 registers), 4 for those with two or more evaluations (128
+// registers): measured on B200 (TP06, 1,048,576 nodes, four fields) against
+// the uncapped 255 registers, GRL1 3.55e9 -> 4.10e9 cell-steps/s (4: 3.90e9),
+// GRL2 1.09e9 -> 1.82e9 (3: 1.57e9); more warps hide the FP64 latencies
+// better than the spills cost.  FP32: uncapped.
+#ifndef GOSS_EXPLICIT_MIN_BLOCKS_FP32
+#define GOSS_EXPLICIT_MIN_BLOCKS_FP32 1
+#endif
+template <typename T, Explicit S>
+struct ExplicitMinBlocks {
+    static constexpr bool one_eval = S == Explicit::Euler || S == Explicit::GRL1 || S == Explicit::RL1 ||
+                                     S == Explicit::GRL1Printed;
+    static constexpr int value = sizeof(T) == 4 ? GOSS_EXPLICIT_MIN_BLOCKS_FP32 : (one_eval ? 3 : 4);
+};
+
 template <class M, typename T, Explicit S>
-__global__ void __launch_bounds__(128) explicit_kernel(const __grid_constant__ ExplicitArgs<M, T> a)
+__global__ void __launch_bounds__(128, (ExplicitMinBlocks<T, S>::value))
+    explicit_kernel(const __grid_constant__ ExplicitArgs<M, T> a)
 {
     const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= a.N)
