@@ -447,7 +447,9 @@ __device__ __forceinline__ void explicit_node_from(const NodeIO& a, uint32_t nod
 // registers): measured on B200 (TP06, 1,048,576 nodes, four fields) against
 // the uncapped 255 registers, GRL1 3.55e9 -> 4.10e9 cell-steps/s (4: 3.90e9),
 // GRL2 1.09e9 -> 1.82e9 (3: 1.57e9); more warps hide the FP64 latencies
-// better than the spills cost.  FP32: uncapped.
+// better than the spills cost.  FP32: uncapped (150 registers for TP06 GRL1,
+// 3 blocks per SM); capping it at 128 registers measured 2.77e10 against
+// 2.91e10 cell-steps/s.
 #ifndef GOSS_EXPLICIT_MIN_BLOCKS_FP32
 #define GOSS_EXPLICIT_MIN_BLOCKS_FP32 1
 #endif
@@ -491,15 +493,6 @@ struct PackedRows {
 struct PackedTile {
     double* base;
     __device__ __forceinline__ double& operator[](int k) const { return base[(uint64_t)k * 32]; }
-};
-
-// ... or in shared memory: entry k of the block's thread t at base[k * stride]
-// with base = smem + t and stride = blockDim.x, so a warp's accesses to one
-// entry are 32 consecutive words (no bank conflicts)
-struct PackedShared {
-    double* base;
-    uint32_t stride;
-    __device__ __forceinline__ double& operator[](int k) const { return base[(uint32_t)k * stride]; }
 };
 
 __device__ __forceinline__ PackedTile packed_tile(double* region, uint32_t node, int nnz)
