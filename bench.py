@@ -324,13 +324,16 @@ def run_gpu(args, rank, world, dist):
         out["state_max_rel_err_fp32_vs_fp64"] = {n: float(e) for n, e in zip(md["state_names"], state_err)}
         del s64
     # --- end to end through the public API with host buffers -----------------
+    # (V in page-locked host memory: the step's input copied in and its result
+    # copied out through the public API every step)
     e2e = make("single")
-    v_host = np.ascontiguousarray(y0[:, iv:iv + 1])
+    v_host = torch.empty((N, 1), dtype=torch.float64, pin_memory=True).numpy()
+    v_host[:] = y0[:, iv:iv + 1]
     t = 0.0
     for _ in range(args.warmup):
         e2e.field_states = v_host
         e2e.forward(t, INTERVAL)
-        v_host = e2e.field_states
+        e2e.get_field_states(out=v_host)
         t += INTERVAL
     torch.cuda.synchronize()
     if dist:
@@ -339,7 +342,7 @@ def run_gpu(args, rank, world, dist):
     for _ in range(args.steps):
         e2e.field_states = v_host          # H2D: this step's input (V), N doubles
         e2e.forward(t, INTERVAL)           # synchronous like the reference
-        v_host = e2e.field_states          # D2H: this step's result (V), N doubles
+        e2e.get_field_states(out=v_host)   # D2H: this step's result (V), N doubles
         t += INTERVAL
     e2e_s = time.perf_counter() - w0
     del e2e
@@ -360,7 +363,8 @@ def run_gpu(args, rank, world, dist):
         fp32_over_fp64=(fp64_ms_max / ms32) if fp64_ms else None,
         v_max_rel_err_fp32_vs_fp64=err,
         e2e={"value": cell_steps / e2e_s, "unit": "cell-steps/s", "h2d_bytes_per_step": 8 * N,
-             "d2h_bytes_per_step": 8 * N, "path": "ODESystemSolver.field_states/forward (public Python API)"},
+             "d2h_bytes_per_step": 8 * N, "path": "ODESystemSolver.field_states / forward / get_field_states "
+                                                   "(public Python API), V in page-locked host memory"},
         model_time_ms=t_end,
     ))
     return out, md
@@ -768,16 +772,17 @@ def run_coupled(dev, steps=200, pde_dt=0.1):
     out["device"] = {"value": cell_steps / (ms / 1e3), "ms_per_exchange": ms / steps}
     del cpl, system
     system = make()
-    vh = np.ascontiguousarray(y0[:, iv:iv + 1])
+    vh = torch.empty((N_NODES, 1), dtype=torch.float64, pin_memory=True).numpy()
+    vh[:] = y0[:, iv:iv + 1]
     for k in range(5):
         system.field_states = vh
         system.forward(k * pde_dt, pde_dt)
-        vh = system.field_states
+        system.get_field_states(out=vh)
     w0 = time.perf_counter()
     for k in range(5, 5 + steps):
         system.field_states = vh
         system.forward(k * pde_dt, pde_dt)
-        vh = system.field_states
+        system.get_field_states(out=vh)
     s = time.perf_counter() - w0
     out["host_copies"] = {"value": cell_steps / s, "ms_per_exchange": 1e3 * s / steps}
     out["workload"] = (f"{MODEL} FP32 GRL1 dt=0.01ms, {N_NODES} nodes, V exchanged every {pde_dt} ms, "

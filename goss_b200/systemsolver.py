@@ -183,6 +183,20 @@ class ODESystemSolver:
         _capi.check(self._L.goss_system_set_field_states(self._h, _capi.ptr(field_states),
                                                           int(self._tangled_storage)), self._h)
 
+    def get_field_states(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The field states, into ``out`` when given (a C-contiguous float64
+        array of num_nodes x num_field_states values, e.g. in page-locked host
+        memory the copy from the device can go to directly)."""
+        if out is None:
+            return self.field_states
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                and out.size == self._num_nodes * self._ode.num_field_states):
+            raise ValueError("out must be a C-contiguous float64 array of "
+                             f"{self._num_nodes * self._ode.num_field_states} values")
+        _capi.check(self._L.goss_system_get_field_states(self._h, _capi.ptr(out), int(self._tangled_storage)),
+                    self._h)
+        return out
+
     def get_field_state_components(self, components) -> np.ndarray:
         comps = np.ascontiguousarray(components, dtype=np.uint32)
         out = np.zeros((self._num_nodes, self._ode.num_field_states))

@@ -172,3 +172,13 @@ def test_solver_trace_rejects_solvers_without_adjoint():
     ode = goss.ParameterizedODE("fitzhughnagumo", field_parameters=["a", "b"])
     with pytest.raises(ValueError):
         SolverTrace(ode, 4, 1.0, 10, 2, 10, solver="ThetaSolver")
+
+
+def test_get_field_states_into_a_caller_array_checks_its_shape():
+    import goss_b200 as goss
+
+    ode = goss.ParameterizedODE("oscilator", field_states=["x"])
+    with pytest.raises(ValueError):
+        # the check precedes any device work
+        goss.ODESystemSolver.get_field_states(
+            type("S", (), {"_num_nodes": 4, "_ode": ode})(), out=np.zeros((3, 1)))

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 import pytest
+import torch
 
 import goss_b200 as goss
 from goss_b200._capi import GossError
@@ -143,6 +144,11 @@ def test_field_states():
     assert (system.field_states == 0).all()
     with pytest.raises(ValueError):
         system.field_states = np.zeros((4, 2))
+    # into a caller's page-locked array
+    pinned = torch.empty((3, 2), dtype=torch.float64, pin_memory=True).numpy()
+    system.field_states = np.arange(6.0).reshape(3, 2)
+    assert system.get_field_states(out=pinned) is pinned
+    assert np.array_equal(pinned, np.arange(6.0).reshape(3, 2))
 
 
 def test_field_state_components_untangled_layout():
