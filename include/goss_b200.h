@@ -403,11 +403,10 @@ GOSS_API const char* goss_batch_last_error(const goss_batch* batch);
  * this library keeps until the process exits; (n + nfp + width) * count,
  * with count rounded up to 32, must fit or the call fails with
  * GOSS_ERR_ARGUMENT.  The first call on a device, and the first after the
- * device's context was reset, looks up that array's device address; make
- * that first call before any stream capture begins.  All calls share the
- * array and it keeps the last call's contents, so calls that overlap on the
- * GPU (other streams, other threads) race; the call synchronises `stream`
- * before it returns.  A CUDA error left pending by earlier work is reported
+ * device's context was reset, looks up that array's device address.  All
+ * calls share the array and it keeps the last call's contents, so calls that
+ * overlap on the GPU (other streams, other threads) race; the call
+ * synchronises `stream` before it returns.  A CUDA error left pending by earlier work is reported
  * (GOSS_ERR_CUDA) and left pending. */
 GOSS_API int goss_model_eval_noalloc(const goss_model_desc* model, int32_t what, int32_t precision,
                                      const double* params, const double* states, const double* field_params,
