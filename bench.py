@@ -230,6 +230,14 @@ def max_over_ranks(values, dist, device):
     return [float(x) for x in t.tolist()]
 
 
+def side_legs(args, world):
+    """Whether this run adds the one-GPU figures after the headline (GRL2,
+    accuracy against the reference, batched, adjoint, implicit, coupled legs):
+    at one process only, since every one of them is a per-GPU figure and under
+    torchrun they would hold all N GPUs for minutes without changing."""
+    return not args.skip_fp64 and world == 1
+
+
 def run_gpu(args, rank, world, dist):
     import torch
 
@@ -347,12 +355,13 @@ def run_gpu(args, rank, world, dist):
     e2e_s = time.perf_counter() - w0
     del e2e
 
-    out["grl2"] = run_grl2(dev, y0, fp) if not args.skip_fp64 else None
-    out["accuracy"] = run_accuracy(dev) if not args.skip_fp64 and rank == 0 else None
-    out["batched"] = run_batched(args, dev) if not args.skip_fp64 else None
-    out["adjoint"] = run_adjoint(dev) if not args.skip_fp64 else None
-    out["implicit"] = run_implicit(dev) if not args.skip_fp64 else None
-    out["coupled"] = run_coupled(dev) if not args.skip_fp64 else None
+    side = side_legs(args, world)
+    out["grl2"] = run_grl2(dev, y0, fp) if side else None
+    out["accuracy"] = run_accuracy(dev) if side and rank == 0 else None
+    out["batched"] = run_batched(args, dev) if side else None
+    out["adjoint"] = run_adjoint(dev) if side else None
+    out["implicit"] = run_implicit(dev) if side else None
+    out["coupled"] = run_coupled(dev) if side else None
 
     ms32, fp64_ms_max, e2e_s = max_over_ranks([ms32, fp64_ms or 0.0, e2e_s], dist, "cuda")
     cell_steps = float(N) * steps_per_call * args.steps * world

@@ -75,3 +75,13 @@ def test_reference_arm_on_a_non_zero_rank_exits_without_output():
                           env=env, capture_output=True, text=True, timeout=300)
     assert proc.returncode == 0
     assert proc.stdout.strip() == ""
+
+
+def test_side_legs_run_at_one_process_only():
+    class A:
+        skip_fp64 = False
+
+    assert bench.side_legs(A, 1)
+    assert not bench.side_legs(A, 2) and not bench.side_legs(A, 8)
+    A.skip_fp64 = True
+    assert not bench.side_legs(A, 1)
