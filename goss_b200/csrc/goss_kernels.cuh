@@ -936,6 +936,9 @@ __device__ __forceinline__ EsdirkCoef esdirk_coefficients()
 #ifndef GOSS_ESDIRK_MIN_BLOCKS
 #define GOSS_ESDIRK_MIN_BLOCKS 1
 #endif
+#ifndef GOSS_ESDIRK_REUSE_F
+#define GOSS_ESDIRK_REUSE_F 1
+#endif
 template <class M, bool J32 = false>
 __global__ void __launch_bounds__(GOSS_ESDIRK_THREADS, GOSS_ESDIRK_MIN_BLOCKS)
     esdirk_kernel(const __grid_constant__ ImplicitArgs<M> a)
@@ -1049,6 +1052,9 @@ __global__ void __launch_bounds__(GOSS_ESDIRK_THREADS, GOSS_ESDIRK_MIN_BLOCKS)
 
     bool running = outer_begin();
     while (running) {
+        // f(y, t_step) of an attempt's first stage, when this pass's Jacobian
+        // evaluation produced it (then held in z1)
+        bool f_known = false;
         if (jac_pending || fact_pending) {
             // both are due only before an attempt's first stage, which
             // rewrites z1, z and prev before reading them, and z2, z3 before
@@ -1076,6 +1082,19 @@ __global__ void __launch_bounds__(GOSS_ESDIRK_THREADS, GOSS_ESDIRK_MIN_BLOCKS)
             jac_comp += jac_pending;
             jac_pending = 0;
             new_jacobian = 1;
+            // The Jacobian is due only before an attempt's first stage and is
+            // taken at that stage's (y, t_step); the evaluation that fused it
+            // with f(y) leaves f(y, t_step), which do_step (ESDIRK23a.cpp:
+            // 134-140) evaluates once more for z1.  Only the FP32 Jacobian
+            // does not produce it.
+            if constexpr (!J32 && GOSS_ESDIRK_REUSE_F) {
+                if (phase == PH_BEGIN && t_jac == t_step) {
+#pragma unroll
+                    for (int i = 0; i < n; i++)
+                        z1[i] = g1[i];
+                    f_known = true;
+                }
+            }
         }
         // ESDIRK23a::compute_factorized_jacobian(dt) (ESDIRK23a.cpp:101-115)
         if (fact_pending) {
@@ -1086,7 +1105,7 @@ __global__ void __launch_bounds__(GOSS_ESDIRK_THREADS, GOSS_ESDIRK_MIN_BLOCKS)
         // the pass's right-hand side: f(y, t) at an attempt's start, else
         // f(y + h prev + gamma h z, t_s) of a Newton iteration
         double f[n];
-        if (phase != PH_ERROR) {
+        if (phase != PH_ERROR && !f_known) {
             double x[n];
 #pragma unroll
             for (int i = 0; i < n; i++)
@@ -1109,9 +1128,10 @@ __global__ void __launch_bounds__(GOSS_ESDIRK_THREADS, GOSS_ESDIRK_MIN_BLOCKS)
             // do_step: z1 = f(y, t0), z2 = z1, prev = a21 z1
 #pragma unroll
             for (int i = 0; i < n; i++) {
-                z1[i] = f[i];
-                z[i] = f[i];
-                prev[i] = f[i] * c.a21;
+                const double fi = f_known ? z1[i] : f[i];
+                z1[i] = fi;
+                z[i] = fi;
+                prev[i] = fi * c.a21;
             }
             start_stage(2, t_step + c.c2 * h);
         } else if (phase == PH_NEWTON) {
