@@ -182,3 +182,24 @@ def test_get_field_states_into_a_caller_array_checks_its_shape():
         # the check precedes any device work
         goss.ODESystemSolver.get_field_states(
             type("S", (), {"_num_nodes": 4, "_ode": ode})(), out=np.zeros((3, 1)))
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the behaviour without a GPU")
+def test_without_a_gpu_the_system_fails_loudly():
+    # no CPU path stands behind the API: without a device the runtime's first
+    # CUDA call raises
+    import goss_b200 as goss
+    from goss_b200._capi import GossError
+
+    ode = goss.ParameterizedODE("oscilator")
+    with pytest.raises(GossError, match="CUDA"):
+        goss.ODESystemSolver(4, goss.solvers.GRL1(ode), ode)
+
+
+def test_missing_runtime_library_raises(monkeypatch, tmp_path):
+    from goss_b200 import _capi
+
+    monkeypatch.setattr(_capi, "RUNTIME_SO", tmp_path / "libgoss_b200.so")
+    monkeypatch.setattr(_capi, "_lib", None)
+    with pytest.raises(_capi.ExtensionMissingError, match="is missing"):
+        _capi.lib()
