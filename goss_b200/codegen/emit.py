@@ -588,7 +588,57 @@ class ModelSource:
                                     prT, prD)
         return lines
 
-    def _dev_fd_jacobian_lines(self, with_rhs: bool = False, with_t0: bool = False) -> List[str]:
+    def _dev_rhs_jacobian_sel_lines(self) -> List[str]:
+        """Body of ``rhs_jacobian_sel``: ``rhs2_jacobian``'s program with the
+        statements that only the Jacobian needs, and the Jacobian's outputs,
+        under ``if (want_jac)``, and f0's time-dependent statements under
+        ``if (want_f0)``: one inlined copy of the model serves every Newton
+        iteration (f alone, f and the Jacobian, f at two times)."""
+        rhs, jac = self.rhs, self._packed_jacobian()
+        names = {b.name for b in rhs.body if isinstance(b, Assign)}
+        body = [b for b in rhs.body if isinstance(b, Assign)]
+        body += [b for b in jac.body if isinstance(b, Assign) and b.name not in names]
+        body += [b for b in rhs.body if isinstance(b, Output)] + [b for b in jac.body if isinstance(b, Output)]
+        folded = self._fold(Program("rhs_jacobian", body, None))
+        inter = {n: self.model.sym(n) for n in self.model.intermediates}
+        rp = ReverseProgram(folded, [self.model.sym(s) for s in self.states],
+                            [self.model.sym(p) for p in self.fparams], inter, reverse=False)
+        prT, prD = self._dev_printers(split=True)
+        fwd = list(rp.forward)
+        f_outs = [o for o in rp.outputs if o.array == "values"]
+        j_outs = [o for o in rp.outputs if o.array == "jac"]
+        by_name = {b.name: b for b in fwd}
+        need, stack = set(), [x.name for o in f_outs for x in o.expr.free_symbols]
+        while stack:
+            nm = stack.pop()
+            if nm in by_name and nm not in need:
+                need.add(nm)
+                stack.extend(x.name for x in by_name[nm].expr.free_symbols)
+
+        def stmt(b):
+            if b.cls == TIME_CLS:
+                return f"const double v_{b.name} = {prD(b.expr)};"
+            return f"const T v_{b.name} = {prT(factor_common(b.expr))};"
+
+        n = len(self.states)
+        lines = [stmt(b) for b in fwd if b.name in need]
+        lines += [f"f1[{o.index}] = {prT(factor_common(o.expr))};" for o in f_outs]
+        done = {o.index for o in f_outs}
+        lines += [f"f1[{i}] = T(0.0);" for i in range(n) if i not in done]
+        lines.append("if (want_jac) {")
+        lines += ["  " + stmt(b) for b in fwd if b.name not in need]
+        lines += [f"  J[{o.index}] = {prT(factor_common(o.expr))};" for o in j_outs]
+        done = {o.index for o in j_outs}
+        lines += [f"  J[{i}] = T(0.0);" for i in range(self.lus.nnz) if i not in done]
+        lines.append("}")
+        lines.append("if (want_f0) {")
+        lines += ["  " + x for x in self._t0_lines([b for b in fwd if b.name in need],
+                                                  {o.index: o for o in f_outs}, prT, prD)]
+        lines.append("}")
+        return lines
+
+    def _dev_fd_jacobian_lines(self, with_rhs: bool = False, with_t0: bool = False,
+                               select: bool = False) -> List[str]:
         """Body of ``fd_jacobian``: the forward-difference Jacobian of the split
         right-hand side into the packed Newton matrix.  The unperturbed
         statements are evaluated once; column i then recomputes, for
@@ -632,6 +682,8 @@ class ModelSource:
                 lines.append(f"f1[{r}] = {prT(factor_common(outs[r].expr)) if r in outs else 'T(0.0)'};")
             if with_t0:
                 lines += self._t0_lines(binds, outs, prT, prD)
+        if select:  # the columns only if want_jac (J is left as it is otherwise)
+            lines += ["if (want_jac) {", "fd_clear(J);"]
         for i in range(n):
             rows = [r for r in range(n) if self.lus.jac[r][i] and r in outs]
             if not rows:
@@ -655,6 +707,8 @@ class ModelSource:
             for r in rows:
                 f2 = prT(factor_common(outs[r].expr.xreplace(sub)))
                 lines.append(f"  J[{self.lus.pos[(r, i)]}] = (({f2}) - f1[{r}]) / d;")
+            lines.append("}")
+        if select:
             lines.append("}")
         return lines
 
@@ -789,11 +843,31 @@ class ModelSource:
             L.append("    (void)time; (void)t0; (void)P; (void)PD; (void)F; (void)f0; (void)f1; (void)J;")
             L.append("  }")
             L.append("")
+            L.append("  // f1 = f(y, time); the Jacobian only if want_jac (J is left as it is otherwise), f0 =")
+            L.append("  // f(y, t0) only if want_f0: rhs2_jacobian with its parts selected at run time")
+            L.append("  template <typename T, class A>")
+            L.append(f"  __device__ static __forceinline__ void rhs_jacobian_sel({sig}, const double t0,")
+            L.append("      const bool want_f0, const bool want_jac, T* __restrict__ f0, T* __restrict__ f1, A J)")
+            L.append("  {")
+            L += ["    " + x for x in head + self._dev_rhs_jacobian_sel_lines()]
+            L.append("    (void)time; (void)t0; (void)P; (void)PD; (void)F; (void)f0; (void)f1; (void)J;")
+            L.append("  }")
+            L.append("")
         L.append("  // the same, also writing f1 = f(y, time) (rhs_split) from its unperturbed statements")
         L.append("  template <typename T, class A>")
         L.append(f"  __device__ static __forceinline__ void rhs_fd_jacobian({sig}, T* __restrict__ f1, A J)")
         L.append("  {")
         L += ["    " + x for x in head + self._dev_fd_jacobian_lines(with_rhs=True)]
+        L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
+        L.append("  }")
+        L.append("")
+        L.append("  // f1 = f(y, time), and the forward-difference Jacobian only if want_jac (J is left as it")
+        L.append("  // is otherwise): rhs_fd_jacobian with its columns selected at run time")
+        L.append("  template <typename T, class A>")
+        L.append(f"  __device__ static __forceinline__ void rhs_fd_jacobian_sel({sig}, const bool want_jac,")
+        L.append("      T* __restrict__ f1, A J)")
+        L.append("  {")
+        L += ["    " + x for x in head + self._dev_fd_jacobian_lines(with_rhs=True, select=True)]
         L.append("    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;")
         L.append("  }")
         L.append("")

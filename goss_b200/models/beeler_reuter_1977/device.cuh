@@ -820,6 +820,197 @@ struct M_beeler_reuter_1977 {
     (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
   }
 
+  // f1 = f(y, time), and the forward-difference Jacobian only if want_jac (J is left as it
+  // is otherwise): rhs_fd_jacobian with its columns selected at run time
+  template <typename T, class A>
+  __device__ static __forceinline__ void rhs_fd_jacobian_sel(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const bool want_jac,
+      T* __restrict__ f1, A J)
+  {
+    const T s_m = y[0];
+    const T s_h = y[1];
+    const T s_j = y[2];
+    const T s_Cai = y[3];
+    const T s_d = y[4];
+    const T s_f = y[5];
+    const T s_x1 = y[6];
+    const T s_V = y[7];
+    const T v_i_Na = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
+    const T v_V_eff_0 = ((gfabs((T(47.0) + s_V)) < T(0.01)) ? T(0.01) : (T(47.0) + s_V));
+    const T v___t0 = gexp2((-T(0.14426950408889636))*v_V_eff_0);
+    const T v___t1 = (T(1.0)/((-T(1.0)) + v___t0));
+    const T v_alpha_m = (v___t1*((-T(47.0)) - ((s_V))));
+    const T v___t2 = gexp2((-T(0.08079092228978195))*s_V);
+    const T v_beta_m = (T(0.7095526727489909)*v___t2);
+    const T v___t3 = gexp2((-T(0.36067376022224085))*s_V);
+    const T v_alpha_h = (T(5.497962438709065e-10)*v___t3);
+    const T v___t4 = gexp2((-T(0.118300993352895))*s_V);
+    const T v___t5 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4)));
+    const T v_beta_h = (T(1.7)*v___t5);
+    const T v___t6 = gexp2((-T(0.14426950408889636))*s_V);
+    const T v___t7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6*v___t6))));
+    const T v_alpha_j = (T(1.8690473007222892e-10)*v___t3*v___t7);
+    const T v___t8 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6)));
+    const T v_beta_j = (T(0.3)*v___t8);
+    const T v___t9 = glog((T(0.001)*s_Cai));
+    const T v___t10 = (T(1.0)/s_Cai);
+    const T v_E_s = ((-T(82.3)) - ((T(13.0287)*v___t9)));
+    const T v_i_s = (s_d*s_f*P[3]*(s_V - ((v_E_s))));
+    const T v___t11 = gexp2((-T(0.10386573368531053))*s_V);
+    const T v___t12 = gexp2((-T(0.014426950408889635))*s_V);
+    const T v___t13 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11)));
+    const T v_alpha_d = (T(0.09987075415572229)*v___t12*v___t13);
+    const T v___t14 = gexp2(T(0.07213475204444818)*s_V);
+    const T v___t15 = gexp2((-T(0.024452458320151922))*s_V);
+    const T v___t16 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14)));
+    const T v_beta_d = (T(0.03320606467536786)*v___t15*v___t16);
+    const T v___t17 = gexp2(T(0.21629610807930486)*s_V);
+    const T v___t18 = gexp2((-T(0.011541560327111707))*s_V);
+    const T v___t19 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17)));
+    const T v_alpha_f = (T(0.009591781612432381)*v___t18*v___t19);
+    const T v___t20 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6*v___t6))));
+    const T v_beta_f = (T(0.0035672756346111717)*v___t20*(v___t12*v___t12));
+    const T v___t21 = gexp2(T(0.05770780163555854)*s_V);
+    const T v___t22 = gexp2((-T(0.05770780163555854))*s_V);
+    const T v_i_x1 = (T(0.0019727757115328517)*v___t22*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
+    const T v___t23 = gexp2(T(0.08243971662222647)*s_V);
+    const T v___t24 = gexp2(T(0.11923099511479036)*s_V);
+    const T v___t25 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23)));
+    const T v_alpha_x1 = (T(0.031158410986342627)*v___t24*v___t25);
+    const T v___t26 = gexp2((-T(0.08654439357462287))*s_V);
+    const T v___t27 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22)));
+    const T v_beta_x1 = (T(0.0003916464405623223)*v___t26*v___t27);
+    const T v_V_eff_1 = ((gfabs((T(23.0) + s_V)) < T(0.01)) ? T(0.01) : (T(23.0) + s_V));
+    const T v___t28 = gexp2((-T(0.05770780163555854))*v_V_eff_1);
+    const T v___t29 = (T(1.0)/(T(1.0) - ((v___t28))));
+    const T v___t30 = (T(1.0)/(v___t21*(T(8.331137487687693) + (T(69.4078518387552)*v___t21))));
+    const T v_i_K1 = (T(0.0035)*((v___t29*(T(4.6000000000000005) + (T(0.2)*s_V))) + (v___t30*((-T(4.0)) + (T(119.85640018958804)*v___t21)))));
+    const double v_Istim = (((time >= PD[8]) && (time <= PD[5]) && ((PD[11] + time + (PD[13]*floor((PD[12]*(PD[11] + time))))) <= PD[7])) ? PD[4] : 0.0);
+    f1[0] = ((v_alpha_m*(T(1.0) - ((s_m)))) - ((v_beta_m*s_m)));
+    f1[1] = ((v_alpha_h*(T(1.0) - ((s_h)))) - ((v_beta_h*s_h)));
+    f1[2] = ((v_alpha_j*(T(1.0) - ((s_j)))) - ((v_beta_j*s_j)));
+    f1[3] = (T(7.000000000000001e-06) - ((T(0.07)*s_Cai)) - ((T(0.01)*v_i_s)));
+    f1[4] = ((v_alpha_d*(T(1.0) - ((s_d)))) - ((v_beta_d*s_d)));
+    f1[5] = ((v_alpha_f*(T(1.0) - ((s_f)))) - ((v_beta_f*s_f)));
+    f1[6] = ((v_alpha_x1*(T(1.0) - ((s_x1)))) - ((v_beta_x1*s_x1)));
+    f1[7] = (P[14]*(T(v_Istim) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s)) - ((v_i_x1))));
+    if (want_jac) {
+    fd_clear(J);
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[0])) ? 1e-5 : fabs(double(y[0]))));
+      const T v___yp0 = T(double(y[0]) + d);
+      const T v_i_Na__k0 = ((s_V + P[10])*(P[2] + (P[1]*s_h*s_j*(v___yp0*v___yp0*v___yp0))));
+      J[0] = ((((v_alpha_m*(T(1.0) - ((v___yp0)))) - ((v___yp0*v_beta_m)))) - f1[0]) / d;
+      J[16] = (((P[14]*(T(v_Istim) - ((v_i_Na__k0)) - ((v_i_K1)) - ((v_i_s)) - ((v_i_x1))))) - f1[7]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[1])) ? 1e-5 : fabs(double(y[1]))));
+      const T v___yp1 = T(double(y[1]) + d);
+      const T v_i_Na__k1 = ((s_V + P[10])*(P[2] + (v___yp1*P[1]*s_j*(s_m*s_m*s_m))));
+      J[2] = ((((v_alpha_h*(T(1.0) - ((v___yp1)))) - ((v___yp1*v_beta_h)))) - f1[1]) / d;
+      J[17] = (((P[14]*(T(v_Istim) - ((v_i_Na__k1)) - ((v_i_K1)) - ((v_i_s)) - ((v_i_x1))))) - f1[7]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[2])) ? 1e-5 : fabs(double(y[2]))));
+      const T v___yp2 = T(double(y[2]) + d);
+      const T v_i_Na__k2 = ((s_V + P[10])*(P[2] + (v___yp2*P[1]*s_h*(s_m*s_m*s_m))));
+      J[4] = ((((v_alpha_j*(T(1.0) - ((v___yp2)))) - ((v___yp2*v_beta_j)))) - f1[2]) / d;
+      J[18] = (((P[14]*(T(v_Istim) - ((v_i_Na__k2)) - ((v_i_K1)) - ((v_i_s)) - ((v_i_x1))))) - f1[7]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[3])) ? 1e-5 : fabs(double(y[3]))));
+      const T v___yp3 = T(double(y[3]) + d);
+      const T v___t9__k3 = glog((T(0.001)*v___yp3));
+      const T v_E_s__k3 = ((-T(82.3)) - ((T(13.0287)*v___t9__k3)));
+      const T v_i_s__k3 = (s_d*s_f*P[3]*(s_V - ((v_E_s__k3))));
+      J[6] = (((T(7.000000000000001e-06) - ((T(0.07)*v___yp3)) - ((T(0.01)*v_i_s__k3)))) - f1[3]) / d;
+      J[19] = (((P[14]*(T(v_Istim) - ((v_i_s__k3)) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_x1))))) - f1[7]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[4])) ? 1e-5 : fabs(double(y[4]))));
+      const T v___yp4 = T(double(y[4]) + d);
+      const T v_i_s__k4 = (v___yp4*s_f*P[3]*(s_V - ((v_E_s))));
+      J[7] = (((T(7.000000000000001e-06) - ((T(0.07)*s_Cai)) - ((T(0.01)*v_i_s__k4)))) - f1[3]) / d;
+      J[10] = ((((v_alpha_d*(T(1.0) - ((v___yp4)))) - ((v___yp4*v_beta_d)))) - f1[4]) / d;
+      J[20] = (((P[14]*(T(v_Istim) - ((v_i_s__k4)) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_x1))))) - f1[7]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[5])) ? 1e-5 : fabs(double(y[5]))));
+      const T v___yp5 = T(double(y[5]) + d);
+      const T v_i_s__k5 = (v___yp5*s_d*P[3]*(s_V - ((v_E_s))));
+      J[8] = (((T(7.000000000000001e-06) - ((T(0.07)*s_Cai)) - ((T(0.01)*v_i_s__k5)))) - f1[3]) / d;
+      J[12] = ((((v_alpha_f*(T(1.0) - ((v___yp5)))) - ((v___yp5*v_beta_f)))) - f1[5]) / d;
+      J[21] = (((P[14]*(T(v_Istim) - ((v_i_s__k5)) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_x1))))) - f1[7]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[6])) ? 1e-5 : fabs(double(y[6]))));
+      const T v___yp6 = T(double(y[6]) + d);
+      const T v_i_x1__k6 = (T(0.0019727757115328517)*v___yp6*v___t22*((-T(1.0)) + (T(21.75840239619708)*v___t21)));
+      J[14] = ((((v_alpha_x1*(T(1.0) - ((v___yp6)))) - ((v___yp6*v_beta_x1)))) - f1[6]) / d;
+      J[22] = (((P[14]*(T(v_Istim) - ((v_i_x1__k6)) - ((v_i_K1)) - ((v_i_Na)) - ((v_i_s))))) - f1[7]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[7])) ? 1e-5 : fabs(double(y[7]))));
+      const T v___yp7 = T(double(y[7]) + d);
+      const T v_i_Na__k7 = ((v___yp7 + P[10])*(P[2] + (P[1]*s_h*s_j*(s_m*s_m*s_m))));
+      const T v_V_eff_0__k7 = ((gfabs((T(47.0) + v___yp7)) < T(0.01)) ? T(0.01) : (T(47.0) + v___yp7));
+      const T v___t0__k7 = gexp2((-T(0.14426950408889636))*v_V_eff_0__k7);
+      const T v___t1__k7 = (T(1.0)/((-T(1.0)) + v___t0__k7));
+      const T v_alpha_m__k7 = (v___t1__k7*((-T(47.0)) - ((v___yp7))));
+      const T v___t2__k7 = gexp2((-T(0.08079092228978195))*v___yp7);
+      const T v_beta_m__k7 = (T(0.7095526727489909)*v___t2__k7);
+      const T v___t3__k7 = gexp2((-T(0.36067376022224085))*v___yp7);
+      const T v_alpha_h__k7 = (T(5.497962438709065e-10)*v___t3__k7);
+      const T v___t4__k7 = gexp2((-T(0.118300993352895))*v___yp7);
+      const T v___t5__k7 = (T(1.0)/(T(1.0) + (T(0.1580253208896478)*v___t4__k7)));
+      const T v_beta_h__k7 = (T(1.7)*v___t5__k7);
+      const T v___t6__k7 = gexp2((-T(0.14426950408889636))*v___yp7);
+      const T v___t7__k7 = (T(1.0)/(T(1.0) + (T(1.6788275299956603e-07)*(v___t6__k7*v___t6__k7))));
+      const T v_alpha_j__k7 = (T(1.8690473007222892e-10)*v___t3__k7*v___t7__k7);
+      const T v___t8__k7 = (T(1.0)/(T(1.0) + (T(0.040762203978366204)*v___t6__k7)));
+      const T v_beta_j__k7 = (T(0.3)*v___t8__k7);
+      const T v_i_s__k7 = (s_d*s_f*P[3]*(v___yp7 - ((v_E_s))));
+      const T v___t11__k7 = gexp2((-T(0.10386573368531053))*v___yp7);
+      const T v___t12__k7 = gexp2((-T(0.014426950408889635))*v___yp7);
+      const T v___t13__k7 = (T(1.0)/(T(1.0) + (T(1.4332881385696572)*v___t11__k7)));
+      const T v_alpha_d__k7 = (T(0.09987075415572229)*v___t12__k7*v___t13__k7);
+      const T v___t14__k7 = gexp2(T(0.07213475204444818)*v___yp7);
+      const T v___t15__k7 = gexp2((-T(0.024452458320151922))*v___yp7);
+      const T v___t16__k7 = (T(1.0)/(T(1.0) + (T(9.02501349943412)*v___t14__k7)));
+      const T v_beta_d__k7 = (T(0.03320606467536786)*v___t15__k7*v___t16__k7);
+      const T v___t17__k7 = gexp2(T(0.21629610807930486)*v___yp7);
+      const T v___t18__k7 = gexp2((-T(0.011541560327111707))*v___yp7);
+      const T v___t19__k7 = (T(1.0)/(T(1.0) + (T(66.5465065250986)*v___t17__k7)));
+      const T v_alpha_f__k7 = (T(0.009591781612432381)*v___t18__k7*v___t19__k7);
+      const T v___t20__k7 = (T(1.0)/(T(1.0) + (T(0.0024787521766663585)*(v___t6__k7*v___t6__k7))));
+      const T v_beta_f__k7 = (T(0.0035672756346111717)*v___t20__k7*(v___t12__k7*v___t12__k7));
+      const T v___t21__k7 = gexp2(T(0.05770780163555854)*v___yp7);
+      const T v___t22__k7 = gexp2((-T(0.05770780163555854))*v___yp7);
+      const T v_i_x1__k7 = (T(0.0019727757115328517)*v___t22__k7*s_x1*((-T(1.0)) + (T(21.75840239619708)*v___t21__k7)));
+      const T v___t23__k7 = gexp2(T(0.08243971662222647)*v___yp7);
+      const T v___t24__k7 = gexp2(T(0.11923099511479036)*v___yp7);
+      const T v___t25__k7 = (T(1.0)/(T(1.0) + (T(17.41170806332765)*v___t23__k7)));
+      const T v_alpha_x1__k7 = (T(0.031158410986342627)*v___t24__k7*v___t25__k7);
+      const T v___t26__k7 = gexp2((-T(0.08654439357462287))*v___yp7);
+      const T v___t27__k7 = (T(1.0)/(T(1.0) + (T(0.4493289641172216)*v___t22__k7)));
+      const T v_beta_x1__k7 = (T(0.0003916464405623223)*v___t26__k7*v___t27__k7);
+      const T v_V_eff_1__k7 = ((gfabs((T(23.0) + v___yp7)) < T(0.01)) ? T(0.01) : (T(23.0) + v___yp7));
+      const T v___t28__k7 = gexp2((-T(0.05770780163555854))*v_V_eff_1__k7);
+      const T v___t29__k7 = (T(1.0)/(T(1.0) - ((v___t28__k7))));
+      const T v___t30__k7 = (T(1.0)/(v___t21__k7*(T(8.331137487687693) + (T(69.4078518387552)*v___t21__k7))));
+      const T v_i_K1__k7 = (T(0.0035)*((v___t29__k7*(T(4.6000000000000005) + (T(0.2)*v___yp7))) + (v___t30__k7*((-T(4.0)) + (T(119.85640018958804)*v___t21__k7)))));
+      J[1] = ((((v_alpha_m__k7*(T(1.0) - ((s_m)))) - ((v_beta_m__k7*s_m)))) - f1[0]) / d;
+      J[3] = ((((v_alpha_h__k7*(T(1.0) - ((s_h)))) - ((v_beta_h__k7*s_h)))) - f1[1]) / d;
+      J[5] = ((((v_alpha_j__k7*(T(1.0) - ((s_j)))) - ((v_beta_j__k7*s_j)))) - f1[2]) / d;
+      J[9] = (((T(7.000000000000001e-06) - ((T(0.07)*s_Cai)) - ((T(0.01)*v_i_s__k7)))) - f1[3]) / d;
+      J[11] = ((((v_alpha_d__k7*(T(1.0) - ((s_d)))) - ((v_beta_d__k7*s_d)))) - f1[4]) / d;
+      J[13] = ((((v_alpha_f__k7*(T(1.0) - ((s_f)))) - ((v_beta_f__k7*s_f)))) - f1[5]) / d;
+      J[15] = ((((v_alpha_x1__k7*(T(1.0) - ((s_x1)))) - ((v_beta_x1__k7*s_x1)))) - f1[6]) / d;
+      J[23] = (((P[14]*(T(v_Istim) - ((v_i_K1__k7)) - ((v_i_Na__k7)) - ((v_i_s__k7)) - ((v_i_x1__k7))))) - f1[7]) / d;
+    }
+    }
+    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
+  }
+
   // the same, also writing f0 = f(y, t0) (only the time-dependent statements again)
   template <typename T, class A>
   __device__ static __forceinline__ void rhs2_fd_jacobian(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const double t0,

@@ -210,6 +210,38 @@ struct M_fhn {
     (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
   }
 
+  // f1 = f(y, time), and the forward-difference Jacobian only if want_jac (J is left as it
+  // is otherwise): rhs_fd_jacobian with its columns selected at run time
+  template <typename T, class A>
+  __device__ static __forceinline__ void rhs_fd_jacobian_sel(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const bool want_jac,
+      T* __restrict__ f1, A J)
+  {
+    const T s_v = y[0];
+    const T s_s = y[1];
+    const T v_I = ((P[11] + s_v)*((P[12]*s_s) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v))))));
+    const double v_i_Stim = (PD[5]*(1.0 - ((1.0/(1.0 + exp((PD[16] + (5.0*time)))))))/(1.0 + exp((PD[15] + (5.0*time)))));
+    f1[0] = (v_I + T(v_i_Stim));
+    f1[1] = (P[1]*(P[11] + s_v + (P[17]*s_s)));
+    if (want_jac) {
+    fd_clear(J);
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[0])) ? 1e-5 : fabs(double(y[0]))));
+      const T v___yp0 = T(double(y[0]) + d);
+      const T v_I__k0 = ((v___yp0 + P[11])*((P[12]*s_s) + (P[14]*(v___yp0 + P[13])*(P[9] - ((v___yp0))))));
+      J[0] = (((v_I__k0 + T(v_i_Stim))) - f1[0]) / d;
+      J[2] = (((P[1]*(v___yp0 + P[11] + (P[17]*s_s)))) - f1[1]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[1])) ? 1e-5 : fabs(double(y[1]))));
+      const T v___yp1 = T(double(y[1]) + d);
+      const T v_I__k1 = ((P[11] + s_v)*((v___yp1*P[12]) + (P[14]*(P[13] + s_v)*(P[9] - ((s_v))))));
+      J[1] = (((v_I__k1 + T(v_i_Stim))) - f1[0]) / d;
+      J[3] = (((P[1]*(P[11] + s_v + (v___yp1*P[17])))) - f1[1]) / d;
+    }
+    }
+    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
+  }
+
   // the same, also writing f0 = f(y, t0) (only the time-dependent statements again)
   template <typename T, class A>
   __device__ static __forceinline__ void rhs2_fd_jacobian(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const double t0,

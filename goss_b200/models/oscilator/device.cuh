@@ -180,6 +180,32 @@ struct M_oscilator {
     (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
   }
 
+  // f1 = f(y, time), and the forward-difference Jacobian only if want_jac (J is left as it
+  // is otherwise): rhs_fd_jacobian with its columns selected at run time
+  template <typename T, class A>
+  __device__ static __forceinline__ void rhs_fd_jacobian_sel(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const bool want_jac,
+      T* __restrict__ f1, A J)
+  {
+    const T s_x = y[0];
+    const T s_y = y[1];
+    f1[0] = (P[2]*s_y);
+    f1[1] = (P[1]*s_x);
+    if (want_jac) {
+    fd_clear(J);
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[0])) ? 1e-5 : fabs(double(y[0]))));
+      const T v___yp0 = T(double(y[0]) + d);
+      J[2] = (((v___yp0*P[1])) - f1[1]) / d;
+    }
+    {
+      const double d = sqrt(1e-15 * (1e-5 > fabs(double(y[1])) ? 1e-5 : fabs(double(y[1]))));
+      const T v___yp1 = T(double(y[1]) + d);
+      J[1] = (((v___yp1*P[2])) - f1[0]) / d;
+    }
+    }
+    (void)time; (void)P; (void)PD; (void)F; (void)f1; (void)J;
+  }
+
   // the same, also writing f0 = f(y, t0) (only the time-dependent statements again)
   template <typename T, class A>
   __device__ static __forceinline__ void rhs2_fd_jacobian(const T* __restrict__ y, const double time, const T* __restrict__ P, const double* __restrict__ PD, const T* __restrict__ F, const double t0,
