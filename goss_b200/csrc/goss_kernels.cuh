@@ -129,7 +129,10 @@ __device__ __forceinline__ double grl_increment(double a, double b, double h, do
 }
 
 // GRL increment of one state, FP32: b*h*phi1(a*h), algebraically identical
-// and free of the cancellation in exp(a*h) - 1 (see phi1f)
+// and free of the cancellation in exp(a*h) - 1 (see phi1f).  (h phi1 with
+// the polynomial's coefficients scaled by h, one multiply fewer per state,
+// measured 1.4 % slower on B200: TP06, 1,048,576 nodes, 162 registers
+// instead of 150.)
 __device__ __forceinline__ float grl_increment(float a, float b, float h, float /*delta*/)
 {
     return b * h * phi1f(a * h);
