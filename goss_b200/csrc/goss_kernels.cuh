@@ -627,7 +627,10 @@ enum ThetaRows { TH_ETA = 0, TH_RECOMPUTE, TH_ALWAYS, TH_JUSTREFINED, TH_JACCOMP
 // nested-loop kernel's bit for bit).  Measured on B200 (TT04, 262,144 nodes,
 // 0.1 ms intervals, blocks of 256 against the nested loops in blocks of 64):
 // ImplicitEuler with the analytic Jacobian 2.49 -> 1.53 ms, ThetaSolver with
-// it 1.24 -> 1.16 ms, with forward differences unchanged (4.41 ms).  Blocks of
+// it 1.24 -> 1.16 ms, with forward differences unchanged (4.41 ms).  Again
+// with one model evaluation site per iteration (below), against each warp
+// looping on its own (__any_sync): ImplicitEuler 1.03 against 1.33 ms (1.56
+// against 2.36 with forward differences), ThetaSolver within 2 %.  Blocks of
 // up to 256 threads; __launch_bounds__(256, 1) keeps the 255-register budget
 // (without the minimum of one block ptxas capped it at 128 and spilled more).
 //
