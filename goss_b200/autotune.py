@@ -123,7 +123,8 @@ def tune_system(system: ODESystemSolver, interval: float, t0: float = 0.0, steps
     saved = system.states
     best = None
     try:
-        lockstep = type(system.solver).__name__ in ("ThetaSolver", "ImplicitEuler")  # kernel blocks up to 256
+        # the implicit kernels run in block lockstep, in blocks of up to 256
+        lockstep = type(system.solver).__name__ in ("ThetaSolver", "ImplicitEuler", "ESDIRK23a")
         for block in (32, 64, 96, 128) + ((192, 256) if lockstep else ()):
             system.set_block_size(block)
             system.forward(t0, interval)
