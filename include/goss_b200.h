@@ -325,8 +325,8 @@ GOSS_API uint32_t goss_system_get_num_threads(const goss_system* sys);
 GOSS_API uint32_t goss_system_num_nodes(const goss_system* sys);
 
 /* Launch configuration (threads per block, a multiple of 32; 0 = the default:
- * 128 for the explicit solvers, 256 for ThetaSolver and ImplicitEuler, 64 for
- * ESDIRK23a; their kernels take at most 128, 256 and 128). */
+ * 128 for the explicit solvers, 256 for the implicit ones, whose blocks run in
+ * lockstep; the kernels take at most 128 and 256). */
 GOSS_API int goss_system_set_block_size(goss_system* sys, uint32_t block);
 
 /* Status word accumulated since the last clear (goss_flag_bits). */
