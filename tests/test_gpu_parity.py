@@ -148,6 +148,26 @@ def test_esdirk_accepting_steps_analytic_jacobian_fp64():
     assert ac.min() > 0
 
 
+@pytest.mark.parametrize("jacobian", [False, True])
+def test_esdirk_lockstep_blocks_with_a_ragged_last_block(jacobian):
+    """The ESDIRK23a kernel runs its per-node passes in block lockstep (blocks
+    of 256, a barrier after every pass until the block's slowest node is done;
+    threads past the last node only take part in the barriers): 3 full blocks
+    and a ragged fourth, nodes with different field values and so different
+    step sequences, against the oracle node by node."""
+    fps = ("g_Kr", "g_CaL")
+    md = meta(variant_dir("tentusscher_2004_mcell", fps, jacobian))
+    rng = np.random.default_rng(31)
+    N = 3 * 256 + 37
+    defaults = np.array([md["default_parameters"][i] for i in md["field_parameter_indices"]])
+    fp = defaults[None, :] * np.exp(0.2 * rng.standard_normal((N, 2)))
+    gpu, cpu, system = run_pair("tentusscher_2004_mcell", "ESDIRK23a", N, 10, 0.1, -1.0, fps, fp,
+                                jacobian=jacobian, solver_params={"min_dt": 1e-4}, spread=0.05)
+    assert parity_scaled(gpu, cpu, rtol=1e-9) <= 1.0
+    _, _, ac = system.counters()
+    assert ac.min() > 0 and len(np.unique(ac)) > 1  # the lanes' step sequences differ
+
+
 def test_tt04_implicit_with_field_parameters():
     fps = ("g_Kr", "g_CaL")
     md = meta(variant_dir("tentusscher_2004_mcell", fps))
